@@ -1,0 +1,243 @@
+/*
+ * memphys.h -- C ABI of libmemphys_cuda.so, the B200 (sm_100a) hot path of
+ * the MeMPhyS meshless solver: PHS-RBF-FD stencil weights, the fixed-width
+ * grad_x/grad_y/grad_z/laplacian operators applied as SpMV, and the
+ * fractional-step pressure-Poisson solve.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (mp_status).  On failure a
+ *    message is kept per host thread and read with mp_last_error().  The
+ *    reference reports the same failures with printf + throw bad_exception()
+ *    (e.g. cloud.cpp:632-636, solver.cpp:317-321); the C++ adapters in
+ *    memphys_b200/host turn non-OK statuses back into that exception.
+ *  - Array arguments may be host or device memory (unified addressing).
+ *    Host arrays are copied in/out on the call's stream; device arrays are
+ *    used in place.  Handles own their device buffers.
+ *  - Handles are not re-entrant: one handle per host thread / stream.
+ *  - Node ordering, stencil ordering and the CSR-aligned weight layout are
+ *    those of the reference's CLOUD (cloud.cpp:251-258): stencil row i has
+ *    exactly n entries, the node itself first.
+ *  - Reference paths are relative to "MeMPhyS Latest Version/" of
+ *    aakashvshah/MemPhys.
+ */
+#ifndef MEMPHYS_H_
+#define MEMPHYS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MP_OK = 0,
+    MP_NOT_CONVERGED = 1,    /* solver.cpp:317-321 (HYPRE branch throws; Eigen branch only logs) */
+    MP_BREAKDOWN = 2,        /* BiCGSTAB rho or omega collapsed to zero */
+    MP_NAN_DETECTED = 3,     /* non-finite residual or input */
+    MP_SINGULAR_STENCIL = 4, /* zero pivot in a stencil system (duplicate nodes) */
+    MP_BAD_ARG = 5,          /* invalid size, flag or pointer */
+    MP_CUDA_ERROR = 6,       /* a CUDA runtime call failed */
+    MP_NO_DEVICE = 7,        /* no sm_100 device visible */
+    MP_TIMEOUT = 8,          /* a bounded device-side wait ran out */
+    MP_KNN_FAILED = 9        /* a node has fewer candidates than the stencil size */
+} mp_status;
+
+typedef void *mp_stream; /* a cudaStream_t; NULL is the legacy default stream */
+
+/* ---------------------------------------------------------------- runtime */
+int mp_last_error(char *buf, size_t len);
+int mp_version(void);
+int mp_device_info(int *sm_count, int *cc_major, int *cc_minor, size_t *total_mem);
+int mp_malloc(void **ptr, size_t bytes);
+int mp_free(void *ptr);
+int mp_malloc_host(void **ptr, size_t bytes); /* pinned */
+int mp_free_host(void *ptr);
+int mp_memcpy(void *dst, const void *src, size_t bytes, mp_stream s); /* any direction */
+int mp_memset(void *dst, int value, size_t bytes, mp_stream s);
+int mp_stream_create(mp_stream *s);
+int mp_stream_destroy(mp_stream s);
+int mp_stream_sync(mp_stream s);
+/* CUDA-event timer on a stream: mp_timer_start / mp_timer_stop -> milliseconds */
+int mp_timer_start(mp_stream s, void **timer);
+int mp_timer_stop(void *timer, mp_stream s, double *ms);
+/* launches of this library's kernels since the last reset (process-wide counter) */
+int mp_launch_count(int64_t *count, int reset);
+
+/* ------------------------------------------------------------- parameters */
+/* parameters.cpp:122-130 (PARAMETERS::calc_cloud_num_points) */
+int mp_num_poly_terms(int dim, int poly_deg);
+int mp_cloud_size(int dim, int poly_deg, double cloud_size_multiplier);
+/* parameters.cpp:217-267 (PARAMETERS::calc_polynomial_term_exponents); exps is m x dim */
+int mp_poly_exponents(int dim, int poly_deg, int *exps);
+
+/* ---------------------------------------------------------------- stencils */
+/*
+ * kNN stencils, replacing CLOUD::calc_cloud_points_fast (cloud.cpp:570-648):
+ * interior node -> its n nearest nodes (itself first); boundary node ->
+ * itself + its n-1 nearest interior nodes.  Ties by node index.
+ * xyz: nv x dim; boundary: nv flags; nb_col: nv x n (output).
+ */
+int mp_knn_stencils(const double *xyz, const uint8_t *boundary, int nv, int dim, int n,
+                    int *nb_col, mp_stream s);
+
+/*
+ * PHS-RBF-FD weights of every stencil of a cloud, replacing the loop of
+ * CLOUD::calc_grad_laplace_coeffs (cloud.cpp:207-279) over
+ * calc_PHS_RBF_grad_laplace_single_vert (coefficient_computations.cpp:294-328).
+ * nb_col: nv x n, row i = stencil of node i with node i first.
+ * gx, gy, gz (3D only, else NULL), lap: nv x n weights aligned with nb_col.
+ * cond (nullable): 1/rcond of each stencil matrix as Eigen's
+ *   PartialPivLU::rcond reports it (coefficient_computations.cpp:312).
+ * Returns MP_SINGULAR_STENCIL if any system had a zero pivot.
+ */
+int mp_stencil_weights(const double *xyz, int nv, int dim, const int *nb_col, int n,
+                       int phs_deg, int poly_deg, double *gx, double *gy, double *gz,
+                       double *lap, double *cond, mp_stream s);
+
+/*
+ * Independent stencil systems of uneven size in one persistent launch
+ * (the batched form of coefficient_computations.cpp:294-328, as the moving
+ * boundary path fractional_step_fsi.cpp:239-273 re-solves subsets).
+ * System i has sizes[i] nodes at pts[offsets[i] .. offsets[i]+sizes[i]) (each
+ * dim coordinates, node 0 = centre); its weights go to
+ * w[(dim+1)*offsets[i] ...] as (dim+1) rows of sizes[i].  cond nullable.
+ * sizes[i] + m must not exceed 96.
+ */
+int mp_stencil_weights_batched(int nsys, const int *sizes, const int64_t *offsets,
+                               const double *pts, int dim, int phs_deg, int poly_deg, double *w,
+                               double *cond, mp_stream s);
+
+/* ------------------------------------------------------------------ cloud */
+typedef struct mp_cloud_s *mp_cloud;
+
+/*
+ * CLOUD::CLOUD (cloud.cpp:29-48) without the RCM reordering: GPU kNN
+ * stencils + GPU weights, kept resident on the device.
+ * cloud_size_multiplier as in parameters_file.csv (n = ceil(mult * m)).
+ */
+int mp_cloud_create(const double *xyz, const uint8_t *boundary, int nv, int dim, int phs_deg,
+                    int poly_deg, double cloud_size_multiplier, int compute_cond, mp_stream s,
+                    mp_cloud *out);
+/* same with caller-provided stencils (nv x n) */
+int mp_cloud_create_stencils(const double *xyz, const uint8_t *boundary, int nv, int dim,
+                             const int *nb_col, int n, int phs_deg, int poly_deg,
+                             int compute_cond, mp_stream s, mp_cloud *out);
+int mp_cloud_info(mp_cloud c, int *nv, int *n, int *dim);
+/* copies out CLOUD::nb_points_col / grad_*_coeff / laplacian_coeff / cond_num_RBF
+ * (class.hpp:145-151); any pointer may be NULL */
+int mp_cloud_get(mp_cloud c, int *nb_col, double *gx, double *gy, double *gz, double *lap,
+                 double *cond, mp_stream s);
+int mp_cloud_destroy(mp_cloud c);
+
+/* -------------------------------------------------------------- operators */
+typedef struct mp_op_s *mp_op;
+
+enum { MP_FP64 = 0, MP_FP32 = 1 };
+enum { MP_GRAD_X = 0, MP_GRAD_Y = 1, MP_GRAD_Z = 2, MP_LAPLACIAN = 3 };
+enum { MP_ROWS_ALL = 0, MP_ROWS_INTERNAL = 1, MP_ROWS_BOUNDARY = 2 };
+
+/*
+ * Fixed-width (ELL) operator with nrows rows of exactly `width` entries,
+ * cols/vals row-major nrows x width; stored on the device in 64-row slices.
+ * Replaces the Eigen::SparseMatrix<double,RowMajor> operators of POINTS
+ * (class.hpp:116-124) for `matrix * vector` products.
+ */
+int mp_op_create_ell(int nrows, int ncols, int width, const int *cols, const double *vals,
+                     int precision, mp_op *out);
+/* POINTS::{grad_x,grad_y,grad_z,laplacian}_matrix_EIGEN[_internal|_boundary]
+ * (cloud.cpp:89-205): rows outside the mask are zero */
+int mp_op_from_cloud(mp_cloud c, int which, int rows, int precision, mp_op *out);
+/* y = alpha * A x + beta * y; x, y device (or host, staged) vectors of the op's precision */
+int mp_op_apply(mp_op op, const void *x, void *y, double alpha, double beta, mp_stream s);
+/* y_k = A_k x for up to 4 operators sharing one column structure (one pass over the indices) */
+int mp_op_apply_multi(int nops, const mp_op *ops, const void *x, void *const *ys, mp_stream s);
+int mp_op_info(mp_op op, int *nrows, int *ncols, int *width, int *precision);
+int mp_op_destroy(mp_op op);
+
+/* --------------------------------------------------------- pressure solve */
+typedef struct mp_ppe_s *mp_ppe;
+
+enum { MP_PRECOND_NONE = 0, MP_PRECOND_JACOBI = 1, MP_PRECOND_AMG = 2 };
+enum { MP_GUESS_PREVIOUS = 0, MP_GUESS_ZERO = 1, MP_GUESS_LEARNED = 2 };
+
+typedef struct {
+    double tol;        /* relative residual ||b - A x|| / ||b||, solver.cpp:154 */
+    int maxit;         /* solver.cpp:155 */
+    int precond;       /* MP_PRECOND_* */
+    int precision;     /* MP_FP64, or MP_FP32 = FP32 Krylov + FP64 iterative refinement */
+    int guess;         /* MP_GUESS_* */
+    double inner_tol;  /* mixed precision: relative reduction per refinement sweep */
+    int amg_max_levels;
+    int amg_coarse_size;
+    int smoother_sweeps;
+    double smoother_omega;
+} mp_solver_cfg;
+
+/* sensible defaults for the fields above */
+int mp_solver_cfg_default(mp_solver_cfg *cfg);
+
+/*
+ * SOLVER::init (solver.cpp:14-79) + calc_coeff_matrix (solver.cpp:165-214)
+ * for the operator  unsteady*I + conv*(Gx+Gy[+Gz]) + diff*L  on interior rows,
+ * identity on Dirichlet boundary rows and normal.grad on Neumann boundary
+ * rows; bordered with the nv+1 regularisation row/column when no boundary
+ * node is Dirichlet (solver.cpp:29-38, 205-213).
+ */
+int mp_ppe_create(mp_cloud c, const uint8_t *boundary, const uint8_t *dirichlet,
+                  const double *normal, double unsteady, double conv, double diff,
+                  const mp_solver_cfg *cfg, mp_ppe *out);
+int mp_ppe_system_size(mp_ppe p);
+/*
+ * SOLVER::general_solve (solver.cpp:283-363), eigen_ilu_bicgstab branch:
+ * x_inout holds the initial guess (field_old) and receives the solution.
+ * iters, relres (= ||A x - b|| / ||b|| recomputed in FP64), abs_res nullable.
+ * Returns MP_NOT_CONVERGED if relres > tol after maxit.
+ */
+int mp_ppe_solve(mp_ppe p, const double *rhs, double *x_inout, int *iters, double *relres,
+                 double *abs_res, mp_stream s);
+int mp_ppe_destroy(mp_ppe p);
+
+/* ------------------------------------------------------- fractional step */
+typedef struct mp_fs1_s *mp_fs1;
+
+typedef struct {
+    double rho, mu, dt;
+    int temporal_order; /* 1 = Euler, 2 = Adams-Bashforth 2 (Euler on the first step) */
+} mp_fs1_cfg;
+
+/*
+ * FRACTIONAL_STEP_1::FRACTIONAL_STEP_1 (fractional_step_1.cpp:22-50).
+ * w_dirichlet is ignored in 2D.  Keeps u, v, [w], p resident on the device.
+ */
+int mp_fs1_create(mp_cloud c, const uint8_t *boundary, const double *normal,
+                  const uint8_t *u_dirichlet, const uint8_t *v_dirichlet,
+                  const uint8_t *w_dirichlet, const uint8_t *p_dirichlet,
+                  const mp_fs1_cfg *cfg, const mp_solver_cfg *solver, mp_fs1 *out);
+int mp_fs1_system_size(mp_fs1 f);
+/* resident state: vel = dim arrays of nv; p = system_size entries */
+int mp_fs1_set_state(mp_fs1 f, const double *const *vel, const double *p, int it, mp_stream s);
+int mp_fs1_get_state(mp_fs1 f, double *const *vel, double *p, mp_stream s);
+/* advance the resident state nsteps timesteps (one CUDA graph launch per step
+ * when use_graph); the step counter continues from set_state's `it` */
+int mp_fs1_step(mp_fs1 f, int nsteps, int use_graph, mp_stream s);
+/*
+ * Drop-in for FRACTIONAL_STEP_1::single_timestep_2d (fractional_step_1.cpp:52-63):
+ * vel_old/p_old in, vel_new/p_new out (host or device arrays; p of system_size).
+ */
+int mp_fs1_single_timestep(mp_fs1 f, double *const *vel_new, double *p_new,
+                           const double *const *vel_old, const double *p_old, int it,
+                           mp_stream s);
+/* per-solve logs of the last step (class.hpp:83-84: rel_res_log, abs_res_log,
+ * n_iter_actual, regul_alpha_log) */
+int mp_fs1_last_stats(mp_fs1 f, int *iters, double *relres, double *abs_res, double *alpha);
+/* the same four logs for `count` steps starting at step `first` (4 doubles per step:
+ * iterations, relative residual, absolute residual, regularisation alpha); the
+ * device keeps the last 4096 steps */
+int mp_fs1_log(mp_fs1 f, int first, int count, double *out);
+int mp_fs1_destroy(mp_fs1 f);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MEMPHYS_H_ */

@@ -1,0 +1,634 @@
+// mp_amg.cu -- smoothed-aggregation multigrid: host setup, GPU V-cycle.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <unordered_map>
+#include "mp_amg.cuh"
+#include "mp_ppe.cuh"
+
+namespace mp {
+
+// ================================================================ host setup
+struct Csr {
+    int n = 0, m = 0;
+    std::vector<int> rp, ci;
+    std::vector<double> v;
+};
+
+static int csr_from_ell(const Ell &E, Csr &C) {
+    const int np = ell_padded_rows(E.nrows), K = E.K;
+    std::vector<int> cols((size_t)np * K);
+    std::vector<double> vals((size_t)np * K);
+    MP_CUDA(cudaMemcpy(cols.data(), E.cols.p, sizeof(int) * cols.size(), cudaMemcpyDeviceToHost));
+    MP_CUDA(cudaMemcpy(vals.data(), E.v64.p, sizeof(double) * vals.size(), cudaMemcpyDeviceToHost));
+    C.n = E.nrows;
+    C.m = E.nrows;
+    C.rp.assign(C.n + 1, 0);
+    C.ci.clear();
+    C.v.clear();
+    C.ci.reserve((size_t)C.n * K);
+    C.v.reserve((size_t)C.n * K);
+    for (int i = 0; i < C.n; i++) {
+        // merge duplicate columns (setFromTriplets semantics)
+        const size_t base = (size_t)(i / SLICE) * K * SLICE + (i % SLICE);
+        const int start = (int)C.ci.size();
+        for (int k = 0; k < K; k++) {
+            const int c = cols[base + (size_t)k * SLICE];
+            const double a = vals[base + (size_t)k * SLICE];
+            if (a == 0.0 && c != i)
+                continue;
+            if (c < 0 || c >= C.m)
+                return fail(MP_BAD_ARG, "operator column %d out of range in row %d", c, i);
+            bool merged = false;
+            for (int t = start; t < (int)C.ci.size(); t++)
+                if (C.ci[t] == c) {
+                    C.v[t] += a;
+                    merged = true;
+                    break;
+                }
+            if (!merged) {
+                C.ci.push_back(c);
+                C.v.push_back(a);
+            }
+        }
+        C.rp[i + 1] = (int)C.ci.size();
+    }
+    return MP_OK;
+}
+
+static std::vector<double> diag_of(const Csr &A) {
+    std::vector<double> d(A.n, 0.0);
+    for (int i = 0; i < A.n; i++)
+        for (int t = A.rp[i]; t < A.rp[i + 1]; t++)
+            if (A.ci[t] == i)
+                d[i] += A.v[t];
+    return d;
+}
+
+// largest |eigenvalue| of D^-1 A by power iteration (deterministic start)
+static double lmax_power(const Csr &A, const std::vector<double> &dinv, int iters) {
+    std::vector<double> x(A.n), y(A.n);
+    uint64_t s = 0x9E3779B97F4A7C15ull;
+    for (int i = 0; i < A.n; i++) {
+        s ^= s << 13;
+        s ^= s >> 7;
+        s ^= s << 17;
+        x[i] = 0.5 + (double)(s >> 11) / 9007199254740992.0;
+    }
+    double lam = 1.0;
+    for (int it = 0; it < iters; it++) {
+        double ny = 0.0, nx = 0.0;
+        for (int i = 0; i < A.n; i++) {
+            double a = 0.0;
+            for (int t = A.rp[i]; t < A.rp[i + 1]; t++)
+                a += A.v[t] * x[A.ci[t]];
+            y[i] = dinv[i] * a;
+            ny += y[i] * y[i];
+            nx += x[i] * x[i];
+        }
+        if (ny == 0.0)
+            return 1.0;
+        lam = std::sqrt(ny / nx);
+        const double inv = 1.0 / std::sqrt(ny);
+        for (int i = 0; i < A.n; i++)
+            x[i] = y[i] * inv;
+    }
+    return lam;
+}
+
+// greedy aggregation on the symmetrised strong graph; isolated rows
+// (Dirichlet identities) get no aggregate
+static int aggregate(const Csr &A, double theta, std::vector<int> &agg) {
+    const int n = A.n;
+    std::vector<std::vector<int>> S(n);
+    for (int i = 0; i < n; i++) {
+        double mx = 0.0;
+        for (int t = A.rp[i]; t < A.rp[i + 1]; t++)
+            if (A.ci[t] != i)
+                mx = std::max(mx, std::fabs(A.v[t]));
+        if (mx == 0.0)
+            continue;
+        for (int t = A.rp[i]; t < A.rp[i + 1]; t++) {
+            const int j = A.ci[t];
+            if (j != i && std::fabs(A.v[t]) >= theta * mx) {
+                S[i].push_back(j);
+                S[j].push_back(i);
+            }
+        }
+    }
+    for (auto &s : S) {
+        std::sort(s.begin(), s.end());
+        s.erase(std::unique(s.begin(), s.end()), s.end());
+    }
+    agg.assign(n, -1);
+    int na = 0;
+    for (int i = 0; i < n; i++) {  // pass 1: roots whose neighbourhood is free
+        if (agg[i] >= 0 || S[i].empty())
+            continue;
+        bool free_ = true;
+        for (int j : S[i])
+            if (agg[j] >= 0) {
+                free_ = false;
+                break;
+            }
+        if (!free_)
+            continue;
+        agg[i] = na;
+        for (int j : S[i])
+            agg[j] = na;
+        na++;
+    }
+    std::vector<int> pass1 = agg;
+    for (int i = 0; i < n; i++) {  // pass 2: join a neighbouring pass-1 aggregate
+        if (agg[i] >= 0 || S[i].empty())
+            continue;
+        for (int j : S[i])
+            if (pass1[j] >= 0) {
+                agg[i] = pass1[j];
+                break;
+            }
+    }
+    for (int i = 0; i < n; i++) {  // pass 3: leftovers form new aggregates
+        if (agg[i] >= 0 || S[i].empty())
+            continue;
+        agg[i] = na;
+        for (int j : S[i])
+            if (agg[j] < 0)
+                agg[j] = na;
+        na++;
+    }
+    return na;
+}
+
+// C = A * B (Gustavson)
+static void spgemm(const Csr &A, const Csr &B, Csr &C) {
+    C.n = A.n;
+    C.m = B.m;
+    C.rp.assign(A.n + 1, 0);
+    C.ci.clear();
+    C.v.clear();
+    std::vector<int> mark(B.m, -1);
+    std::vector<double> acc(B.m, 0.0);
+    std::vector<int> cols;
+    for (int i = 0; i < A.n; i++) {
+        cols.clear();
+        for (int t = A.rp[i]; t < A.rp[i + 1]; t++) {
+            const int k = A.ci[t];
+            const double a = A.v[t];
+            for (int u = B.rp[k]; u < B.rp[k + 1]; u++) {
+                const int j = B.ci[u];
+                if (mark[j] != i) {
+                    mark[j] = i;
+                    acc[j] = 0.0;
+                    cols.push_back(j);
+                }
+                acc[j] += a * B.v[u];
+            }
+        }
+        std::sort(cols.begin(), cols.end());
+        for (int j : cols) {
+            C.ci.push_back(j);
+            C.v.push_back(acc[j]);
+        }
+        C.rp[i + 1] = (int)C.ci.size();
+    }
+}
+
+static void transpose(const Csr &A, Csr &T) {
+    T.n = A.m;
+    T.m = A.n;
+    T.rp.assign(T.n + 1, 0);
+    for (int c : A.ci)
+        T.rp[c + 1]++;
+    for (int i = 0; i < T.n; i++)
+        T.rp[i + 1] += T.rp[i];
+    T.ci.resize(A.ci.size());
+    T.v.resize(A.v.size());
+    std::vector<int> pos(T.rp.begin(), T.rp.end() - 1);
+    for (int i = 0; i < A.n; i++)
+        for (int t = A.rp[i]; t < A.rp[i + 1]; t++) {
+            const int p = pos[A.ci[t]]++;
+            T.ci[p] = i;
+            T.v[p] = A.v[t];
+        }
+}
+
+// CSR -> ELL slices on the device; padded entries: column `self ? row : 0`, value 0
+static int upload_ell(const Csr &C, Ell &E, bool self_pad, cudaStream_t s) {
+    int K = 1;
+    for (int i = 0; i < C.n; i++)
+        K = std::max(K, C.rp[i + 1] - C.rp[i]);
+    const int np = ell_padded_rows(C.n);
+    std::vector<int> cols((size_t)np * K);
+    std::vector<double> vals((size_t)np * K, 0.0);
+    for (int i = 0; i < np; i++) {
+        const int len = i < C.n ? C.rp[i + 1] - C.rp[i] : 0;
+        for (int k = 0; k < K; k++) {
+            const size_t o = ell_index(i, k, K);
+            if (k < len) {
+                cols[o] = C.ci[C.rp[i] + k];
+                vals[o] = C.v[C.rp[i] + k];
+            } else {
+                cols[o] = (self_pad && i < C.n && i < C.m) ? i : 0;
+            }
+        }
+    }
+    E.nrows = C.n;
+    E.ncols = C.m;
+    E.K = K;
+    MP_TRY(E.cols.alloc(cols.size()));
+    MP_TRY(E.v64.alloc(vals.size()));
+    MP_CUDA(cudaMemcpyAsync(E.cols.p, cols.data(), sizeof(int) * cols.size(), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaMemcpyAsync(E.v64.p, vals.data(), sizeof(double) * vals.size(), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    return MP_OK;
+}
+
+// bordered dense inverse of the coarsest operator (LU with partial pivoting)
+static int coarse_inverse(const Csr &A, std::vector<double> &inv) {
+    const int n = A.n, m = n + 1;
+    std::vector<double> M((size_t)m * m, 0.0);
+    for (int i = 0; i < n; i++)
+        for (int t = A.rp[i]; t < A.rp[i + 1]; t++)
+            M[(size_t)i * m + A.ci[t]] += A.v[t];
+    for (int i = 0; i < n; i++) {
+        M[(size_t)i * m + n] = 1.0;
+        M[(size_t)n * m + i] = 1.0;
+    }
+    inv.assign((size_t)m * m, 0.0);
+    for (int i = 0; i < m; i++)
+        inv[(size_t)i * m + i] = 1.0;
+    for (int k = 0; k < m; k++) {
+        int p = k;
+        for (int i = k + 1; i < m; i++)
+            if (std::fabs(M[(size_t)i * m + k]) > std::fabs(M[(size_t)p * m + k]))
+                p = i;
+        if (M[(size_t)p * m + k] == 0.0)
+            return fail(MP_BREAKDOWN, "multigrid coarse operator is singular");
+        if (p != k)
+            for (int j = 0; j < m; j++) {
+                std::swap(M[(size_t)k * m + j], M[(size_t)p * m + j]);
+                std::swap(inv[(size_t)k * m + j], inv[(size_t)p * m + j]);
+            }
+        const double d = 1.0 / M[(size_t)k * m + k];
+        for (int j = 0; j < m; j++) {
+            M[(size_t)k * m + j] *= d;
+            inv[(size_t)k * m + j] *= d;
+        }
+        for (int i = 0; i < m; i++) {
+            if (i == k)
+                continue;
+            const double f = M[(size_t)i * m + k];
+            if (f == 0.0)
+                continue;
+            for (int j = 0; j < m; j++) {
+                M[(size_t)i * m + j] -= f * M[(size_t)k * m + j];
+                inv[(size_t)i * m + j] -= f * inv[(size_t)k * m + j];
+            }
+        }
+    }
+    return MP_OK;
+}
+
+__global__ void k_to_f32(const double *a, float *b, size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        b[i] = (float)a[i];
+}
+
+static int make_f32(const dbuf<double> &a, dbuf<float> &b, cudaStream_t s) {
+    MP_TRY(b.alloc(a.n));
+    k_to_f32<<<(unsigned)((a.n + 255) / 256), 256, 0, s>>>(a.p, b.p, a.n);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+Amg::~Amg() {
+    for (auto *l : L)
+        delete l;
+}
+
+int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, bool mixed, cudaStream_t s) {
+    auto t0 = std::chrono::steady_clock::now();
+    const double theta = 0.25;
+    Amg *a = new Amg;
+    Csr A;
+    int rc = csr_from_ell(A0, A);
+    if (rc != MP_OK) {
+        delete a;
+        return rc;
+    }
+    auto bail = [&](int r) {
+        delete a;
+        return r;
+    };
+    for (int lev = 0;; lev++) {
+        AmgLevel *L = new AmgLevel;
+        a->L.push_back(L);
+        L->n = A.n;
+        std::vector<double> d = diag_of(A);
+        std::vector<double> dinv(A.n);
+        for (int i = 0; i < A.n; i++)
+            dinv[i] = (d[i] != 0.0 && std::isfinite(d[i])) ? 1.0 / d[i] : 0.0;
+        if (lev == 0) {
+            L->borrowed = true;
+            L->A64 = A0.view64();
+            L->A32 = A0.view32();
+        } else {
+            if ((rc = upload_ell(A, L->A, true, s)) != MP_OK)
+                return bail(rc);
+            L->A64 = L->A.view64();
+        }
+        if ((rc = L->dinv.alloc(A.n)) != MP_OK)
+            return bail(rc);
+        MP_CUDA(cudaMemcpy(L->dinv.p, dinv.data(), sizeof(double) * A.n, cudaMemcpyHostToDevice));
+        const bool coarsest = A.n <= cfg.amg_coarse_size || lev + 1 >= cfg.amg_max_levels;
+        if (!coarsest) {
+            std::vector<int> agg;
+            const int na = aggregate(A, theta, agg);
+            if (na == 0 || na >= A.n) {
+                // cannot coarsen further: this level becomes the coarsest
+            } else {
+                L->lmax = 1.1 * lmax_power(A, dinv, 30);
+                const double w = 4.0 / (3.0 * (L->lmax / 1.1));
+                // AT = A * T, then P = T - w D^-1 AT
+                Csr T;
+                T.n = A.n;
+                T.m = na;
+                T.rp.assign(A.n + 1, 0);
+                for (int i = 0; i < A.n; i++) {
+                    if (agg[i] >= 0) {
+                        T.ci.push_back(agg[i]);
+                        T.v.push_back(1.0);
+                    }
+                    T.rp[i + 1] = (int)T.ci.size();
+                }
+                Csr AT, P, R, AP, Ac;
+                spgemm(A, T, AT);
+                P.n = A.n;
+                P.m = na;
+                P.rp.assign(A.n + 1, 0);
+                for (int i = 0; i < A.n; i++) {
+                    const int ti = agg[i];
+                    bool diag_done = false;
+                    for (int t = AT.rp[i]; t < AT.rp[i + 1]; t++) {
+                        double v = -w * dinv[i] * AT.v[t];
+                        if (AT.ci[t] == ti) {
+                            v += 1.0;
+                            diag_done = true;
+                        }
+                        if (v != 0.0) {
+                            P.ci.push_back(AT.ci[t]);
+                            P.v.push_back(v);
+                        }
+                    }
+                    if (ti >= 0 && !diag_done) {
+                        P.ci.push_back(ti);
+                        P.v.push_back(1.0);
+                    }
+                    P.rp[i + 1] = (int)P.ci.size();
+                }
+                transpose(P, R);
+                spgemm(A, P, AP);
+                spgemm(R, AP, Ac);
+                if ((rc = upload_ell(P, L->P, false, s)) != MP_OK ||
+                    (rc = upload_ell(R, L->R, false, s)) != MP_OK)
+                    return bail(rc);
+                if (lev > 0) {
+                    if ((rc = L->b.alloc(A.n)) != MP_OK || (rc = L->x.alloc(A.n)) != MP_OK)
+                        return bail(rc);
+                }
+                if ((rc = L->d.alloc(A.n)) != MP_OK || (rc = L->r.alloc(A.n)) != MP_OK)
+                    return bail(rc);
+                A = std::move(Ac);
+                continue;
+            }
+        }
+        // coarsest level: bordered dense inverse
+        std::vector<double> inv;
+        if ((rc = coarse_inverse(A, inv)) != MP_OK)
+            return bail(rc);
+        a->nc = A.n;
+        if ((rc = a->cinv.alloc(inv.size())) != MP_OK)
+            return bail(rc);
+        MP_CUDA(cudaMemcpy(a->cinv.p, inv.data(), sizeof(double) * inv.size(), cudaMemcpyHostToDevice));
+        if (lev > 0) {
+            if ((rc = L->b.alloc(A.n)) != MP_OK || (rc = L->x.alloc(A.n)) != MP_OK)
+                return bail(rc);
+        }
+        break;
+    }
+    if (mixed) {
+        for (size_t l = 0; l < a->L.size(); l++) {
+            AmgLevel *L = a->L[l];
+            if (!L->borrowed && L->A.v64.p) {
+                if ((rc = ell_make_fp32(L->A, s)) != MP_OK)
+                    return bail(rc);
+                L->A32 = L->A.view32();
+            }
+            if (L->P.v64.p && ((rc = ell_make_fp32(L->P, s)) != MP_OK || (rc = ell_make_fp32(L->R, s)) != MP_OK))
+                return bail(rc);
+            if ((rc = make_f32(L->dinv, L->dinv32, s)) != MP_OK)
+                return bail(rc);
+            for (auto pr : {std::make_pair(&L->b, &L->b32), std::make_pair(&L->x, &L->x32),
+                            std::make_pair(&L->d, &L->d32), std::make_pair(&L->r, &L->r32)})
+                if (pr.first->p && (rc = pr.second->alloc(pr.first->n)) != MP_OK)
+                    return bail(rc);
+        }
+        if ((rc = make_f32(a->cinv, a->cinv32, s)) != MP_OK)
+            return bail(rc);
+    }
+    MP_CUDA(cudaStreamSynchronize(s));
+    a->setup_seconds =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = a;
+    return MP_OK;
+}
+
+void amg_destroy(Amg *a) { delete a; }
+
+// ================================================================ GPU cycle
+template <class T> struct V2a;
+template <> struct V2a<double> { using type = double2; };
+template <> struct V2a<float> { using type = float2; };
+
+template <class T>
+__device__ __forceinline__ void spmv_pair(const EllView<T> &A, int w, int lane,
+                                          const T *__restrict__ x, T &a0, T &a1) {
+    using V2 = typename V2a<T>::type;
+    const size_t base = (size_t)w * A.K * SLICE + 2 * lane;
+    a0 = 0;
+    a1 = 0;
+#pragma unroll 4
+    for (int k = 0; k < A.K; k++) {
+        const size_t o = base + (size_t)k * SLICE;
+        const int2 c = __ldcs(reinterpret_cast<const int2 *>(A.cols + o));
+        const V2 v = __ldcs(reinterpret_cast<const V2 *>(A.vals + o));
+        a0 = fma(v.x, __ldg(x + c.x), a0);
+        a1 = fma(v.y, __ldg(x + c.y), a1);
+    }
+}
+
+__device__ __forceinline__ int gwarp_a() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+
+// Epilogue kinds of the fused level kernels
+enum { EP_CHEB_PRE = 0, EP_RESID, EP_PLAIN, EP_PROLONG, EP_CHEB_POST1, EP_CHEB_POST2 };
+
+struct ChebC {
+    double inv_theta, theta, c1, c2, c3, c4;
+};
+
+// One fused SpMV + epilogue over the rows of M (warp per slice, 2 rows/lane):
+//   EP_CHEB_PRE  : x = c1 d + c2 dinv (b - M d)            (u = d)
+//   EP_RESID     : r = b - M x                              (u = x)
+//   EP_PLAIN     : y = M u
+//   EP_PROLONG   : x = x + M u                              (M = P, u = coarse x)
+//   EP_CHEB_POST1: d = dinv (b - M x) / theta               (u = x)
+//   EP_CHEB_POST2: x = x + (1 + c3) d + c4 (theta d - dinv M d)   (u = d)
+// No kernel writes the vector it gathers.
+template <class T, int EP>
+__global__ void __launch_bounds__(256)
+    k_level(EllView<T> M, const T *__restrict__ u, const T *__restrict__ b,
+            const T *__restrict__ dinv, T *d, T *x, T *y, ChebC c, const int *done) {
+    if (*done)
+        return;
+    const int w = gwarp_a(), lane = threadIdx.x & 31;
+    if (w >= (M.nrows + SLICE - 1) / SLICE)
+        return;
+    T a[2];
+    spmv_pair(M, w, lane, u, a[0], a[1]);
+    const int i0 = w * SLICE + 2 * lane;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int i = i0 + q;
+        if (i >= M.nrows)
+            continue;
+        if (EP == EP_CHEB_PRE) {
+            x[i] = (T)c.c1 * d[i] + (T)c.c2 * dinv[i] * (b[i] - a[q]);
+        } else if (EP == EP_RESID) {
+            y[i] = b[i] - a[q];
+        } else if (EP == EP_PLAIN) {
+            y[i] = a[q];
+        } else if (EP == EP_PROLONG) {
+            x[i] = x[i] + a[q];
+        } else if (EP == EP_CHEB_POST1) {
+            d[i] = dinv[i] * (b[i] - a[q]) * (T)c.inv_theta;
+        } else {
+            const T di = d[i];
+            x[i] = x[i] + (T)(1.0 + c.c3) * di + (T)c.c4 * ((T)c.theta * di - dinv[i] * a[q]);
+        }
+    }
+}
+
+// d = dinv b / theta (start of the pre-smoother from a zero guess)
+template <class T>
+__global__ void k_cheb_start(int n, const T *b, const T *dinv, T *d, T inv_theta, const int *done) {
+    if (*done)
+        return;
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        d[i] = dinv[i] * b[i] * inv_theta;
+}
+
+// coarsest level: x = first nc entries of Cinv [b; 0] (one warp per row)
+template <class T>
+__global__ void k_coarse(int nc, const T *__restrict__ cinv, const T *__restrict__ b, T *x,
+                         const int *done) {
+    if (*done)
+        return;
+    const int row = gwarp_a(), lane = threadIdx.x & 31;
+    if (row >= nc)
+        return;
+    const T *ci = cinv + (size_t)row * (nc + 1);
+    T acc = 0;
+    for (int j = lane; j < nc; j += 32)
+        acc = fma(ci[j], b[j], acc);
+    acc = warp_sum(acc);
+    if (lane == 0)
+        x[row] = acc;
+}
+
+static ChebC cheb_consts(double lmax) {
+    const double lmin = lmax / 6.0;
+    const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+    const double sigma = theta / delta, rho0 = 1.0 / sigma, rho1 = 1.0 / (2.0 * sigma - rho0);
+    ChebC c;
+    c.theta = theta;
+    c.inv_theta = 1.0 / theta;
+    c.c1 = 1.0 + rho1 * rho0;
+    c.c2 = 2.0 * rho1 / delta;
+    c.c3 = rho1 * rho0;
+    c.c4 = 2.0 * rho1 / delta;
+    return c;
+}
+
+template <class T> struct LvlPtr;
+template <> struct LvlPtr<double> {
+    static EllView<double> A(const AmgLevel &L) { return L.A64; }
+    static EllView<double> P(const AmgLevel &L) { return L.P.view64(); }
+    static EllView<double> R(const AmgLevel &L) { return L.R.view64(); }
+    static const double *dinv(const AmgLevel &L) { return L.dinv.p; }
+    static double *b(AmgLevel &L) { return L.b.p; }
+    static double *x(AmgLevel &L) { return L.x.p; }
+    static double *d(AmgLevel &L) { return L.d.p; }
+    static double *r(AmgLevel &L) { return L.r.p; }
+    static const double *cinv(const Amg &a) { return a.cinv.p; }
+};
+template <> struct LvlPtr<float> {
+    static EllView<float> A(const AmgLevel &L) { return L.A32; }
+    static EllView<float> P(const AmgLevel &L) { return L.P.view32(); }
+    static EllView<float> R(const AmgLevel &L) { return L.R.view32(); }
+    static const float *dinv(const AmgLevel &L) { return L.dinv32.p; }
+    static float *b(AmgLevel &L) { return L.b32.p; }
+    static float *x(AmgLevel &L) { return L.x32.p; }
+    static float *d(AmgLevel &L) { return L.d32.p; }
+    static float *r(AmgLevel &L) { return L.r32.p; }
+    static const float *cinv(const Amg &a) { return a.cinv32.p; }
+};
+
+static unsigned sblocks(int n) { return (unsigned)(((n + SLICE - 1) / SLICE + 7) / 8); }
+
+template <class T>
+static int vcycle(const Amg &a, size_t l, const T *b, T *x, const int *done, cudaStream_t s) {
+    using LP = LvlPtr<T>;
+    AmgLevel &L = *a.L[l];
+    if (l + 1 == a.L.size()) {
+        k_coarse<T><<<(unsigned)((a.nc + 7) / 8), 256, 0, s>>>(a.nc, LP::cinv(a), b, x, done);
+        MP_CHECK_LAUNCH();
+        return MP_OK;
+    }
+    AmgLevel &N = *a.L[l + 1];
+    const ChebC c = cheb_consts(L.lmax);
+    const EllView<T> A = LP::A(L);
+    const T *dinv = LP::dinv(L);
+    T *d = LP::d(L), *r = LP::r(L);
+    const unsigned nb = sblocks(L.n);
+    const unsigned vb = (unsigned)std::min((L.n + 255) / 256, sm_count() * 8);
+    k_cheb_start<T><<<vb, 256, 0, s>>>(L.n, b, dinv, d, (T)c.inv_theta, done);
+    MP_CHECK_LAUNCH();
+    k_level<T, EP_CHEB_PRE><<<nb, 256, 0, s>>>(A, d, b, dinv, d, x, nullptr, c, done);
+    MP_CHECK_LAUNCH();
+    k_level<T, EP_RESID><<<nb, 256, 0, s>>>(A, x, b, dinv, d, x, r, c, done);
+    MP_CHECK_LAUNCH();
+    k_level<T, EP_PLAIN><<<sblocks(N.n), 256, 0, s>>>(LP::R(L), r, nullptr, nullptr, nullptr,
+                                                      nullptr, LP::b(N), c, done);
+    MP_CHECK_LAUNCH();
+    MP_TRY(vcycle<T>(a, l + 1, LP::b(N), LP::x(N), done, s));
+    k_level<T, EP_PROLONG><<<nb, 256, 0, s>>>(LP::P(L), LP::x(N), nullptr, nullptr, nullptr, x,
+                                              nullptr, c, done);
+    MP_CHECK_LAUNCH();
+    k_level<T, EP_CHEB_POST1><<<nb, 256, 0, s>>>(A, x, b, dinv, d, x, nullptr, c, done);
+    MP_CHECK_LAUNCH();
+    k_level<T, EP_CHEB_POST2><<<nb, 256, 0, s>>>(A, d, b, dinv, d, x, nullptr, c, done);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+template <class T>
+int amg_apply(const Amg &a, const T *in, T *out, const int *done, cudaStream_t s) {
+    return vcycle<T>(a, 0, in, out, done, s);
+}
+template int amg_apply<double>(const Amg &, const double *, double *, const int *, cudaStream_t);
+template int amg_apply<float>(const Amg &, const float *, float *, const int *, cudaStream_t);
+
+}  // namespace mp

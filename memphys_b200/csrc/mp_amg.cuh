@@ -1,0 +1,56 @@
+// mp_amg.cuh -- smoothed-aggregation multigrid preconditioner for the
+// pressure-Poisson stencil operator.
+//
+// The reference has no working multigrid (multigrid.cpp builds per-level
+// clouds and an SOR smoother, without transfers or a cycle), so this is a
+// new design for the BiCGSTAB preconditioner:
+//   setup (host, once per operator): strength of connection |a_ij| >=
+//     theta * max_k |a_ik| (symmetrised), greedy aggregation, tentative
+//     piecewise-constant prolongator T, smoothed P = (I - w D^-1 A) T with
+//     w = 4 / (3 lambda_max(D^-1 A)), R = P^T, Galerkin A_c = R A P, until
+//     the coarse size is small; the coarsest operator (singular for pure
+//     Neumann problems) is bordered like solver.cpp:205-213 and inverted.
+//   apply (GPU, every preconditioner call): V(1,1) cycle with degree-2
+//     Chebyshev smoothing on [lambda_max / 6, lambda_max] of D^-1 A; the
+//     RBF-FD Laplacian's Jacobi-scaled spectrum reaches ~2.85, where damped
+//     Jacobi is unstable or weak.
+// All level operators are ELL (64-row slices) padded to the level's widest row.
+#pragma once
+#include "mp_ell.cuh"
+
+namespace mp {
+
+struct Cfg;
+
+struct AmgLevel {
+    int n = 0;
+    Ell A;                   // level operator (level 0 borrows the PPE operator)
+    bool borrowed = false;
+    EllView<double> A64;
+    EllView<float> A32;
+    Ell P, R;                // prolongation (n x n_next), restriction (n_next x n)
+    dbuf<double> dinv;
+    dbuf<float> dinv32;
+    double lmax = 2.0;
+    // work vectors (b, x, d, r) per precision
+    dbuf<double> b, x, d, r;
+    dbuf<float> b32, x32, d32, r32;
+};
+
+struct Amg {
+    std::vector<AmgLevel *> L;
+    int nc = 0;                       // coarsest size
+    dbuf<double> cinv;                // (nc+1)^2 bordered inverse, row-major
+    dbuf<float> cinv32;
+    double setup_seconds = 0;
+    ~Amg();
+};
+
+int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, bool mixed, cudaStream_t s);
+void amg_destroy(Amg *a);
+// out = V-cycle(in) on the first n0 entries (the border entry is handled by
+// the caller); kernels return immediately while *done is set
+template <class T>
+int amg_apply(const Amg &a, const T *in, T *out, const int *done, cudaStream_t s);
+
+}  // namespace mp

@@ -1,0 +1,64 @@
+// mp_ell.cuh -- fixed-width sparse operators in 64-row slices.
+//
+// Every MeMPhyS operator row has exactly n entries (its stencil, cloud.cpp:627,644),
+// so the natural layout is ELL with width K = n.  Rows are grouped in slices of
+// 64; inside a slice entry k of all 64 rows is contiguous:
+//     idx(row, k) = (row / 64) * K * 64 + k * 64 + (row % 64)
+// One warp owns a slice and each lane two adjacent rows, so every load is a
+// 16-byte (FP64 pair) or 8-byte (FP32 pair / int pair) vector and a warp reads
+// 512 contiguous bytes of values and 256 of indices per stencil entry.  Padded
+// rows point at column 0 with value 0.
+#pragma once
+#include <memory>
+#include "mp_common.cuh"
+
+namespace mp {
+
+constexpr int SLICE = 64;
+
+__host__ __device__ inline size_t ell_index(int row, int k, int K) {
+    return (size_t)(row / SLICE) * K * SLICE + (size_t)k * SLICE + (row % SLICE);
+}
+
+__host__ __device__ inline int ell_padded_rows(int nrows) { return (nrows + SLICE - 1) / SLICE * SLICE; }
+
+// Device ELL matrix (non-owning view)
+template <class T> struct EllView {
+    int nrows, ncols, K;
+    const int *cols;
+    const T *vals;
+};
+
+// Owning ELL storage
+struct Ell {
+    int nrows = 0, ncols = 0, K = 0;
+    dbuf<int> cols;
+    dbuf<double> v64;
+    dbuf<float> v32;
+    EllView<double> view64() const { return {nrows, ncols, K, cols.p, v64.p}; }
+    EllView<float> view32() const { return {nrows, ncols, K, cols.p, v32.p}; }
+};
+
+// Build an Ell from row-major host or device arrays (copied).
+int ell_create(Ell &E, int nrows, int ncols, int K, const int *cols, const double *vals,
+               bool fp32, cudaStream_t s);
+// Convert existing FP64 values to an FP32 copy on the device.
+int ell_make_fp32(Ell &E, cudaStream_t s);
+
+// up to 4 value arrays sharing one column structure (mp_op_apply_multi)
+template <class T> struct MultiVals {
+    const T *v[4];
+};
+template <class T> struct MultiOut {
+    T *y[4];
+};
+
+// y = alpha * A x + beta * y
+template <class T>
+int ell_spmv(const EllView<T> &A, const T *x, T *y, double alpha, double beta, cudaStream_t s);
+
+template <class T>
+int ell_spmv_multi(int nops, int nrows, int K, const int *cols, const MultiVals<T> &V, const T *x,
+                   const MultiOut<T> &Y, cudaStream_t s);
+
+}  // namespace mp

@@ -1,0 +1,568 @@
+// mp_fs1.cu -- FRACTIONAL_STEP_1 (fractional_step_1.cpp) resident on the GPU.
+//
+// One timestep (single_timestep_2d, :52-63):
+//   calc_vel_hat  (:120-134)  src = rho(-u Gx q - v Gy q [- w Gz q]) + mu L q,
+//                             q_hat = q + dt/rho (src | 1.5 src - 0.5 src_prev)
+//   calc_pressure (:136-151)  b = (Gx_int u_hat + Gy_int v_hat [+ Gz w_hat]) rho/dt,
+//                             boundary rows p_old (Dirichlet) or
+//                             -rho ((q_old - q_hat) . n)/dt (Neumann), b[nv] = 0,
+//                             then the pressure solve with p_old as initial guess
+//   calc_vel_corr (:153-209)  q_new = q_hat - dt G p / rho; boundary rows without
+//                             Dirichlet pressure: q_new = q_old (Dirichlet) or
+//                             the normal-derivative row solved for q_new[i]
+//   extras        (:211-222)  src_prev = src (Adams-Bashforth 2)
+// The reference integrates 2D only; the 3D path adds the w component with the
+// same steps.  Each kernel streams the stencil indices once for all the
+// operators it applies.  With graphs enabled the whole step (including the
+// solver's device-controlled while loop) is a single graph launch.
+#include "mp_cloud.cuh"
+#include "mp_ppe.cuh"
+
+namespace mp {
+
+struct Fs1Const {
+    double rho, mu, dt;
+    int order, nv, K, bordered;
+};
+
+struct Vec3 {
+    const double *q[3];
+};
+struct Vec3w {
+    double *q[3];
+};
+
+__device__ __forceinline__ int fgwarp() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+
+template <int DIM>
+__global__ void __launch_bounds__(256)
+    k_vel_hat(const int *__restrict__ cols, const double *__restrict__ g0,
+              const double *__restrict__ g1, const double *__restrict__ g2,
+              const double *__restrict__ lap, Vec3 vel, Vec3w hat, Vec3w hist, Fs1Const c,
+              const int *step) {
+    const int w = fgwarp(), lane = threadIdx.x & 31, K = c.K;
+    if (w >= (c.nv + SLICE - 1) / SLICE)
+        return;
+    const size_t base = (size_t)w * K * SLICE + 2 * lane;
+    // acc[op][component][row]: op 0..DIM-1 gradients, DIM Laplacian
+    double acc[DIM + 1][DIM][2];
+#pragma unroll
+    for (int o = 0; o <= DIM; o++)
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+            acc[o][d][0] = acc[o][d][1] = 0.0;
+    const double *G[3] = {g0, g1, g2};
+#pragma unroll 2
+    for (int k = 0; k < K; k++) {
+        const size_t o = base + (size_t)k * SLICE;
+        const int2 cc = __ldcs(reinterpret_cast<const int2 *>(cols + o));
+        double q0[DIM], q1[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            q0[d] = __ldg(vel.q[d] + cc.x);
+            q1[d] = __ldg(vel.q[d] + cc.y);
+        }
+#pragma unroll
+        for (int op = 0; op <= DIM; op++) {
+            const double2 wv = __ldcs(reinterpret_cast<const double2 *>((op < DIM ? G[op] : lap) + o));
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+                acc[op][d][0] = fma(wv.x, q0[d], acc[op][d][0]);
+                acc[op][d][1] = fma(wv.y, q1[d], acc[op][d][1]);
+            }
+        }
+    }
+    const bool euler = c.order == 1 || *step == 0;
+    const double dtr = c.dt / c.rho;
+    const int i0 = w * SLICE + 2 * lane;
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int i = i0 + r;
+        if (i >= c.nv)
+            continue;
+        double qi[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+            qi[d] = vel.q[d][i];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            double conv = -(qi[0] * acc[0][d][r]);
+#pragma unroll
+            for (int e = 1; e < DIM; e++)
+                conv = conv - qi[e] * acc[e][d][r];
+            const double src = c.rho * conv + c.mu * acc[DIM][d][r];
+            double h;
+            if (euler)
+                h = qi[d] + dtr * src;
+            else
+                h = qi[d] + dtr * (1.5 * src - 0.5 * hist.q[d][i]);
+            hat.q[d][i] = h;
+            if (c.order == 2)
+                hist.q[d][i] = src;
+        }
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256)
+    k_p_rhs(const int *__restrict__ cols, const double *__restrict__ g0,
+            const double *__restrict__ g1, const double *__restrict__ g2, Vec3 hat, Vec3 vel,
+            const uint8_t *__restrict__ bflag, const uint8_t *__restrict__ pdir,
+            const double *__restrict__ normal, const double *p, double *b, Fs1Const c) {
+    const int w = fgwarp(), lane = threadIdx.x & 31, K = c.K;
+    if (w == 0 && lane == 0 && c.bordered)
+        b[c.nv] = 0.0;
+    if (w >= (c.nv + SLICE - 1) / SLICE)
+        return;
+    const size_t base = (size_t)w * K * SLICE + 2 * lane;
+    const double *G[3] = {g0, g1, g2};
+    double acc[DIM][2];
+#pragma unroll
+    for (int d = 0; d < DIM; d++)
+        acc[d][0] = acc[d][1] = 0.0;
+#pragma unroll 2
+    for (int k = 0; k < K; k++) {
+        const size_t o = base + (size_t)k * SLICE;
+        const int2 cc = __ldcs(reinterpret_cast<const int2 *>(cols + o));
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            const double2 wv = __ldcs(reinterpret_cast<const double2 *>(G[d] + o));
+            acc[d][0] = fma(wv.x, __ldg(hat.q[d] + cc.x), acc[d][0]);
+            acc[d][1] = fma(wv.y, __ldg(hat.q[d] + cc.y), acc[d][1]);
+        }
+    }
+    const int i0 = w * SLICE + 2 * lane;
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int i = i0 + r;
+        if (i >= c.nv)
+            continue;
+        double v;
+        if (!bflag[i]) {
+            double s = acc[0][r];
+#pragma unroll
+            for (int d = 1; d < DIM; d++)
+                s = s + acc[d][r];
+            v = s * c.rho / c.dt;
+        } else if (pdir[i]) {
+            v = p[i];
+        } else {
+            double s = (vel.q[0][i] - hat.q[0][i]) * normal[(size_t)DIM * i];
+#pragma unroll
+            for (int d = 1; d < DIM; d++)
+                s = s + (vel.q[d][i] - hat.q[d][i]) * normal[(size_t)DIM * i + d];
+            v = -c.rho * s / c.dt;
+        }
+        b[i] = v;
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256)
+    k_vel_corr(const int *__restrict__ cols, const double *__restrict__ g0,
+               const double *__restrict__ g1, const double *__restrict__ g2, Vec3 hat, Vec3 vel_old,
+               Vec3w vel_new, const double *__restrict__ p, const uint8_t *__restrict__ bflag,
+               const uint8_t *__restrict__ pdir, const uint8_t *__restrict__ d0,
+               const uint8_t *__restrict__ d1, const uint8_t *__restrict__ d2, Fs1Const c) {
+    const int w = fgwarp(), lane = threadIdx.x & 31, K = c.K;
+    if (w >= (c.nv + SLICE - 1) / SLICE)
+        return;
+    const size_t base = (size_t)w * K * SLICE + 2 * lane;
+    const double *G[3] = {g0, g1, g2};
+    const uint8_t *vd[3] = {d0, d1, d2};
+    double acc[DIM][2];
+#pragma unroll
+    for (int d = 0; d < DIM; d++)
+        acc[d][0] = acc[d][1] = 0.0;
+#pragma unroll 2
+    for (int k = 0; k < K; k++) {
+        const size_t o = base + (size_t)k * SLICE;
+        const int2 cc = __ldcs(reinterpret_cast<const int2 *>(cols + o));
+        const double p0 = __ldg(p + cc.x), p1 = __ldg(p + cc.y);
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            const double2 wv = __ldcs(reinterpret_cast<const double2 *>(G[d] + o));
+            acc[d][0] = fma(wv.x, p0, acc[d][0]);
+            acc[d][1] = fma(wv.y, p1, acc[d][1]);
+        }
+    }
+    const int i0 = w * SLICE + 2 * lane;
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int i = i0 + r;
+        if (i >= c.nv)
+            continue;
+        const bool fix = bflag[i] && !pdir[i];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            double q = hat.q[d][i] - (c.dt * acc[d][r]) / c.rho;
+            if (fix && vd[d][i])
+                q = vel_old.q[d][i];
+            vel_new.q[d][i] = q;
+        }
+    }
+}
+
+// normal-derivative velocity rows (:166-181): q[i] = -sum_{j != i} c_ij q[j] / c_ii
+template <int DIM>
+__global__ void k_vel_neumann(int nb, const int *__restrict__ rows, const int *__restrict__ cols,
+                              const double *__restrict__ g0, const double *__restrict__ g1,
+                              const double *__restrict__ g2, const double *__restrict__ normal,
+                              const uint8_t *__restrict__ d0, const uint8_t *__restrict__ d1,
+                              const uint8_t *__restrict__ d2, Vec3w vel_new, int K) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nb)
+        return;
+    const int i = rows[t];
+    const double *G[3] = {g0, g1, g2};
+    const uint8_t *vd[3] = {d0, d1, d2};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        if (vd[d][i])
+            continue;
+        double rhs = 0.0, diag = 0.0;
+        for (int k = 0; k < K; k++) {
+            const size_t o = ell_index(i, k, K);
+            const int j = cols[o];
+            double cf = G[0][o] * normal[(size_t)DIM * i];
+#pragma unroll
+            for (int e = 1; e < DIM; e++)
+                cf = cf + G[e][o] * normal[(size_t)DIM * i + e];
+            if (j == i)
+                diag = cf;
+            else
+                rhs = rhs - cf * vel_new.q[d][j];
+        }
+        vel_new.q[d][i] = rhs / diag;
+    }
+}
+
+__global__ void k_step_log(int *step, const BicgScalars *S, double *log, int cap, const double *x,
+                           int nv, int bordered, int mixed) {
+    const int s = *step;
+    double *e = log + 4 * (size_t)(s % cap);
+    e[0] = mixed ? S->total_inner : S->it;
+    e[1] = S->b64_sq > 0 ? sqrt(S->rr_true / S->b64_sq) : 0.0;
+    e[2] = sqrt(S->rr_true);
+    e[3] = bordered ? x[nv] : 0.0;
+    *step = s + 1;
+}
+
+}  // namespace mp
+
+using namespace mp;
+
+struct mp_fs1_s {
+    mp_cloud c = nullptr;
+    int nv = 0, K = 0, dim = 0;
+    Fs1Const k{};
+    dbuf<uint8_t> bflag, vdir[3], pdir;
+    dbuf<double> normal;
+    dbuf<int> nrows;  // boundary rows that need the Neumann velocity solve
+    int n_neumann = 0;
+    dbuf<double> vel[2][3], hat[3], hist[3];
+    Ppe P;
+    dbuf<int> step;
+    dbuf<double> log;
+    int log_cap = 4096;
+    GraphExec graph[2];
+    int cur = 0;
+    int use_graph = 1;
+};
+
+namespace mp {
+
+static int fs1_issue_pre(mp_fs1_s *f, int cur, cudaStream_t s) {
+    CloudView cv = cloud_view(f->c);
+    const unsigned nb = (unsigned)(((f->nv + SLICE - 1) / SLICE + 7) / 8);
+    Vec3 vel{}, hatc{};
+    Vec3w hat{}, hist{};
+    for (int d = 0; d < f->dim; d++) {
+        vel.q[d] = f->vel[cur][d].p;
+        hat.q[d] = f->hat[d].p;
+        hatc.q[d] = f->hat[d].p;
+        hist.q[d] = f->hist[d].p;
+    }
+    if (f->dim == 2) {
+        k_vel_hat<2><<<nb, 256, 0, s>>>(cv.cols, cv.w[0], cv.w[1], nullptr, cv.w[3], vel, hat, hist,
+                                         f->k, f->step.p);
+        MP_CHECK_LAUNCH();
+        k_p_rhs<2><<<nb, 256, 0, s>>>(cv.cols, cv.w[0], cv.w[1], nullptr, hatc, vel, f->bflag.p,
+                                       f->pdir.p, f->normal.p, f->P.W.x.p, f->P.W.b64.p, f->k);
+    } else {
+        k_vel_hat<3><<<nb, 256, 0, s>>>(cv.cols, cv.w[0], cv.w[1], cv.w[2], cv.w[3], vel, hat, hist,
+                                         f->k, f->step.p);
+        MP_CHECK_LAUNCH();
+        k_p_rhs<3><<<nb, 256, 0, s>>>(cv.cols, cv.w[0], cv.w[1], cv.w[2], hatc, vel, f->bflag.p,
+                                       f->pdir.p, f->normal.p, f->P.W.x.p, f->P.W.b64.p, f->k);
+    }
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+static int fs1_issue_post(mp_fs1_s *f, int cur, cudaStream_t s) {
+    CloudView cv = cloud_view(f->c);
+    const unsigned nb = (unsigned)(((f->nv + SLICE - 1) / SLICE + 7) / 8);
+    const int nxt = 1 - cur;
+    Vec3 hat{}, vo{};
+    Vec3w vn{};
+    for (int d = 0; d < f->dim; d++) {
+        hat.q[d] = f->hat[d].p;
+        vo.q[d] = f->vel[cur][d].p;
+        vn.q[d] = f->vel[nxt][d].p;
+    }
+    const uint8_t *d2 = f->dim == 3 ? f->vdir[2].p : f->vdir[0].p;
+    if (f->dim == 2)
+        k_vel_corr<2><<<nb, 256, 0, s>>>(cv.cols, cv.w[0], cv.w[1], nullptr, hat, vo, vn, f->P.W.x.p,
+                                          f->bflag.p, f->pdir.p, f->vdir[0].p, f->vdir[1].p, d2, f->k);
+    else
+        k_vel_corr<3><<<nb, 256, 0, s>>>(cv.cols, cv.w[0], cv.w[1], cv.w[2], hat, vo, vn, f->P.W.x.p,
+                                          f->bflag.p, f->pdir.p, f->vdir[0].p, f->vdir[1].p, d2, f->k);
+    MP_CHECK_LAUNCH();
+    if (f->n_neumann > 0) {
+        const unsigned bb = (unsigned)((f->n_neumann + 127) / 128);
+        if (f->dim == 2)
+            k_vel_neumann<2><<<bb, 128, 0, s>>>(f->n_neumann, f->nrows.p, cv.cols, cv.w[0], cv.w[1],
+                                                 nullptr, f->normal.p, f->vdir[0].p, f->vdir[1].p,
+                                                 d2, vn, f->K);
+        else
+            k_vel_neumann<3><<<bb, 128, 0, s>>>(f->n_neumann, f->nrows.p, cv.cols, cv.w[0], cv.w[1],
+                                                 cv.w[2], f->normal.p, f->vdir[0].p, f->vdir[1].p,
+                                                 d2, vn, f->K);
+        MP_CHECK_LAUNCH();
+    }
+    k_step_log<<<1, 1, 0, s>>>(f->step.p, f->P.W.scal.p, f->log.p, f->log_cap, f->P.W.x.p, f->nv,
+                               f->P.sys.bordered, f->P.cfg.precision == MP_FP32);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+static int fs1_step_once(mp_fs1_s *f, bool graph, cudaStream_t s) {
+    const int cur = f->cur;
+    if (graph) {
+        GraphExec &G = f->graph[cur];
+        if (!G.e) {
+            GraphBuilder gb;
+            MP_TRY(gb.init_root(f->P.cap_stream()));
+            int rc = gb.captured([&](cudaStream_t cs) { return fs1_issue_pre(f, cur, cs); });
+            if (rc == MP_OK)
+                rc = f->P.build_solve_graph(gb);
+            if (rc == MP_OK)
+                rc = gb.captured([&](cudaStream_t cs) { return fs1_issue_post(f, cur, cs); });
+            if (rc != MP_OK) {
+                if (gb.g)
+                    cudaGraphDestroy(gb.g);
+                return rc;
+            }
+            MP_TRY(G.instantiate(gb));
+        }
+        MP_TRY(G.launch(s));
+    } else {
+        MP_TRY(fs1_issue_pre(f, cur, s));
+        MP_TRY(f->P.solve_eager(s));
+        MP_TRY(fs1_issue_post(f, cur, s));
+    }
+    f->cur = 1 - cur;
+    return MP_OK;
+}
+
+}  // namespace mp
+
+extern "C" int mp_fs1_create(mp_cloud c, const uint8_t *boundary, const double *normal,
+                             const uint8_t *u_dir, const uint8_t *v_dir, const uint8_t *w_dir,
+                             const uint8_t *p_dir, const mp_fs1_cfg *cfg,
+                             const mp_solver_cfg *solver, mp_fs1 *out) {
+    if (!c || !boundary || !normal || !u_dir || !v_dir || !p_dir || !cfg || !solver || !out)
+        return fail(MP_BAD_ARG, "mp_fs1_create: null argument");
+    int nv, n, dim;
+    MP_TRY(mp_cloud_info(c, &nv, &n, &dim));
+    if (dim == 3 && !w_dir)
+        return fail(MP_BAD_ARG, "3D fractional step needs w_dirichlet");
+    // fractional_step_1.cpp:78-102 (check_bc)
+    std::vector<uint8_t> hu(nv), hv(nv), hw(nv, 1), hp(nv), hb(nv);
+    MP_CUDA(cudaMemcpy(hu.data(), u_dir, nv, cudaMemcpyDefault));
+    MP_CUDA(cudaMemcpy(hv.data(), v_dir, nv, cudaMemcpyDefault));
+    if (dim == 3)
+        MP_CUDA(cudaMemcpy(hw.data(), w_dir, nv, cudaMemcpyDefault));
+    MP_CUDA(cudaMemcpy(hp.data(), p_dir, nv, cudaMemcpyDefault));
+    MP_CUDA(cudaMemcpy(hb.data(), boundary, nv, cudaMemcpyDefault));
+    long su = 0, sv = 0, sw = 0;
+    for (int i = 0; i < nv; i++) {
+        su += hu[i];
+        sv += hv[i];
+        sw += hw[i];
+    }
+    if (su == 0)
+        return fail(MP_BAD_ARG, "Setting u_dirichlet_flag to full Neumann BC is not permitted");
+    if (sv == 0)
+        return fail(MP_BAD_ARG, "Setting v_dirichlet_flag to full Neumann BC is not permitted");
+    if (dim == 3 && sw == 0)
+        return fail(MP_BAD_ARG, "Setting w_dirichlet_flag to full Neumann BC is not permitted");
+    if (cfg->rho < 0 || cfg->mu < 0)
+        return fail(MP_BAD_ARG, "Some parameters are not set; rho: %g, mu: %g", cfg->rho, cfg->mu);
+    if (cfg->temporal_order != 1 && cfg->temporal_order != 2)
+        return fail(MP_BAD_ARG, "temporal_order should be either '1' or '2'; current value: %d",
+                    cfg->temporal_order);
+    if (!(cfg->dt > 0))
+        return fail(MP_BAD_ARG, "dt must be positive");
+    mp_fs1 f = new mp_fs1_s;
+    f->c = c;
+    f->nv = nv;
+    f->K = n;
+    f->dim = dim;
+    auto bail = [&](int rc) {
+        delete f;
+        return rc;
+    };
+    int rc = f->P.create(c, boundary, p_dir, normal, 0.0, 0.0, 1.0, *solver, 0);
+    if (rc != MP_OK)
+        return bail(rc);
+    f->k.rho = cfg->rho;
+    f->k.mu = cfg->mu;
+    f->k.dt = cfg->dt;
+    f->k.order = cfg->temporal_order;
+    f->k.nv = nv;
+    f->k.K = n;
+    f->k.bordered = f->P.sys.bordered;
+    const uint8_t *dirs[3] = {u_dir, v_dir, w_dir};
+    if ((rc = f->bflag.alloc(nv)) || (rc = f->pdir.alloc(nv)) || (rc = f->normal.alloc((size_t)nv * dim)))
+        return bail(rc);
+    cudaMemcpy(f->bflag.p, hb.data(), nv, cudaMemcpyHostToDevice);
+    cudaMemcpy(f->pdir.p, hp.data(), nv, cudaMemcpyHostToDevice);
+    cudaMemcpy(f->normal.p, normal, sizeof(double) * nv * dim, cudaMemcpyDefault);
+    for (int d = 0; d < dim; d++) {
+        if ((rc = f->vdir[d].alloc(nv)))
+            return bail(rc);
+        cudaMemcpy(f->vdir[d].p, dirs[d], nv, cudaMemcpyDefault);
+        for (int b = 0; b < 2; b++)
+            if ((rc = f->vel[b][d].alloc(nv)))
+                return bail(rc);
+        if ((rc = f->hat[d].alloc(nv)) || (rc = f->hist[d].alloc(nv)))
+            return bail(rc);
+        cudaMemset(f->hist[d].p, 0, sizeof(double) * nv);
+        cudaMemset(f->vel[0][d].p, 0, sizeof(double) * nv);
+        cudaMemset(f->vel[1][d].p, 0, sizeof(double) * nv);
+    }
+    std::vector<int> rows;
+    for (int i = 0; i < nv; i++) {
+        if (!hb[i] || hp[i])
+            continue;
+        bool need = !hu[i] || !hv[i] || (dim == 3 && !hw[i]);
+        if (need)
+            rows.push_back(i);
+    }
+    f->n_neumann = (int)rows.size();
+    if (!rows.empty()) {
+        if ((rc = f->nrows.alloc(rows.size())))
+            return bail(rc);
+        cudaMemcpy(f->nrows.p, rows.data(), sizeof(int) * rows.size(), cudaMemcpyHostToDevice);
+    }
+    if ((rc = f->step.alloc(1)) || (rc = f->log.alloc(4 * (size_t)f->log_cap)))
+        return bail(rc);
+    cudaMemset(f->step.p, 0, sizeof(int));
+    cudaMemset(f->P.W.x.p, 0, sizeof(double) * f->P.sys.nsys);
+    if (cudaDeviceSynchronize() != cudaSuccess)
+        return bail(fail(MP_CUDA_ERROR, "mp_fs1_create: %s", cudaGetErrorString(cudaGetLastError())));
+    *out = f;
+    return MP_OK;
+}
+
+extern "C" int mp_fs1_system_size(mp_fs1 f) { return f ? f->P.sys.nsys : -1; }
+
+extern "C" int mp_fs1_set_state(mp_fs1 f, const double *const *vel, const double *p, int it,
+                                mp_stream s) {
+    if (!f || !vel)
+        return fail(MP_BAD_ARG, "mp_fs1_set_state: null argument");
+    cudaStream_t st = S(s);
+    for (int d = 0; d < f->dim; d++)
+        MP_CUDA(cudaMemcpyAsync(f->vel[f->cur][d].p, vel[d], sizeof(double) * f->nv,
+                                cudaMemcpyDefault, st));
+    if (p)
+        MP_CUDA(cudaMemcpyAsync(f->P.W.x.p, p, sizeof(double) * f->P.sys.nsys, cudaMemcpyDefault, st));
+    MP_CUDA(cudaMemcpyAsync(f->step.p, &it, sizeof(int), cudaMemcpyHostToDevice, st));
+    MP_CUDA(cudaStreamSynchronize(st));
+    return MP_OK;
+}
+
+extern "C" int mp_fs1_get_state(mp_fs1 f, double *const *vel, double *p, mp_stream s) {
+    if (!f)
+        return fail(MP_BAD_ARG, "null fractional-step handle");
+    cudaStream_t st = S(s);
+    if (vel)
+        for (int d = 0; d < f->dim; d++)
+            if (vel[d])
+                MP_CUDA(cudaMemcpyAsync(vel[d], f->vel[f->cur][d].p, sizeof(double) * f->nv,
+                                        cudaMemcpyDefault, st));
+    if (p)
+        MP_CUDA(cudaMemcpyAsync(p, f->P.W.x.p, sizeof(double) * f->P.sys.nsys, cudaMemcpyDefault, st));
+    MP_CUDA(cudaStreamSynchronize(st));
+    return MP_OK;
+}
+
+extern "C" int mp_fs1_step(mp_fs1 f, int nsteps, int use_graph, mp_stream s) {
+    if (!f || nsteps < 0)
+        return fail(MP_BAD_ARG, "mp_fs1_step: bad arguments");
+    for (int i = 0; i < nsteps; i++)
+        MP_TRY(fs1_step_once(f, use_graph != 0, S(s)));
+    return MP_OK;
+}
+
+extern "C" int mp_fs1_single_timestep(mp_fs1 f, double *const *vel_new, double *p_new,
+                                      const double *const *vel_old, const double *p_old, int it,
+                                      mp_stream s) {
+    if (!f || !vel_new || !p_new || !vel_old || !p_old)
+        return fail(MP_BAD_ARG, "mp_fs1_single_timestep: null argument");
+    MP_TRY(mp_fs1_set_state(f, vel_old, p_old, it, s));
+    MP_TRY(fs1_step_once(f, f->use_graph != 0, S(s)));
+    MP_TRY(mp_fs1_get_state(f, vel_new, p_new, s));
+    int iters;
+    double rr;
+    MP_TRY(mp_fs1_last_stats(f, &iters, &rr, nullptr, nullptr));
+    if (!(rr <= f->P.cfg.tol))
+        return fail(std::isfinite(rr) ? MP_NOT_CONVERGED : MP_NAN_DETECTED,
+                    "pressure solve: relative residual %g after %d iterations", rr, iters);
+    return MP_OK;
+}
+
+extern "C" int mp_fs1_last_stats(mp_fs1 f, int *iters, double *relres, double *abs_res,
+                                 double *alpha) {
+    if (!f)
+        return fail(MP_BAD_ARG, "null fractional-step handle");
+    MP_CUDA(cudaDeviceSynchronize());
+    int step = 0;
+    MP_CUDA(cudaMemcpy(&step, f->step.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (step <= 0)
+        return fail(MP_BAD_ARG, "no step has been taken");
+    double e[4];
+    MP_CUDA(cudaMemcpy(e, f->log.p + 4 * (size_t)((step - 1) % f->log_cap), sizeof(e),
+                       cudaMemcpyDeviceToHost));
+    if (iters)
+        *iters = (int)e[0];
+    if (relres)
+        *relres = e[1];
+    if (abs_res)
+        *abs_res = e[2];
+    if (alpha)
+        *alpha = e[3];
+    return MP_OK;
+}
+
+extern "C" int mp_fs1_log(mp_fs1 f, int first, int count, double *out) {
+    if (!f || !out || first < 0 || count < 0 || count > f->log_cap)
+        return fail(MP_BAD_ARG, "mp_fs1_log: bad arguments");
+    MP_CUDA(cudaDeviceSynchronize());
+    int step = 0;
+    MP_CUDA(cudaMemcpy(&step, f->step.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (first + count > step || first < step - f->log_cap)
+        return fail(MP_BAD_ARG, "mp_fs1_log: steps %d..%d not in the log (last step %d)", first,
+                    first + count - 1, step - 1);
+    for (int i = 0; i < count; i++)
+        MP_CUDA(cudaMemcpy(out + 4 * (size_t)i, f->log.p + 4 * (size_t)((first + i) % f->log_cap),
+                           4 * sizeof(double), cudaMemcpyDeviceToHost));
+    return MP_OK;
+}
+
+extern "C" int mp_fs1_destroy(mp_fs1 f) {
+    delete f;
+    return MP_OK;
+}

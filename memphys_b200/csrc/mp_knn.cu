@@ -1,0 +1,235 @@
+// mp_knn.cu -- stencil selection on the GPU (replaces CLOUD::calc_cloud_points_fast,
+// cloud.cpp:570-648, which queries two nanoflann KD-trees on the host).
+//
+// Rule (cloud.cpp:617-646): an interior node's stencil is its n nearest nodes of
+// the whole cloud (itself first, at distance 0); a boundary node's stencil is the
+// node itself followed by its n-1 nearest INTERIOR nodes (the reference places
+// boundary nodes at infinity in the second tree, :596-601).  Neighbours are in
+// ascending distance, ties broken by node index.
+//
+// Method: points are bucketed on a uniform grid (about two per cell) by a radix
+// sort of their cell ids; each query thread scans square/cubic shells of cells
+// of growing radius, keeping the best candidates in a sorted list, and stops
+// once the k-th distance is within the radius already covered.  This is an
+// exact search, so it selects the same stencils as the KD-tree.
+#include <cub/cub.cuh>
+#include <cmath>
+#include "mp_common.cuh"
+
+namespace mp {
+
+constexpr int KNN_MAX = 64;
+
+struct Grid {
+    double lo[3];
+    double cell;
+    int g[3];
+};
+
+__global__ void knn_cell_ids(const double *xyz, int nv, int dim, Grid G, unsigned int *cid,
+                             int *idx) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv)
+        return;
+    unsigned int c = 0;
+    for (int d = dim - 1; d >= 0; d--) {
+        int k = (int)((xyz[(size_t)i * dim + d] - G.lo[d]) / G.cell);
+        k = k < 0 ? 0 : (k >= G.g[d] ? G.g[d] - 1 : k);
+        c = c * G.g[d] + k;
+    }
+    cid[i] = c;
+    idx[i] = i;
+}
+
+__global__ void knn_cell_ranges(const unsigned int *cid_sorted, int nv, int *start, int *end) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv)
+        return;
+    unsigned int c = cid_sorted[i];
+    if (i == 0 || cid_sorted[i - 1] != c)
+        start[c] = i;
+    if (i == nv - 1 || cid_sorted[i + 1] != c)
+        end[c] = i + 1;
+}
+
+__global__ void __launch_bounds__(128)
+    knn_query(const double *xyz, const uint8_t *bflag, int nv, int dim, int n, Grid G,
+              const int *order, const int *start, const int *end, int *nb_col, int *failed) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nv)
+        return;
+    double bd[KNN_MAX];
+    int bi[KNN_MAX];
+    const bool isb = bflag[q] != 0;
+    const int want = isb ? n - 1 : n;
+    double xq[3] = {0, 0, 0};
+    int qc[3] = {0, 0, 0};
+    for (int d = 0; d < dim; d++) {
+        xq[d] = xyz[(size_t)q * dim + d];
+        int k = (int)((xq[d] - G.lo[d]) / G.cell);
+        qc[d] = k < 0 ? 0 : (k >= G.g[d] ? G.g[d] - 1 : k);
+    }
+    int cnt = 0;
+    for (int R = 0;; R++) {
+        int zlo = dim == 3 ? qc[2] - R : 0, zhi = dim == 3 ? qc[2] + R : 0;
+        for (int cz = zlo; cz <= zhi; cz++)
+            for (int cy = qc[1] - R; cy <= qc[1] + R; cy++)
+                for (int cx = qc[0] - R; cx <= qc[0] + R; cx++) {
+                    bool shell = cx == qc[0] - R || cx == qc[0] + R || cy == qc[1] - R ||
+                                 cy == qc[1] + R || (dim == 3 && (cz == zlo || cz == zhi));
+                    if (!shell)
+                        continue;
+                    if (cx < 0 || cx >= G.g[0] || cy < 0 || cy >= G.g[1] || cz < 0 || cz >= G.g[2])
+                        continue;
+                    unsigned int c = ((unsigned)cz * G.g[1] + cy) * G.g[0] + cx;
+                    int s0 = start[c], s1 = end[c];
+                    for (int t = s0; t < s1; t++) {
+                        int j = order[t];
+                        if (isb && bflag[j])
+                            continue;
+                        double dd = 0.0;
+                        for (int d = 0; d < dim; d++) {
+                            double df = xyz[(size_t)j * dim + d] - xq[d];
+                            dd += df * df;
+                        }
+                        if (cnt == want &&
+                            (dd > bd[want - 1] || (dd == bd[want - 1] && j > bi[want - 1])))
+                            continue;
+                        int pos = cnt < want ? cnt++ : want - 1;
+                        while (pos > 0 && (bd[pos - 1] > dd || (bd[pos - 1] == dd && bi[pos - 1] > j))) {
+                            bd[pos] = bd[pos - 1];
+                            bi[pos] = bi[pos - 1];
+                            pos--;
+                        }
+                        bd[pos] = dd;
+                        bi[pos] = j;
+                    }
+                }
+        double reach = R * G.cell;
+        bool covered = true;
+        for (int d = 0; d < dim; d++)
+            if (qc[d] - R > 0 || qc[d] + R < G.g[d] - 1)
+                covered = false;
+        if (cnt == want && bd[want - 1] <= reach * reach)
+            break;
+        if (covered)
+            break;
+    }
+    int *out = nb_col + (size_t)q * n;
+    if (cnt < want) {
+        atomicAdd(failed, 1);
+        for (int k = 0; k < n; k++)
+            out[k] = q;
+        return;
+    }
+    if (isb) {
+        out[0] = q;
+        for (int k = 0; k < n - 1; k++)
+            out[k + 1] = bi[k];
+    } else {
+        for (int k = 0; k < n; k++)
+            out[k] = bi[k];
+    }
+}
+
+int knn_device(const double *d_xyz, const uint8_t *d_bflag, int nv, int dim, int n, int *d_nb,
+               cudaStream_t s) {
+    if (nv <= 0 || (dim != 2 && dim != 3) || n < 2 || n > KNN_MAX)
+        return fail(MP_BAD_ARG, "mp_knn_stencils: nv=%d dim=%d n=%d (n must be 2..%d)", nv, dim, n,
+                    KNN_MAX);
+    // bounding box on the host (one small copy; setup path)
+    std::vector<double> h((size_t)nv * dim);
+    MP_CUDA(cudaMemcpyAsync(h.data(), d_xyz, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    Grid G;
+    double hi[3] = {0, 0, 0};
+    for (int d = 0; d < 3; d++)
+        G.lo[d] = 0.0, G.g[d] = 1;
+    for (int d = 0; d < dim; d++)
+        G.lo[d] = hi[d] = h[d];
+    for (int i = 0; i < nv; i++)
+        for (int d = 0; d < dim; d++) {
+            double v = h[(size_t)i * dim + d];
+            if (!std::isfinite(v))
+                return fail(MP_BAD_ARG, "node %d has a non-finite coordinate", i);
+            G.lo[d] = v < G.lo[d] ? v : G.lo[d];
+            hi[d] = v > hi[d] ? v : hi[d];
+        }
+    double vol = 1.0;
+    for (int d = 0; d < dim; d++)
+        vol *= (hi[d] - G.lo[d]) > 0 ? (hi[d] - G.lo[d]) : 1.0;
+    G.cell = std::pow(vol * 2.0 / nv, 1.0 / dim);
+    long long ncell = 1;
+    for (int d = 0; d < dim; d++) {
+        G.g[d] = (int)((hi[d] - G.lo[d]) / G.cell) + 1;
+        ncell *= G.g[d];
+    }
+    if (ncell > (1ll << 31))
+        return fail(MP_BAD_ARG, "kNN grid too large (%lld cells)", ncell);
+    dbuf<unsigned int> cid, cid2;
+    dbuf<int> idx, idx2, st, en, failed;
+    MP_TRY(cid.alloc(nv));
+    MP_TRY(cid2.alloc(nv));
+    MP_TRY(idx.alloc(nv));
+    MP_TRY(idx2.alloc(nv));
+    MP_TRY(st.alloc(ncell));
+    MP_TRY(en.alloc(ncell));
+    MP_TRY(failed.alloc(1));
+    MP_CUDA(cudaMemsetAsync(st.p, 0, sizeof(int) * ncell, s));
+    MP_CUDA(cudaMemsetAsync(en.p, 0, sizeof(int) * ncell, s));
+    MP_CUDA(cudaMemsetAsync(failed.p, 0, sizeof(int), s));
+    const int tb = 256, nb = (nv + tb - 1) / tb;
+    knn_cell_ids<<<nb, tb, 0, s>>>(d_xyz, nv, dim, G, cid.p, idx.p);
+    MP_CHECK_LAUNCH();
+    size_t tmp_bytes = 0;
+    int bits = 1;
+    while ((1ll << bits) < ncell)
+        bits++;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, cid.p, cid2.p, idx.p, idx2.p, nv, 0, bits, s);
+    dbuf<char> tmp;
+    MP_TRY(tmp.alloc(tmp_bytes));
+    MP_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, cid.p, cid2.p, idx.p, idx2.p, nv, 0,
+                                            bits, s));
+    count_launch();
+    knn_cell_ranges<<<nb, tb, 0, s>>>(cid2.p, nv, st.p, en.p);
+    MP_CHECK_LAUNCH();
+    knn_query<<<(nv + 127) / 128, 128, 0, s>>>(d_xyz, d_bflag, nv, dim, n, G, idx2.p, st.p, en.p,
+                                                d_nb, failed.p);
+    MP_CHECK_LAUNCH();
+    int bad = 0;
+    MP_CUDA(cudaMemcpyAsync(&bad, failed.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    if (bad)
+        return fail(MP_KNN_FAILED, "%d nodes found fewer than %d stencil candidates", bad, n);
+    return MP_OK;
+}
+
+}  // namespace mp
+
+using namespace mp;
+
+extern "C" int mp_knn_stencils(const double *xyz, const uint8_t *boundary, int nv, int dim, int n,
+                               int *nb_col, mp_stream s) {
+    if (!xyz || !boundary || !nb_col)
+        return fail(MP_BAD_ARG, "mp_knn_stencils: null argument");
+    cudaStream_t st = S(s);
+    dbuf<double> tx;
+    dbuf<uint8_t> tb;
+    const double *dx;
+    const uint8_t *db;
+    MP_TRY(stage_in(xyz, (size_t)nv * dim, tx, &dx, st));
+    MP_TRY(stage_in(boundary, (size_t)nv, tb, &db, st));
+    int *dn = nb_col;
+    dbuf<int> tn;
+    bool host_out = !is_device_ptr(nb_col);
+    if (host_out) {
+        MP_TRY(tn.alloc((size_t)nv * n));
+        dn = tn.p;
+    }
+    MP_TRY(knn_device(dx, db, nv, dim, n, dn, st));
+    if (host_out) {
+        MP_CUDA(cudaMemcpyAsync(nb_col, dn, sizeof(int) * nv * n, cudaMemcpyDeviceToHost, st));
+        MP_CUDA(cudaStreamSynchronize(st));
+    }
+    return MP_OK;
+}

@@ -1,0 +1,900 @@
+// mp_krylov.cu -- pressure-Poisson system assembly and BiCGSTAB (FP64, and
+// FP32 inner iterations under FP64 iterative refinement), with the mp_ppe_*
+// C ABI (SOLVER::init / SOLVER::general_solve, solver.cpp:14-79, 283-363).
+#include <cmath>
+#include "mp_krylov.cuh"
+#include "mp_amg.cuh"
+#include "mp_cloud.cuh"
+#include "mp_ppe.cuh"
+
+namespace mp {
+
+template <class T> struct V2t;
+template <> struct V2t<double> { using type = double2; };
+template <> struct V2t<float> { using type = float2; };
+
+constexpr double EPS2 = 2.220446049250313e-16 * 2.220446049250313e-16;
+constexpr int KT = 256;  // threads per block in all Krylov kernels (8 slices)
+
+__device__ __forceinline__ int gwarp() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
+
+// Rows r0 = 64w + 2 lane and r0 + 1 of slice w: a = (A x)_row, xs = x at the
+// self column (stencil entry 0 is the row's own node).
+template <class T>
+__device__ __forceinline__ void ell_pair(const EllView<T> &A, int w, int lane,
+                                         const T *__restrict__ x, T &a0, T &a1, T &xs0, T &xs1) {
+    using V2 = typename V2t<T>::type;
+    const size_t base = (size_t)w * A.K * SLICE + 2 * lane;
+    int2 c = __ldcs(reinterpret_cast<const int2 *>(A.cols + base));
+    V2 v = __ldcs(reinterpret_cast<const V2 *>(A.vals + base));
+    xs0 = __ldg(x + c.x);
+    xs1 = __ldg(x + c.y);
+    a0 = v.x * xs0;
+    a1 = v.y * xs1;
+#pragma unroll 4
+    for (int k = 1; k < A.K; k++) {
+        const size_t o = base + (size_t)k * SLICE;
+        c = __ldcs(reinterpret_cast<const int2 *>(A.cols + o));
+        v = __ldcs(reinterpret_cast<const V2 *>(A.vals + o));
+        a0 = fma(v.x, __ldg(x + c.x), a0);
+        a1 = fma(v.y, __ldg(x + c.y), a1);
+    }
+}
+
+struct RedBuf {
+    double *partials;
+    unsigned int *ticket;
+};
+
+#define KRYLOV_SMEM __shared__ double red_smem[32 * 4];
+
+// ---------------------------------------------------------------- init
+// r = b - A x, r0 = r, p = v = 0, scalars of Eigen's BiCGSTAB prologue.
+template <class T, bool ZERO_X>
+__global__ void __launch_bounds__(KT)
+    k_init(EllView<T> A, int bordered, const T *x, const T *b, T *r, T *r0, T *p, T *v,
+           BicgScalars *S, RedBuf R, double tol, int maxit, cudaGraphConditionalHandle h) {
+    KRYLOV_SMEM
+    const int nv = A.nrows, w = gwarp(), lane = threadIdx.x & 31;
+    const int nsl = (nv + SLICE - 1) / SLICE;
+    double acc[3] = {0, 0, 0};
+    if (w < nsl) {
+        T a0 = 0, a1 = 0, s0 = 0, s1 = 0;
+        if (!ZERO_X)
+            ell_pair(A, w, lane, x, a0, a1, s0, s1);
+        const T xb = (bordered && !ZERO_X) ? x[nv] : T(0);
+        const int i0 = w * SLICE + 2 * lane;
+        T as[2] = {a0, a1}, ss[2] = {s0, s1};
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int i = i0 + q;
+            if (i < nv) {
+                const T ri = b[i] - (as[q] + xb);
+                r[i] = ri;
+                r0[i] = ri;
+                p[i] = 0;
+                v[i] = 0;
+                acc[0] += (double)ri * ri;
+                acc[1] += (double)b[i] * b[i];
+                acc[2] += (double)ss[q];
+            }
+        }
+    }
+    if (grid_reduce<3>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
+        double rr = acc[0], bb = acc[1];
+        if (bordered) {
+            const T rn = b[nv] - (T)acc[2];
+            r[nv] = rn;
+            r0[nv] = rn;
+            p[nv] = 0;
+            v[nv] = 0;
+            rr += (double)rn * rn;
+            bb += (double)b[nv] * b[nv];
+        }
+        S->b_sq = bb;
+        S->r0_sq = rr;
+        S->rr = rr;
+        S->rho_old = 1.0;
+        S->rho = rr;
+        S->alpha = 1.0;
+        S->omega = 1.0;
+        S->it = 0;
+        S->restarts = 0;
+        S->need_restart = 0;
+        S->maxit = maxit;
+        S->tol2 = tol * tol * bb;
+        S->zero_x = (bb == 0.0);
+        int done = (bb == 0.0) || !(rr > S->tol2 && maxit > 0);
+        S->status = MP_OK;
+        if (!isfinite(rr) || !isfinite(bb)) {
+            S->status = MP_NAN_DETECTED;
+            done = 1;
+        }
+        S->done = done;
+        if (h)
+            cudaGraphSetConditional(h, done ? 0u : 1u);
+    }
+}
+
+// Eigen's restart: r = b - A x, r0 = r, rho = r0_sq = ||r||^2 (rare path)
+template <class T>
+__global__ void __launch_bounds__(KT)
+    k_restart(EllView<T> A, int bordered, const T *x, const T *b, T *r, T *r0, BicgScalars *S,
+              RedBuf R) {
+    KRYLOV_SMEM
+    if (S->done || !S->need_restart)
+        return;
+    const int nv = A.nrows, w = gwarp(), lane = threadIdx.x & 31;
+    const int nsl = (nv + SLICE - 1) / SLICE;
+    double acc[2] = {0, 0};
+    if (w < nsl) {
+        T a0, a1, s0, s1;
+        ell_pair(A, w, lane, x, a0, a1, s0, s1);
+        const T xb = bordered ? x[nv] : T(0);
+        const int i0 = w * SLICE + 2 * lane;
+        T as[2] = {a0, a1}, ss[2] = {s0, s1};
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int i = i0 + q;
+            if (i < nv) {
+                const T ri = b[i] - (as[q] + xb);
+                r[i] = ri;
+                r0[i] = ri;
+                acc[0] += (double)ri * ri;
+                acc[1] += (double)ss[q];
+            }
+        }
+    }
+    if (grid_reduce<2>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
+        double rr = acc[0];
+        if (bordered) {
+            const T rn = b[nv] - (T)acc[1];
+            r[nv] = rn;
+            r0[nv] = rn;
+            rr += (double)rn * rn;
+        }
+        S->r0_sq = rr;
+        S->rho = rr;
+        if (S->restarts++ == 0)
+            S->it = 0;
+        S->need_restart = 0;
+    }
+}
+
+// p = r + beta (p - omega v); y = M^-1 p for the fused preconditioners
+template <class T, int PK>
+__global__ void __launch_bounds__(KT)
+    k_update_p(int nv, int bordered, const T *r, T *p, const T *v, T *y, const T *dinv,
+               const BicgScalars *S) {
+    if (S->done)
+        return;
+    const double beta = (S->rho / S->rho_old) * (S->alpha / S->omega);
+    const T bt = (T)beta, om = (T)S->omega;
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += stride) {
+        const T pi = r[i] + bt * (p[i] - om * v[i]);
+        p[i] = pi;
+        if (PK == PK_JACOBI)
+            y[i] = dinv[i] * pi;
+    }
+    if (bordered && blockIdx.x == 0 && threadIdx.x == 0) {
+        const T pi = r[nv] + bt * (p[nv] - om * v[nv]);
+        p[nv] = pi;
+        if (PK != PK_NONE)
+            y[nv] = pi;
+    }
+}
+
+// v = A y, alpha = rho / (r0 . v)
+template <class T>
+__global__ void __launch_bounds__(KT)
+    k_spmv_alpha(EllView<T> A, int bordered, const T *y, T *v, const T *r0, BicgScalars *S,
+                 RedBuf R) {
+    KRYLOV_SMEM
+    if (S->done)
+        return;
+    const int nv = A.nrows, w = gwarp(), lane = threadIdx.x & 31;
+    const int nsl = (nv + SLICE - 1) / SLICE;
+    double acc[2] = {0, 0};
+    if (w < nsl) {
+        T a0, a1, s0, s1;
+        ell_pair(A, w, lane, y, a0, a1, s0, s1);
+        const T yb = bordered ? y[nv] : T(0);
+        const int i0 = w * SLICE + 2 * lane;
+        T as[2] = {a0, a1}, ss[2] = {s0, s1};
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int i = i0 + q;
+            if (i < nv) {
+                const T vi = as[q] + yb;
+                v[i] = vi;
+                acc[0] += (double)r0[i] * vi;
+                acc[1] += (double)ss[q];
+            }
+        }
+    }
+    if (grid_reduce<2>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
+        double d = acc[0];
+        if (bordered) {
+            const T vb = (T)acc[1];
+            v[nv] = vb;
+            d += (double)r0[nv] * vb;
+        }
+        S->dot_rv = d;
+        S->alpha = S->rho / d;
+    }
+}
+
+// s = r - alpha v; z = M^-1 s for the fused preconditioners
+template <class T, int PK>
+__global__ void __launch_bounds__(KT)
+    k_update_s(int nv, int bordered, const T *r, const T *v, T *s, T *z, const T *dinv,
+               const BicgScalars *S) {
+    if (S->done)
+        return;
+    const T al = (T)S->alpha;
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += stride) {
+        const T si = r[i] - al * v[i];
+        s[i] = si;
+        if (PK == PK_JACOBI)
+            z[i] = dinv[i] * si;
+    }
+    if (bordered && blockIdx.x == 0 && threadIdx.x == 0) {
+        const T si = r[nv] - al * v[nv];
+        s[nv] = si;
+        if (PK != PK_NONE)
+            z[nv] = si;
+    }
+}
+
+// t = A z, omega = (t . s) / (t . t)
+template <class T>
+__global__ void __launch_bounds__(KT)
+    k_spmv_omega(EllView<T> A, int bordered, const T *z, T *t, const T *s, BicgScalars *S,
+                 RedBuf R) {
+    KRYLOV_SMEM
+    if (S->done)
+        return;
+    const int nv = A.nrows, w = gwarp(), lane = threadIdx.x & 31;
+    const int nsl = (nv + SLICE - 1) / SLICE;
+    double acc[3] = {0, 0, 0};
+    if (w < nsl) {
+        T a0, a1, s0, s1;
+        ell_pair(A, w, lane, z, a0, a1, s0, s1);
+        const T zb = bordered ? z[nv] : T(0);
+        const int i0 = w * SLICE + 2 * lane;
+        T as[2] = {a0, a1}, ss[2] = {s0, s1};
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int i = i0 + q;
+            if (i < nv) {
+                const T ti = as[q] + zb;
+                t[i] = ti;
+                acc[0] += (double)ti * ti;
+                acc[1] += (double)ti * s[i];
+                acc[2] += (double)ss[q];
+            }
+        }
+    }
+    if (grid_reduce<3>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
+        double tt = acc[0], ts = acc[1];
+        if (bordered) {
+            const T tb = (T)acc[2];
+            t[nv] = tb;
+            tt += (double)tb * tb;
+            ts += (double)tb * s[nv];
+        }
+        S->dot_tt = tt;
+        S->dot_ts = ts;
+        S->omega = tt > 0.0 ? ts / tt : 0.0;
+    }
+}
+
+// x += alpha y + omega z; r = s - omega t; convergence test for the next sweep
+template <class T>
+__global__ void __launch_bounds__(KT)
+    k_update_xr(int nsys, T *x, const T *y, const T *z, const T *s, const T *t, T *r, const T *r0,
+                BicgScalars *S, RedBuf R, cudaGraphConditionalHandle h) {
+    KRYLOV_SMEM
+    if (S->done)
+        return;
+    const T al = (T)S->alpha, om = (T)S->omega;
+    double acc[2] = {0, 0};
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += stride) {
+        x[i] = x[i] + (al * y[i] + om * z[i]);
+        const T ri = s[i] - om * t[i];
+        r[i] = ri;
+        acc[0] += (double)ri * ri;
+        acc[1] += (double)r0[i] * ri;
+    }
+    if (grid_reduce<2>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
+        const double rr = acc[0];
+        S->rr = rr;
+        S->it += 1;
+        S->rho_old = S->rho;
+        S->rho = acc[1];
+        S->need_restart = fabs(acc[1]) < EPS2 * S->r0_sq;
+        int done = !(rr > S->tol2 && S->it < S->maxit);
+        if (!isfinite(rr)) {
+            S->status = MP_NAN_DETECTED;
+            done = 1;
+        }
+        S->done = done;
+        if (h)
+            cudaGraphSetConditional(h, done ? 0u : 1u);
+    }
+}
+
+// ||b - A x||^2 in FP64 (the residual solver.cpp:342-343 logs); zero x when
+// ||b|| = 0 as Eigen's BiCGSTAB does.  Optionally stores r64 = b - A x.
+__global__ void __launch_bounds__(KT)
+    k_true_residual(EllView<double> A, int bordered, double *x, const double *b, double *r64,
+                    BicgScalars *S, RedBuf R, int refine, cudaGraphConditionalHandle h) {
+    KRYLOV_SMEM
+    const int nv = A.nrows, w = gwarp(), lane = threadIdx.x & 31;
+    const int nsl = (nv + SLICE - 1) / SLICE;
+    const bool zx = S->zero_x && !refine;
+    double acc[3] = {0, 0, 0};
+    if (w < nsl) {
+        double a0 = 0, a1 = 0, s0 = 0, s1 = 0;
+        if (!zx)
+            ell_pair(A, w, lane, x, a0, a1, s0, s1);
+        const double xb = (bordered && !zx) ? x[nv] : 0.0;
+        const int i0 = w * SLICE + 2 * lane;
+        double as[2] = {a0, a1}, ss[2] = {s0, s1};
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int i = i0 + q;
+            if (i < nv) {
+                if (zx)
+                    x[i] = 0.0;
+                const double ri = b[i] - (as[q] + xb);
+                if (r64)
+                    r64[i] = ri;
+                acc[0] += ri * ri;
+                acc[1] += ss[q];
+                acc[2] += b[i] * b[i];
+            }
+        }
+    }
+    if (grid_reduce<3>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
+        double rr = acc[0], bb = acc[2];
+        if (bordered) {
+            if (zx)
+                x[nv] = 0.0;
+            const double rn = b[nv] - acc[1];
+            if (r64)
+                r64[nv] = rn;
+            rr += rn * rn;
+            bb += b[nv] * b[nv];
+        }
+        S->rr_true = rr;
+        S->b64_sq = bb;
+        if (refine) {  // iterative-refinement loop control
+            int done = !(rr > S->tol_outer2 * bb && S->outer_it < S->outer_max);
+            if (bb == 0.0)
+                done = 1;
+            if (!isfinite(rr) || S->status == MP_NAN_DETECTED) {
+                S->status = MP_NAN_DETECTED;
+                done = 1;
+            }
+            S->outer_done = done;
+            if (h)
+                cudaGraphSetConditional(h, done ? 0u : 1u);
+        }
+    }
+}
+
+// refinement: b32 = r64 / ||r64||, e32 = 0
+__global__ void k_ir_scale(int nsys, const double *r64, float *b32, float *e32, BicgScalars *S) {
+    if (S->outer_done)
+        return;
+    const double sc = sqrt(S->rr_true);
+    const double inv = sc > 0 ? 1.0 / sc : 0.0;
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += stride) {
+        b32[i] = (float)(r64[i] * inv);
+        e32[i] = 0.f;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        S->scale = sc;
+}
+
+// refinement: x64 += ||r64|| * e32
+__global__ void k_ir_update(int nsys, double *x, const float *e32, BicgScalars *S) {
+    if (S->outer_done)
+        return;
+    const double sc = S->scale;
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += stride)
+        x[i] += sc * (double)e32[i];
+    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S->outer_it += 1;
+        S->total_inner += S->it;
+    }
+}
+
+__global__ void k_jacobi_dinv(EllView<double> A, double *dinv, float *dinv32) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.nrows)
+        return;
+    double d = A.vals[ell_index(i, 0, A.K)];
+    double v = (d != 0.0 && isfinite(d)) ? 1.0 / d : 1.0;
+    dinv[i] = v;
+    if (dinv32)
+        dinv32[i] = (float)v;
+}
+
+// ------------------------------------------------------------- assembly
+// solver.cpp:165-204: interior rows diff*L + conv*(Gx+Gy[+Gz]) (+ unsteady on
+// the self entry); Dirichlet rows identity; Neumann rows normal . grad.
+__global__ void k_assemble_ppe(int nv, int K, int dim, const int *cols, const double *gx,
+                               const double *gy, const double *gz, const double *lap,
+                               const uint8_t *bflag, const uint8_t *dir, const double *normal,
+                               double unsteady, double conv, double diff, double *vals,
+                               int *bad_self) {
+    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    size_t total = (size_t)ell_padded_rows(nv) * K;
+    if (t >= total)
+        return;
+    size_t slice = t / ((size_t)K * SLICE);
+    int k = (int)((t / SLICE) % K);
+    int row = (int)(slice * SLICE + (t % SLICE));
+    if (row >= nv) {
+        vals[t] = 0.0;
+        return;
+    }
+    const int col = cols[t];
+    if (k == 0 && col != row)
+        atomicAdd(bad_self, 1);
+    double v;
+    if (bflag[row]) {
+        if (dir[row]) {
+            v = (k == 0) ? 1.0 : 0.0;
+        } else {
+            v = normal[(size_t)dim * row] * gx[t] + normal[(size_t)dim * row + 1] * gy[t];
+            if (dim == 3)
+                v += normal[(size_t)dim * row + 2] * gz[t];
+        }
+    } else {
+        v = diff * lap[t];
+        v += conv * gx[t];
+        v += conv * gy[t];
+        if (dim == 3)
+            v += conv * gz[t];
+        if (col == row)
+            v += unsteady;
+    }
+    vals[t] = v;
+}
+
+// ------------------------------------------------------------ host side
+static unsigned vec_blocks(int n) {
+    int b = (n + KT - 1) / KT;
+    int cap = sm_count() * 8;
+    return (unsigned)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+static unsigned slice_blocks(int nv) {
+    int ns = (nv + SLICE - 1) / SLICE;
+    return (unsigned)((ns + 7) / 8);
+}
+
+int Krylov::alloc(int nv_, int bordered_, bool mixed, bool external_pc) {
+    nv = nv_;
+    bordered = bordered_;
+    nsys = nv + (bordered ? 1 : 0);
+    const size_t n = nsys;
+    for (dbuf<double> *b : {&x, &b64, &r, &r0, &p, &v, &s, &t})
+        MP_TRY(b->alloc(n));
+    MP_TRY(y.alloc(n));
+    MP_TRY(z.alloc(n));
+    if (mixed) {
+        for (dbuf<float> *q : {&e32, &b32, &r32, &r032, &p32, &v32, &s32, &t32, &y32, &z32})
+            MP_TRY(q->alloc(n));
+        MP_TRY(res64.alloc(n));
+    }
+    (void)external_pc;
+    size_t maxb = slice_blocks(nv);
+    if (vec_blocks(nsys) > maxb)
+        maxb = vec_blocks(nsys);
+    MP_TRY(partials.alloc(4 * maxb + 64));
+    MP_TRY(ticket.alloc(4));
+    MP_TRY(scal.alloc(1));
+    MP_CUDA(cudaMemset(ticket.p, 0, 4 * sizeof(unsigned int)));
+    MP_CUDA(cudaMemset(scal.p, 0, sizeof(BicgScalars)));
+    return MP_OK;
+}
+
+// One BiCGSTAB sweep (everything after the prologue), issued on stream s.
+template <class T>
+static int issue_iteration(const PpeSystem &P, const EllView<T> &A, const T *dinv, T *x, T *b,
+                           T *r, T *r0, T *p, T *v, T *s_, T *t, T *y, T *z, BicgScalars *S,
+                           RedBuf R, int pk, cudaGraphConditionalHandle h, cudaStream_t st) {
+    const int nv = P.nv, nsys = P.nsys, bd = P.bordered;
+    T *yy = pk == PK_NONE ? p : y;
+    T *zz = pk == PK_NONE ? s_ : z;
+    k_restart<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, x, b, r, r0, S, R);
+    MP_CHECK_LAUNCH();
+    if (pk == PK_JACOBI)
+        k_update_p<T, PK_JACOBI><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S);
+    else if (pk == PK_NONE)
+        k_update_p<T, PK_NONE><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S);
+    else
+        k_update_p<T, PK_EXTERNAL><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S);
+    MP_CHECK_LAUNCH();
+    if (pk == PK_EXTERNAL)
+        MP_TRY(amg_apply<T>(*P.amg, p, yy, &S->done, st));
+    k_spmv_alpha<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, yy, v, r0, S, R);
+    MP_CHECK_LAUNCH();
+    if (pk == PK_JACOBI)
+        k_update_s<T, PK_JACOBI><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, S);
+    else if (pk == PK_NONE)
+        k_update_s<T, PK_NONE><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, S);
+    else
+        k_update_s<T, PK_EXTERNAL><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, S);
+    MP_CHECK_LAUNCH();
+    if (pk == PK_EXTERNAL)
+        MP_TRY(amg_apply<T>(*P.amg, s_, zz, &S->done, st));
+    k_spmv_omega<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, zz, t, s_, S, R);
+    MP_CHECK_LAUNCH();
+    k_update_xr<T><<<vec_blocks(nsys), KT, 0, st>>>(nsys, x, yy, zz, s_, t, r, r0, S, R, h);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+int Ppe::issue_prologue64(cudaGraphConditionalHandle h, cudaStream_t st) {
+    k_init<double, false><<<slice_blocks(sys.nv), KT, 0, st>>>(
+        sys.A.view64(), sys.bordered, W.x.p, W.b64.p, W.r.p, W.r0.p, W.p.p, W.v.p, W.scal.p,
+        RedBuf{W.partials.p, W.ticket.p}, cfg.tol, cfg.maxit, h);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+int Ppe::issue_sweep64(cudaGraphConditionalHandle h, cudaStream_t st) {
+    return issue_iteration<double>(sys, sys.A.view64(), sys.dinv.p, W.x.p, W.b64.p, W.r.p,
+                                   W.r0.p, W.p.p, W.v.p, W.s.p, W.t.p, W.y.p, W.z.p, W.scal.p,
+                                   RedBuf{W.partials.p, W.ticket.p}, pk(), h, st);
+}
+
+int Ppe::issue_epilogue64(cudaStream_t st) {
+    k_true_residual<<<slice_blocks(sys.nv), KT, 0, st>>>(sys.A.view64(), sys.bordered, W.x.p,
+                                                         W.b64.p, nullptr, W.scal.p,
+                                                         RedBuf{W.partials.p, W.ticket.p}, 0, 0);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+// mixed precision: outer residual (sets the refinement loop condition)
+int Ppe::issue_ir_residual(cudaGraphConditionalHandle h, cudaStream_t st) {
+    k_true_residual<<<slice_blocks(sys.nv), KT, 0, st>>>(sys.A.view64(), sys.bordered, W.x.p,
+                                                         W.b64.p, W.res64.p, W.scal.p,
+                                                         RedBuf{W.partials.p, W.ticket.p}, 1, h);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+int Ppe::issue_ir_inner_prologue(cudaGraphConditionalHandle h, cudaStream_t st) {
+    k_ir_scale<<<vec_blocks(sys.nsys), KT, 0, st>>>(sys.nsys, W.res64.p, W.b32.p, W.e32.p,
+                                                    W.scal.p);
+    MP_CHECK_LAUNCH();
+    // inner solve of A e = b32 from e = 0; BiCGSTAB's prologue skips the SpMV
+    k_init<float, true><<<slice_blocks(sys.nv), KT, 0, st>>>(
+        sys.A.view32(), sys.bordered, W.e32.p, W.b32.p, W.r32.p, W.r032.p, W.p32.p, W.v32.p,
+        W.scal.p, RedBuf{W.partials.p, W.ticket.p}, cfg.inner_tol, cfg.maxit, h);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+int Ppe::issue_ir_sweep(cudaGraphConditionalHandle h, cudaStream_t st) {
+    return issue_iteration<float>(sys, sys.A.view32(), sys.dinv32.p, W.e32.p, W.b32.p, W.r32.p,
+                                  W.r032.p, W.p32.p, W.v32.p, W.s32.p, W.t32.p, W.y32.p, W.z32.p,
+                                  W.scal.p, RedBuf{W.partials.p, W.ticket.p}, pk(), h, st);
+}
+
+int Ppe::issue_ir_update(cudaStream_t st) {
+    k_ir_update<<<vec_blocks(sys.nsys), KT, 0, st>>>(sys.nsys, W.x.p, W.e32.p, W.scal.p);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+// Set the refinement-loop constants before a mixed solve
+__global__ void k_ir_setup(BicgScalars *S, double tol, int outer_max) {
+    S->tol_outer2 = tol * tol;
+    S->outer_it = 0;
+    S->outer_max = outer_max;
+    S->total_inner = 0;
+    S->status = MP_OK;
+}
+
+int Ppe::issue_ir_setup(cudaStream_t st) {
+    k_ir_setup<<<1, 1, 0, st>>>(W.scal.p, cfg.tol, cfg.max_refine);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+// Build the whole solve (prologue, while loop(s), epilogue) into `gb`.
+int Ppe::build_solve_graph(GraphBuilder &gb) {
+    if (cfg.precision == MP_FP64) {
+        cudaGraphConditionalHandle h;
+        MP_TRY(gb.make_handle(&h));
+        MP_TRY(gb.captured([&](cudaStream_t s) { return issue_prologue64(h, s); }));
+        MP_TRY(gb.while_loop(h, [&](GraphBuilder &body) {
+            return body.captured([&](cudaStream_t s) { return issue_sweep64(h, s); });
+        }));
+        MP_TRY(gb.captured([&](cudaStream_t s) { return issue_epilogue64(s); }));
+        return MP_OK;
+    }
+    cudaGraphConditionalHandle ho, hi;
+    MP_TRY(gb.make_handle(&ho));
+    MP_TRY(gb.make_handle(&hi));
+    MP_TRY(gb.captured([&](cudaStream_t s) {
+        MP_TRY(issue_ir_setup(s));
+        return issue_ir_residual(ho, s);
+    }));
+    MP_TRY(gb.while_loop(ho, [&](GraphBuilder &outer) {
+        MP_TRY(outer.captured([&](cudaStream_t s) { return issue_ir_inner_prologue(hi, s); }));
+        MP_TRY(outer.while_loop(hi, [&](GraphBuilder &inner) {
+            return inner.captured([&](cudaStream_t s) { return issue_ir_sweep(hi, s); });
+        }));
+        return outer.captured([&](cudaStream_t s) {
+            MP_TRY(issue_ir_update(s));
+            return issue_ir_residual(ho, s);
+        });
+    }));
+    return MP_OK;
+}
+
+// Eager (no graph) solve: host polls the device scalars every `poll` sweeps.
+int Ppe::solve_eager(cudaStream_t st) {
+    const int poll = 8;
+    BicgScalars hs;
+    auto fetch = [&]() -> int {
+        MP_CUDA(cudaMemcpyAsync(&hs, W.scal.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
+        MP_CUDA(cudaStreamSynchronize(st));
+        return MP_OK;
+    };
+    if (cfg.precision == MP_FP64) {
+        MP_TRY(issue_prologue64(0, st));
+        for (int it = 0;; it++) {
+            if (it % poll == 0) {
+                MP_TRY(fetch());
+                if (hs.done)
+                    break;
+            }
+            MP_TRY(issue_sweep64(0, st));
+        }
+        return issue_epilogue64(st);
+    }
+    MP_TRY(issue_ir_setup(st));
+    MP_TRY(issue_ir_residual(0, st));
+    for (;;) {
+        MP_TRY(fetch());
+        if (hs.outer_done)
+            break;
+        MP_TRY(issue_ir_inner_prologue(0, st));
+        for (int it = 0;; it++) {
+            if (it % poll == 0) {
+                MP_TRY(fetch());
+                if (hs.done)
+                    break;
+            }
+            MP_TRY(issue_ir_sweep(0, st));
+        }
+        MP_TRY(issue_ir_update(st));
+        MP_TRY(issue_ir_residual(0, st));
+    }
+    return MP_OK;
+}
+
+int Ppe::solve_resident(cudaStream_t st, bool use_graph) {
+    if (use_graph) {
+        if (!graph.e) {
+            GraphBuilder gb;
+            MP_TRY(gb.init_root(cap_stream()));
+            int rc = build_solve_graph(gb);
+            if (rc != MP_OK) {
+                if (gb.g)
+                    cudaGraphDestroy(gb.g);
+                return rc;
+            }
+            MP_TRY(graph.instantiate(gb));
+        }
+        return graph.launch(st);
+    }
+    return solve_eager(st);
+}
+
+cudaStream_t Ppe::cap_stream() {
+    if (!capture_stream)
+        cudaStreamCreateWithFlags(&capture_stream, cudaStreamNonBlocking);
+    return capture_stream;
+}
+
+int Ppe::read_stats(cudaStream_t st, SolveStats *out) {
+    BicgScalars hs;
+    MP_CUDA(cudaMemcpyAsync(&hs, W.scal.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    MP_CUDA(cudaStreamSynchronize(st));
+    out->iters = cfg.precision == MP_FP64 ? hs.it : hs.total_inner;
+    out->outer = hs.outer_it;
+    out->abs_res = std::sqrt(hs.rr_true);
+    out->relres = hs.b64_sq > 0 ? std::sqrt(hs.rr_true / hs.b64_sq) : 0.0;
+    out->status = hs.status;
+    if (hs.status == MP_OK && out->relres > cfg.tol && hs.b64_sq > 0)
+        out->status = MP_NOT_CONVERGED;
+    if (hs.status == MP_OK && !std::isfinite(out->relres))
+        out->status = MP_NAN_DETECTED;
+    return MP_OK;
+}
+
+int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet,
+                const double *normal, double unsteady, double conv, double diff,
+                const mp_solver_cfg &cfg_in, cudaStream_t st) {
+    cfg = Cfg::from(cfg_in);
+    CloudView cv = cloud_view(c);
+    const int nv = cv.nv, K = cv.n, dim = cv.dim;
+    // solver.cpp:29-38: bordered unless a boundary node is Dirichlet
+    std::vector<uint8_t> hb(nv), hd(nv);
+    MP_CUDA(cudaMemcpy(hb.data(), boundary, nv, cudaMemcpyDefault));
+    MP_CUDA(cudaMemcpy(hd.data(), dirichlet, nv, cudaMemcpyDefault));
+    int bordered = 1;
+    for (int i = 0; i < nv; i++)
+        if (hb[i] && hd[i]) {
+            bordered = 0;
+            break;
+        }
+    sys.nv = nv;
+    sys.K = K;
+    sys.bordered = bordered;
+    sys.nsys = nv + bordered;
+    dbuf<uint8_t> db, dd;
+    dbuf<double> dn;
+    dbuf<int> bad;
+    MP_TRY(db.alloc(nv));
+    MP_TRY(dd.alloc(nv));
+    MP_TRY(dn.alloc((size_t)nv * dim));
+    MP_TRY(bad.alloc(1));
+    MP_CUDA(cudaMemcpyAsync(db.p, hb.data(), nv, cudaMemcpyHostToDevice, st));
+    MP_CUDA(cudaMemcpyAsync(dd.p, hd.data(), nv, cudaMemcpyHostToDevice, st));
+    MP_CUDA(cudaMemcpyAsync(dn.p, normal, sizeof(double) * nv * dim, cudaMemcpyDefault, st));
+    MP_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
+    // the system shares the cloud's stencil columns
+    shared_cols = cloud_cols(c);
+    sys.A.nrows = nv;
+    sys.A.ncols = sys.nsys;
+    sys.A.K = K;
+    const size_t tot = (size_t)ell_padded_rows(nv) * K;
+    MP_TRY(sys.A.cols.alloc(tot));
+    MP_CUDA(cudaMemcpyAsync(sys.A.cols.p, cv.cols, sizeof(int) * tot, cudaMemcpyDeviceToDevice, st));
+    MP_TRY(sys.A.v64.alloc(tot));
+    k_assemble_ppe<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(
+        nv, K, dim, cv.cols, cv.w[0], cv.w[1], cv.w[2], cv.w[3], db.p, dd.p, dn.p, unsteady, conv,
+        diff, sys.A.v64.p, bad.p);
+    MP_CHECK_LAUNCH();
+    int hbad = 0;
+    MP_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MP_CUDA(cudaStreamSynchronize(st));
+    if (hbad)
+        return fail(MP_BAD_ARG, "%d stencils do not start with their own node", hbad);
+    const bool mixed = cfg.precision == MP_FP32;
+    if (mixed)
+        MP_TRY(ell_make_fp32(sys.A, st));
+    MP_TRY(sys.dinv.alloc(nv));
+    if (mixed)
+        MP_TRY(sys.dinv32.alloc(nv));
+    k_jacobi_dinv<<<(nv + 255) / 256, 256, 0, st>>>(sys.A.view64(), sys.dinv.p,
+                                                   mixed ? sys.dinv32.p : nullptr);
+    MP_CHECK_LAUNCH();
+    if (cfg.precond == MP_PRECOND_AMG) {
+        MP_TRY(amg_create(&sys.amg, sys.A, cfg, mixed, st));
+    }
+    MP_TRY(W.alloc(nv, bordered, mixed, cfg.precond == MP_PRECOND_AMG));
+    MP_CUDA(cudaStreamSynchronize(st));
+    return MP_OK;
+}
+
+Ppe::~Ppe() {
+    graph.reset();
+    if (sys.amg)
+        amg_destroy(sys.amg);
+    if (capture_stream)
+        cudaStreamDestroy(capture_stream);
+}
+
+Cfg Cfg::from(const mp_solver_cfg &c) {
+    Cfg o;
+    o.tol = c.tol;
+    o.maxit = c.maxit;
+    o.precond = c.precond;
+    o.precision = c.precision;
+    o.guess = c.guess;
+    o.inner_tol = c.inner_tol > 0 ? c.inner_tol : 1e-5;
+    o.max_refine = 12;
+    o.amg_max_levels = c.amg_max_levels > 0 ? c.amg_max_levels : 12;
+    o.amg_coarse_size = c.amg_coarse_size > 0 ? c.amg_coarse_size : 256;
+    o.smoother_sweeps = c.smoother_sweeps > 0 ? c.smoother_sweeps : 1;
+    o.smoother_omega = c.smoother_omega > 0 ? c.smoother_omega : 0.7;
+    return o;
+}
+
+}  // namespace mp
+
+using namespace mp;
+
+extern "C" int mp_solver_cfg_default(mp_solver_cfg *c) {
+    if (!c)
+        return fail(MP_BAD_ARG, "null cfg");
+    c->tol = 1e-8;
+    c->maxit = 1000;
+    c->precond = MP_PRECOND_AMG;
+    c->precision = MP_FP64;
+    c->guess = MP_GUESS_PREVIOUS;
+    c->inner_tol = 1e-5;
+    c->amg_max_levels = 12;
+    c->amg_coarse_size = 256;
+    c->smoother_sweeps = 1;
+    c->smoother_omega = 0.7;
+    return MP_OK;
+}
+
+extern "C" int mp_ppe_create(mp_cloud c, const uint8_t *boundary, const uint8_t *dirichlet,
+                             const double *normal, double unsteady, double conv, double diff,
+                             const mp_solver_cfg *cfg, mp_ppe *out) {
+    if (!c || !boundary || !dirichlet || !normal || !cfg || !out)
+        return fail(MP_BAD_ARG, "mp_ppe_create: null argument");
+    if (cfg->tol <= 0 || cfg->maxit <= 0)
+        return fail(MP_BAD_ARG, "solver tolerance and maxit must be positive");
+    if (cfg->precision != MP_FP64 && cfg->precision != MP_FP32)
+        return fail(MP_BAD_ARG, "precision must be MP_FP64 or MP_FP32 (mixed)");
+    if (cfg->precond < MP_PRECOND_NONE || cfg->precond > MP_PRECOND_AMG)
+        return fail(MP_BAD_ARG, "unknown preconditioner %d", cfg->precond);
+    mp_ppe p = new mp_ppe_s;
+    int rc = p->P.create(c, boundary, dirichlet, normal, unsteady, conv, diff, *cfg, 0);
+    if (rc != MP_OK) {
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return MP_OK;
+}
+
+extern "C" int mp_ppe_system_size(mp_ppe p) { return p ? p->P.sys.nsys : -1; }
+
+extern "C" int mp_ppe_solve(mp_ppe p, const double *rhs, double *x_inout, int *iters,
+                            double *relres, double *abs_res, mp_stream s) {
+    if (!p || !rhs || !x_inout)
+        return fail(MP_BAD_ARG, "mp_ppe_solve: null argument");
+    cudaStream_t st = S(s);
+    Ppe &P = p->P;
+    const size_t n = P.sys.nsys;
+    MP_CUDA(cudaMemcpyAsync(P.W.b64.p, rhs, sizeof(double) * n, cudaMemcpyDefault, st));
+    if (P.cfg.guess == MP_GUESS_ZERO)
+        MP_CUDA(cudaMemsetAsync(P.W.x.p, 0, sizeof(double) * n, st));
+    else
+        MP_CUDA(cudaMemcpyAsync(P.W.x.p, x_inout, sizeof(double) * n, cudaMemcpyDefault, st));
+    MP_TRY(P.solve_resident(st, p->use_graph));
+    MP_CUDA(cudaMemcpyAsync(x_inout, P.W.x.p, sizeof(double) * n, cudaMemcpyDefault, st));
+    SolveStats ss;
+    MP_TRY(P.read_stats(st, &ss));
+    if (iters)
+        *iters = ss.iters;
+    if (relres)
+        *relres = ss.relres;
+    if (abs_res)
+        *abs_res = ss.abs_res;
+    if (ss.status == MP_NOT_CONVERGED)
+        return fail(MP_NOT_CONVERGED,
+                    "pressure solve did not converge in %d iterations, relative residual: %g",
+                    ss.iters, ss.relres);
+    if (ss.status != MP_OK)
+        return fail(ss.status, "pressure solve failed (status %d), relative residual: %g",
+                    ss.status, ss.relres);
+    return MP_OK;
+}
+
+extern "C" int mp_ppe_destroy(mp_ppe p) {
+    delete p;
+    return MP_OK;
+}

@@ -1,0 +1,70 @@
+// mp_ppe.cuh -- the pressure-solve handle (SOLVER for the pressure Poisson
+// equation) used by mp_ppe_* and by the fractional-step handle.
+#pragma once
+#include "mp_krylov.cuh"
+
+struct mp_cloud_s;
+
+namespace mp {
+
+struct Cfg {
+    double tol, inner_tol, smoother_omega;
+    int maxit, precond, precision, guess, max_refine, amg_max_levels, amg_coarse_size,
+        smoother_sweeps;
+    static Cfg from(const mp_solver_cfg &c);
+};
+
+struct SolveStats {
+    int iters = 0, outer = 0, status = MP_OK;
+    double relres = 0, abs_res = 0;
+};
+
+// Device vectors of one solve (FP64, and FP32 for mixed precision)
+struct Krylov {
+    int nv = 0, nsys = 0, bordered = 0;
+    dbuf<double> x, b64, r, r0, p, v, s, t, y, z, res64;
+    dbuf<float> e32, b32, r32, r032, p32, v32, s32, t32, y32, z32;
+    dbuf<double> partials;
+    dbuf<unsigned int> ticket;
+    dbuf<BicgScalars> scal;
+    int alloc(int nv, int bordered, bool mixed, bool external_pc);
+};
+
+struct Ppe {
+    Cfg cfg{};
+    PpeSystem sys;
+    Krylov W;
+    GraphExec graph;
+    std::shared_ptr<Ell> shared_cols;
+    cudaStream_t capture_stream = nullptr;
+    ~Ppe();
+    int create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet,
+               const double *normal, double unsteady, double conv, double diff,
+               const mp_solver_cfg &cfg, cudaStream_t st);
+    int pk() const {
+        return cfg.precond == MP_PRECOND_AMG ? PK_EXTERNAL
+                                             : (cfg.precond == MP_PRECOND_JACOBI ? PK_JACOBI : PK_NONE);
+    }
+    // kernel sequences (each can be issued eagerly or captured)
+    int issue_prologue64(cudaGraphConditionalHandle h, cudaStream_t st);
+    int issue_sweep64(cudaGraphConditionalHandle h, cudaStream_t st);
+    int issue_epilogue64(cudaStream_t st);
+    int issue_ir_setup(cudaStream_t st);
+    int issue_ir_residual(cudaGraphConditionalHandle h, cudaStream_t st);
+    int issue_ir_inner_prologue(cudaGraphConditionalHandle h, cudaStream_t st);
+    int issue_ir_sweep(cudaGraphConditionalHandle h, cudaStream_t st);
+    int issue_ir_update(cudaStream_t st);
+    int build_solve_graph(GraphBuilder &gb);
+    int solve_eager(cudaStream_t st);
+    // solve with W.b64 as rhs and W.x as initial guess / solution
+    int solve_resident(cudaStream_t st, bool use_graph);
+    int read_stats(cudaStream_t st, SolveStats *out);
+    cudaStream_t cap_stream();
+};
+
+}  // namespace mp
+
+struct mp_ppe_s {
+    mp::Ppe P;
+    bool use_graph = true;
+};

@@ -1,0 +1,382 @@
+"""Host-side mirror of the reference's solver interface over the C ABI.
+
+Same class names, arguments and error behaviour as the reference's
+header_files/class.hpp (PARAMETERS :58-94, POINTS :96-140, CLOUD :142-169,
+SOLVER :171-217, FRACTIONAL_STEP_1 :246-270); the numerics run in
+libmemphys_cuda.so.  Failures raise MemphysError, the counterpart of the
+reference's printf + throw bad_exception().
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import capi
+from .capi import check, ptr
+from .clouds import Cloud
+
+# solver_type strings (parameters.cpp:94-99): the reference's names select the
+# closest GPU configuration; the cuda_* names choose one explicitly.
+SOLVER_TYPES = {
+    "eigen_ilu_bicgstab": dict(precond=capi.MP_PRECOND_AMG, precision=capi.MP_FP64),
+    "hypre_ilu_gmres": dict(precond=capi.MP_PRECOND_AMG, precision=capi.MP_FP64),
+    "eigen_direct": dict(precond=capi.MP_PRECOND_AMG, precision=capi.MP_FP64),
+    "cuda_bicgstab_amg": dict(precond=capi.MP_PRECOND_AMG, precision=capi.MP_FP64),
+    "cuda_bicgstab_amg_mixed": dict(precond=capi.MP_PRECOND_AMG, precision=capi.MP_FP32),
+    "cuda_bicgstab_jacobi": dict(precond=capi.MP_PRECOND_JACOBI, precision=capi.MP_FP64),
+    "cuda_bicgstab_jacobi_mixed": dict(precond=capi.MP_PRECOND_JACOBI, precision=capi.MP_FP32),
+    "cuda_bicgstab": dict(precond=capi.MP_PRECOND_NONE, precision=capi.MP_FP64),
+}
+
+
+class PARAMETERS:
+    """parameters.cpp:27-130,217-267.  Reads the positional parameters CSV, or
+    takes the same fields as keyword arguments."""
+
+    FIELDS = ["poly_deg", "phs_deg", "cloud_size_multiplier", "nt", "Courant", "solver_type",
+              "steady_tolerance", "solver_tolerance", "euclid_precond_level_hypre", "gmres_kdim",
+              "precond_droptol", "n_iter"]
+
+    def __init__(self, parameter_file: str | None = None, dimension: int = 2, **kw):
+        vals = dict(poly_deg=3, phs_deg=3, cloud_size_multiplier=2.0, nt=1000, Courant=1.0,
+                    solver_type="cuda_bicgstab_amg", steady_tolerance=1e-5, solver_tolerance=1e-8,
+                    euclid_precond_level_hypre=50, gmres_kdim=20, precond_droptol=1e-4,
+                    n_iter=1000)
+        if parameter_file:
+            vals.update(self.read_calc_parameters(parameter_file))
+        vals.update(kw)
+        for k, v in vals.items():
+            setattr(self, k, v)
+        self.dimension = dimension
+        self.rho = -10.0  # class.hpp:74: must be set by the driver
+        self.mu = -10.0
+        self.dt = None
+        self.rel_res_log, self.abs_res_log, self.regul_alpha_log, self.n_iter_actual = [], [], [], []
+        self.verify_parameters()
+        self.calc_cloud_num_points()
+        self.calc_polynomial_term_exponents()
+
+    @classmethod
+    def read_calc_parameters(cls, path: str) -> dict:
+        """parameters.cpp:42-80: `name,value` lines in fixed order."""
+        out = {}
+        with open(path) as f:
+            lines = [ln.strip() for ln in f if ln.strip()]
+        for name, line in zip(cls.FIELDS, lines):
+            v = line.split(",", 1)[1].strip()
+            if name == "solver_type":
+                out[name] = v
+            elif name in ("poly_deg", "phs_deg", "nt", "euclid_precond_level_hypre", "gmres_kdim",
+                          "n_iter"):
+                out[name] = int(v)
+            else:
+                out[name] = float(v)
+        return out
+
+    def verify_parameters(self):
+        """parameters.cpp:82-120 (the mesh-file checks do not apply to in-memory clouds)."""
+        if self.poly_deg < 2 or self.poly_deg > 15:
+            raise capi.MemphysError(capi.MP_BAD_ARG, f"poly_deg should be in range [2, 15]; "
+                                                     f"current value: {self.poly_deg}")
+        if self.phs_deg not in (3, 5, 7, 9, 11):
+            raise capi.MemphysError(capi.MP_BAD_ARG, f"phs_deg should be 3, 5, 7, 9, or 11; "
+                                                     f"current value: {self.phs_deg}")
+        self.solver_type = self.solver_type.lower()
+        if self.solver_type not in SOLVER_TYPES and self.solver_type != "sor":
+            raise capi.MemphysError(capi.MP_BAD_ARG,
+                                    f"solver_type should be one of {sorted(SOLVER_TYPES)}; "
+                                    f"current value: {self.solver_type}")
+
+    def calc_cloud_num_points(self):
+        self.num_poly_terms = capi.lib().mp_num_poly_terms(self.dimension, self.poly_deg)
+        self.cloud_size = capi.lib().mp_cloud_size(self.dimension, self.poly_deg,
+                                                   self.cloud_size_multiplier)
+
+    def calc_polynomial_term_exponents(self):
+        e = np.zeros(self.num_poly_terms * self.dimension, np.int32)
+        check(capi.lib().mp_poly_exponents(self.dimension, self.poly_deg, ptr(e)),
+              "calc_polynomial_term_exponents")
+        self.polynomial_term_exponents = e.reshape(self.num_poly_terms, self.dimension)
+
+    def solver_cfg(self, **overrides) -> capi.SolverCfg:
+        st = SOLVER_TYPES.get(self.solver_type, SOLVER_TYPES["cuda_bicgstab_amg"])
+        kw = dict(tol=self.solver_tolerance, maxit=self.n_iter, **st)
+        kw.update(overrides)
+        return capi.solver_cfg(**kw)
+
+
+class POINTS:
+    """class.hpp:96-140 for an in-memory cloud (the gmsh reader is not ported)."""
+
+    def __init__(self, cloud: Cloud):
+        self.cloud = cloud
+        self.nv = cloud.nv
+        self.dim = cloud.dim
+        self.xyz = np.ascontiguousarray(cloud.xyz, np.float64)
+        self.boundary_flag = np.ascontiguousarray(cloud.boundary, np.uint8)
+        self.normal = np.ascontiguousarray(cloud.normal, np.float64)
+
+
+class CLOUD:
+    """CLOUD::CLOUD (cloud.cpp:29-48) on the GPU: stencils, weights, operators."""
+
+    def __init__(self, points: POINTS, parameters: PARAMETERS, compute_cond: bool = True,
+                 nb_col: np.ndarray | None = None):
+        self.points = points
+        h = C.c_void_p()
+        if nb_col is None:
+            rc = capi.lib().mp_cloud_create(ptr(points.xyz), ptr(points.boundary_flag), points.nv,
+                                            points.dim, parameters.phs_deg, parameters.poly_deg,
+                                            parameters.cloud_size_multiplier, int(compute_cond),
+                                            None, C.byref(h))
+        else:
+            nb = np.ascontiguousarray(nb_col, np.int32)
+            rc = capi.lib().mp_cloud_create_stencils(ptr(points.xyz), ptr(points.boundary_flag),
+                                                     points.nv, points.dim, ptr(nb), nb.shape[1],
+                                                     parameters.phs_deg, parameters.poly_deg,
+                                                     int(compute_cond), None, C.byref(h))
+        check(rc, "CLOUD")
+        self.handle = h
+        nv, n, dim = C.c_int(), C.c_int(), C.c_int()
+        check(capi.lib().mp_cloud_info(h, C.byref(nv), C.byref(n), C.byref(dim)))
+        self.nv, self.n, self.dim = nv.value, n.value, dim.value
+        self.compute_cond = compute_cond
+        self._ops = {}
+
+    def fetch(self):
+        """Copy out nb_points_row/col, grad_*_coeff, laplacian_coeff, cond_num_RBF."""
+        nv, n = self.nv, self.n
+        nb = np.zeros((nv, n), np.int32)
+        w = {k: np.zeros((nv, n)) for k in ("gx", "gy", "lap")}
+        if self.dim == 3:
+            w["gz"] = np.zeros((nv, n))
+        cond = np.zeros(nv) if self.compute_cond else None
+        check(capi.lib().mp_cloud_get(self.handle, ptr(nb), ptr(w["gx"]), ptr(w["gy"]),
+                                      ptr(w.get("gz")), ptr(w["lap"]), ptr(cond), None),
+              "mp_cloud_get")
+        self.nb_points_col = nb
+        self.nb_points_row = np.arange(nv + 1, dtype=np.int32) * n
+        self.grad_x_coeff, self.grad_y_coeff = w["gx"], w["gy"]
+        self.grad_z_coeff = w.get("gz")
+        self.laplacian_coeff = w["lap"]
+        if cond is not None:
+            self.cond_num_RBF = cond
+            self.cond_num_RBF_max = float(cond.max())
+            self.cond_num_RBF_min = float(cond.min())
+            self.cond_num_RBF_avg = float(cond.mean())
+        return self
+
+    def operator(self, which: int, rows: int = capi.MP_ROWS_ALL,
+                 precision: int = capi.MP_FP64) -> "Operator":
+        key = (which, rows, precision)
+        if key not in self._ops:
+            h = C.c_void_p()
+            check(capi.lib().mp_op_from_cloud(self.handle, which, rows, precision, C.byref(h)),
+                  "mp_op_from_cloud")
+            self._ops[key] = Operator(h, self.nv, self.nv, precision)
+        return self._ops[key]
+
+    def __del__(self):
+        try:
+            self._ops.clear()
+            if getattr(self, "handle", None):
+                capi.lib().mp_cloud_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+class Operator:
+    """An ELL operator handle (mp_op); `op @ x` mirrors `matrix * VectorXd`."""
+
+    def __init__(self, handle, nrows, ncols, precision):
+        self.handle, self.nrows, self.ncols, self.precision = handle, nrows, ncols, precision
+
+    @classmethod
+    def from_ell(cls, cols: np.ndarray, vals: np.ndarray, ncols: int | None = None,
+                 precision: int = capi.MP_FP64) -> "Operator":
+        cols = np.ascontiguousarray(cols, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        nrows, width = cols.shape
+        h = C.c_void_p()
+        check(capi.lib().mp_op_create_ell(nrows, ncols or nrows, width, ptr(cols), ptr(vals),
+                                          precision, C.byref(h)), "mp_op_create_ell")
+        return cls(h, nrows, ncols or nrows, precision)
+
+    def apply(self, x, y=None, alpha=1.0, beta=0.0, stream=None):
+        dt = np.float64 if self.precision == capi.MP_FP64 else np.float32
+        if y is None:
+            y = np.zeros(self.nrows, dt)
+        if isinstance(x, np.ndarray):
+            x = np.ascontiguousarray(x, dt)
+        check(capi.lib().mp_op_apply(self.handle, ptr(x), ptr(y), alpha, beta, stream),
+              "mp_op_apply")
+        return y
+
+    def __matmul__(self, x):
+        return self.apply(x)
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                capi.lib().mp_op_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+class SOLVER:
+    """SOLVER (solver.cpp): init() + general_solve() for the pressure operator."""
+
+    def init(self, points: POINTS, cloud: CLOUD, parameters: PARAMETERS, dirichlet_flag,
+             unsteady_term_coeff: float, conv_term_coeff: float, diff_term_coeff: float,
+             log_flag: bool = True, **cfg_overrides):
+        self.log_flag = log_flag
+        self.cfg = parameters.solver_cfg(**cfg_overrides)
+        self.dirichlet = np.ascontiguousarray(dirichlet_flag, np.uint8)
+        h = C.c_void_p()
+        check(capi.lib().mp_ppe_create(cloud.handle, ptr(points.boundary_flag), ptr(self.dirichlet),
+                                       ptr(points.normal), unsteady_term_coeff, conv_term_coeff,
+                                       diff_term_coeff, C.byref(self.cfg), C.byref(h)),
+              "SOLVER::init")
+        self.handle = h
+        self.system_size = capi.lib().mp_ppe_system_size(h)
+        self.nv = points.nv
+        return self
+
+    def general_solve(self, points, parameters, field_new, field_old, rhs):
+        """solver.cpp:283-363: field_new = solve(rhs) from field_old; logs into parameters;
+        the regularisation alpha is copied back into field_old (:361-362)."""
+        x = np.array(field_old, np.float64, copy=True)
+        b = np.ascontiguousarray(rhs, np.float64)
+        it, rr, ar = C.c_int(), C.c_double(), C.c_double()
+        rc = capi.lib().mp_ppe_solve(self.handle, ptr(b), ptr(x), C.byref(it), C.byref(rr),
+                                     C.byref(ar), None)
+        field_new[:] = x
+        if self.log_flag:
+            parameters.rel_res_log.append(rr.value)
+            parameters.abs_res_log.append(ar.value)
+            parameters.n_iter_actual.append(it.value)
+            if self.system_size == points.nv + 1:
+                parameters.regul_alpha_log.append(float(x[-1]))
+        if self.system_size == points.nv + 1:
+            field_old[self.system_size - 1] = x[-1]
+        check(rc, "SOLVER::general_solve")
+        return it.value, rr.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                capi.lib().mp_ppe_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+class FRACTIONAL_STEP_1:
+    """fractional_step_1.cpp: hat-velocity projection method on the GPU."""
+
+    def __init__(self, points: POINTS, cloud: CLOUD, parameters: PARAMETERS, u_dirichlet_flag,
+                 v_dirichlet_flag, p_dirichlet_flag, temporal_order: int,
+                 w_dirichlet_flag=None, use_graph: bool = True, **cfg_overrides):
+        self.dim = points.dim
+        self.nv = points.nv
+        self.use_graph = use_graph
+        self.flags = [np.ascontiguousarray(f, np.uint8) for f in
+                      (u_dirichlet_flag, v_dirichlet_flag,
+                       w_dirichlet_flag if w_dirichlet_flag is not None else u_dirichlet_flag,
+                       p_dirichlet_flag)]
+        self.cfg = capi.Fs1Cfg(parameters.rho, parameters.mu, parameters.dt or 0.0,
+                               temporal_order)
+        self.scfg = parameters.solver_cfg(**cfg_overrides)
+        h = C.c_void_p()
+        check(capi.lib().mp_fs1_create(cloud.handle, ptr(points.boundary_flag), ptr(points.normal),
+                                       ptr(self.flags[0]), ptr(self.flags[1]),
+                                       ptr(self.flags[2]) if self.dim == 3 else None,
+                                       ptr(self.flags[3]), C.byref(self.cfg), C.byref(self.scfg),
+                                       C.byref(h)), "FRACTIONAL_STEP_1")
+        self.handle = h
+        self.system_size = capi.lib().mp_fs1_system_size(h)
+        self.cloud = cloud  # keep the cloud alive as long as the step object
+
+    def _vec_ptrs(self, arrs):
+        return (C.c_void_p * self.dim)(*[ptr(a).value for a in arrs])
+
+    def set_state(self, vel, p, it=0):
+        vel = [np.ascontiguousarray(v, np.float64) for v in vel]
+        p = np.ascontiguousarray(p, np.float64)
+        check(capi.lib().mp_fs1_set_state(self.handle, self._vec_ptrs(vel), ptr(p), it, None),
+              "mp_fs1_set_state")
+
+    def get_state(self):
+        vel = [np.zeros(self.nv) for _ in range(self.dim)]
+        p = np.zeros(self.system_size)
+        check(capi.lib().mp_fs1_get_state(self.handle, self._vec_ptrs(vel), ptr(p), None),
+              "mp_fs1_get_state")
+        return vel, p
+
+    def step(self, nsteps=1, stream=None):
+        check(capi.lib().mp_fs1_step(self.handle, nsteps, int(self.use_graph), stream),
+              "mp_fs1_step")
+
+    def single_timestep_2d(self, points, cloud, parameters, u_new, v_new, p_new, u_old, v_old,
+                           p_old, it):
+        """fractional_step_1.cpp:52-63 with the reference's argument order."""
+        if len(p_new) != self.system_size:
+            raise capi.MemphysError(capi.MP_BAD_ARG, "p_new must have system_size entries")
+        vn = self._vec_ptrs([u_new, v_new])
+        vo = self._vec_ptrs([np.ascontiguousarray(u_old), np.ascontiguousarray(v_old)])
+        rc = capi.lib().mp_fs1_single_timestep(self.handle, vn, ptr(p_new), vo,
+                                               ptr(np.ascontiguousarray(p_old)), it, None)
+        iters, rr, ar, al = self.last_stats()
+        parameters.rel_res_log.append(rr)
+        parameters.abs_res_log.append(ar)
+        parameters.n_iter_actual.append(iters)
+        if self.system_size == self.nv + 1:
+            parameters.regul_alpha_log.append(al)
+            p_old[self.system_size - 1] = p_new[self.system_size - 1]
+        check(rc, "FRACTIONAL_STEP_1::single_timestep_2d")
+
+    def last_stats(self):
+        it, rr, ar, al = C.c_int(), C.c_double(), C.c_double(), C.c_double()
+        check(capi.lib().mp_fs1_last_stats(self.handle, C.byref(it), C.byref(rr), C.byref(ar),
+                                           C.byref(al)), "mp_fs1_last_stats")
+        return it.value, rr.value, ar.value, al.value
+
+    def log(self, first, count):
+        out = np.zeros((count, 4))
+        check(capi.lib().mp_fs1_log(self.handle, first, count, ptr(out)), "mp_fs1_log")
+        return out
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                capi.lib().mp_fs1_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+def cavity_setup(nx: int, solver_type="cuda_bicgstab_amg", dt=None, rho=1.0, mu=0.01,
+                 temporal_order=2, tol=1e-8, maxit=1000, seed=None, use_graph=True, **cfg):
+    """The lid-driven cavity of the benchmark configurations, ready to step."""
+    from . import clouds
+    cl = clouds.cavity_2d(nx) if seed is None else clouds.cavity_2d(nx, seed=seed)
+    prm = PARAMETERS(solver_type=solver_type, solver_tolerance=tol, n_iter=maxit)
+    prm.rho, prm.mu = rho, mu
+    prm.dt = dt if dt is not None else stable_dt(cl.h, mu / rho)
+    pts = POINTS(cl)
+    cld = CLOUD(pts, prm, compute_cond=False)
+    fs = FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet, cl.p_dirichlet,
+                           temporal_order, use_graph=use_graph, **cfg)
+    p0 = np.zeros(fs.system_size)
+    fs.set_state([cl.vel_bc[0], cl.vel_bc[1]], p0, 0)
+    return cl, prm, pts, cld, fs
+
+
+def stable_dt(h: float, nu: float, lid: float = 1.0, safety: float = 0.5) -> float:
+    """Explicit-step limit of the AB2 projection step used by the benchmark cavities:
+    min(0.5 h / u, 0.1 h^2 / nu) times `safety`; 1e-3 at the 100 x 100 cavity."""
+    return min(1e-3, safety * min(0.5 * h / lid, 0.1 * h * h / nu) * 2.0)
