@@ -1,0 +1,382 @@
+"""Benchmark: ms per fractional step of the 1,004,000-node lid-driven cavity.
+
+Workload (the plain-FP64 single-GPU configuration): unit-square cavity,
+1000 x 1000 interior nodes at ((i+1/2)h, (j+1/2)h) jittered by +/-0.2h
+(Philox seed 20261203) plus 4000 boundary nodes; PHS r^3 with a degree-3
+polynomial, 20-node stencils; operators ELL FP64 width 20; pressure by BiCGSTAB
+with the smoothed-aggregation multigrid preconditioner to ||r||/||b|| <= 1e-8;
+Re = 100 (rho 1, mu 0.01), Adams-Bashforth 2; dt from the reference's calc_dt
+rule with Courant 0.25 (the configured dt = 1e-3 is explicitly unstable on
+this cloud).  A "step" is one FRACTIONAL_STEP_1 timestep, graph-launched.
+
+Printed (rank 0, one JSON line): the plain FP64 ms/step as `value`
+(lower is better), the mixed-precision ms/step beside it, the end-to-end
+ms/step through mp_fs1_single_timestep with pinned host buffers, the SpMV
+roofline, and the CPU oracle baseline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--nx NX]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import signal
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=1000)
+    ap.add_argument("--courant", type=float, default=0.25)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    dev = "cuda" if torch.cuda.is_available() and pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p is not None:
+            self.p.send_signal(signal.SIGTERM)
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+        return False
+
+    def summary(self):
+        if self.p is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for ln in open(self.path):
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        j = json.load(open(p))
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per SpMV launch from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "spmv_fp64_cavity1m.md")
+    try:
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
+        return float(m.group(1)) if m else None
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------------- our arm
+def run_ours(args, ws, rank, local, pg):
+    from memphys_b200 import capi, clouds, meshless
+    L = capi.lib()
+    capi.check(L.mp_set_device(local), "mp_set_device")
+    capi.device_info()
+    nx = args.nx
+    cl = clouds.cavity_2d(nx)
+    nv = cl.nv
+    prm = meshless.PARAMETERS(solver_type="cuda_bicgstab_amg", solver_tolerance=1e-8, n_iter=2000)
+    prm.rho, prm.mu = 1.0, 0.01
+    pts = meshless.POINTS(cl)
+    t0 = time.time()
+    cld = meshless.CLOUD(pts, prm, compute_cond=False)
+    t_cloud = time.time() - t0
+    prm.dt = meshless.calc_dt(cld, 1.0, 1.0, 0.0, prm.mu / prm.rho, args.courant)
+    t0 = time.time()
+    fs = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                    cl.p_dirichlet, 2, use_graph=True)
+    t_setup = time.time() - t0
+    ns = fs.system_size
+    vel0 = [cl.vel_bc[0].copy(), cl.vel_bc[1].copy()]
+    p0 = np.zeros(ns)
+    stream = capi.Stream()
+
+    def timed_steps(f, K, W):
+        f.set_state(vel0, p0, 0)
+        for _ in range(W):
+            f.step(1, stream.handle)
+        stream.sync()
+        barrier(pg)
+        stream.sync()
+        with capi.Timer(stream.handle) as tm:
+            for _ in range(K):
+                f.step(1, stream.handle)
+        return tm.ms / K
+
+    # plain FP64 (headline)
+    with Clocks(local) as clk:
+        ms64 = timed_steps(fs, args.steps, args.warmup)
+    clocks = clk.summary()
+    log64 = fs.log(args.warmup, args.steps)
+    fixed, per_sweep, per_ref = (np.zeros(1, np.int32) for _ in range(3))
+    capi.check(L.mp_fs1_kernel_counts(fs.handle, capi.ptr(fixed), capi.ptr(per_sweep),
+                                      capi.ptr(per_ref)))
+    iters64 = log64[:, 0]
+    launches = int(args.steps * fixed[0] + iters64.sum() * per_sweep[0])
+    vel64, p64 = fs.get_state()
+    ms64_max = max_over_ranks(pg, ms64)
+
+    # mixed precision: FP32 BiCGSTAB + multigrid under FP64 iterative refinement
+    mixed = None
+    if not args.no_mixed:
+        fsm = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                         cl.p_dirichlet, 2, use_graph=True,
+                                         precision=capi.MP_FP32, inner_tol=1e-5)
+        msm = timed_steps(fsm, args.steps, args.warmup)
+        logm = fsm.log(args.warmup, args.steps)
+        velm, pm = fsm.get_state()
+        err = [float(np.abs(velm[d] - vel64[d]).max() / np.abs(vel64[d]).max()) for d in range(2)]
+        perr = float(np.abs((pm - p64)[:nv]).max() / np.abs(p64[:nv]).max())
+        mixed = {"ms_per_step": max_over_ranks(pg, msm),
+                 "inner_iters_per_step": float(np.mean(logm[:, 0] % 1e6)),
+                 "refinements_per_step": float(np.mean(logm[:, 0] // 1e6)),
+                 "max_relres": float(logm[:, 1].max()),
+                 "rel_err_vs_fp64": {"u": err[0], "v": err[1], "p": perr}}
+        del fsm
+
+    # end to end through the C ABI drop-in with pinned host buffers
+    u_h = capi.PinnedArray((nv,))
+    v_h = capi.PinnedArray((nv,))
+    p_h = capi.PinnedArray((ns,))
+    un_h = capi.PinnedArray((nv,))
+    vn_h = capi.PinnedArray((nv,))
+    pn_h = capi.PinnedArray((ns,))
+    u_h.array[:] = vel64[0]
+    v_h.array[:] = vel64[1]
+    p_h.array[:] = p64
+    import ctypes as C
+    vo = (C.c_void_p * 2)(u_h.ptr, v_h.ptr)
+    vn = (C.c_void_p * 2)(un_h.ptr, vn_h.ptr)
+    step0 = args.warmup + args.steps
+    barrier(pg)
+    with capi.Timer(stream.handle) as tm:
+        for k in range(args.steps):
+            capi.check(L.mp_fs1_single_timestep(fs.handle, vn if k % 2 == 0 else vo,
+                                                C.c_void_p(pn_h.ptr if k % 2 == 0 else p_h.ptr),
+                                                vo if k % 2 == 0 else vn,
+                                                C.c_void_p(p_h.ptr if k % 2 == 0 else pn_h.ptr),
+                                                step0 + k, stream.handle), "single_timestep")
+    e2e_ms = max_over_ranks(pg, tm.ms / args.steps)
+    e2e_bytes = (2 * nv + ns) * 8
+
+    # SpMV roofline: the FP64 Laplacian at this size, CUDA events on its stream
+    op = cld.operator(capi.MP_LAPLACIAN)
+    x = capi.DeviceArray.from_host(np.random.default_rng(0).standard_normal(nv))
+    y = capi.DeviceArray((nv,))
+    for _ in range(5):
+        op.apply(x, y, stream=stream.handle)
+    reps = 50
+    with capi.Timer(stream.handle) as tm:
+        for _ in range(reps):
+            op.apply(x, y, stream=stream.handle)
+    spmv_ms = tm.ms / reps
+    K = cld.n
+    alg_bytes = nv * (12 * K + 16)
+    achieved = alg_bytes / (spmv_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    out = {
+        "metric": "ms/fractional-step at 1M pts (learned+mixed vs plain FP64 GPU); SpMV HBM GB/s",
+        "value": round(ms64_max, 4), "unit": "ms/step", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms64_max, 4), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"cavity_2d {nx}x{nx} jittered + {4 * nx} boundary = {nv} nodes, "
+                               "plain FP64, BiCGSTAB + SA multigrid to 1e-8",
+                   "nodes": nv, "stencil": K, "phs": 3, "poly_deg": 3, "dt": prm.dt,
+                   "courant": args.courant, "re": 100, "temporal_order": 2,
+                   "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (ELL operators 257 MB, step working set > 1 GB)"},
+        "pressure_iters_per_step": float(iters64.mean()),
+        "max_relres": float(log64[:, 1].max()),
+        "mixed": mixed,
+        "spmv_gbs": round(achieved, 1),
+        "e2e": {"value": round(e2e_ms, 4), "unit": "ms/step", "h2d_bytes_per_step": e2e_bytes,
+                "d2h_bytes_per_step": e2e_bytes},
+        "roofline": {"kernel": "ell_spmv_kernel<double> (laplacian, width 20)", "bound": "hbm",
+                     "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": profile_traffic(), "algorithmic_bytes": alg_bytes,
+                     "launch_ms": round(spmv_ms, 5)},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "setup_s": {"cloud": round(t_cloud, 2), "fs1_and_multigrid": round(t_setup, 2)},
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(cl, cld)
+    return out
+
+
+def cpu_baseline(cl, cld, max_iters=40):
+    """The CPU oracle (C restatement of the reference's FS1 step with BiCGSTAB+ILUT),
+    one thread, one timestep of the same cloud with the pressure solve capped."""
+    import oracle
+    cld.fetch()
+    w = {"gx": cld.grad_x_coeff, "gy": cld.grad_y_coeff, "lap": cld.laplacian_coeff}
+    t0 = time.time()
+    f = oracle.FS1(cl, cld.nb_points_col, w, 1.0, 0.01, 1e-6, 2, 1e-8, max_iters, 1e-6, 50)
+    t_setup = time.time() - t0
+    vel = [cl.vel_bc[0].copy(), cl.vel_bc[1].copy()]
+    p = np.zeros(f.nsys)
+    t0 = time.time()
+    iters, rr = f.step(vel, p, 0)
+    dt = time.time() - t0
+    return {"value": round(dt * 1e3, 1), "unit": "ms/step", "cores": 1, "kind": "port",
+            "sample": f"1 timestep of the same {cl.nv}-node cavity; BiCGSTAB + ILUT(1e-6, 50) "
+                      f"capped at {max_iters} iterations ({iters} run, relres {rr:.1e}); "
+                      f"ILUT setup {t_setup:.1f} s excluded; a lower bound when the cap binds"}
+
+
+# ----------------------------------------------------------- reference arm
+def run_reference(args, ws, rank):
+    """The reference's CPU path (the oracle restatement: Eigen/HYPRE are not
+    installable here) timed on the host cores on a bounded sample per step."""
+    import oracle
+    from memphys_b200 import clouds
+    cl = clouds.cavity_2d(args.nx)
+    n = oracle.cloud_size(2, 3, 2.0)
+    t0 = time.time()
+    nb = oracle.knn_stencils(cl.xyz, cl.boundary, n)
+    w = parallel_weights(cl.xyz, nb)
+    t_setup = time.time() - t0
+    cap = 8
+    f = oracle.FS1(cl, nb, w, 1.0, 0.01, 1e-6, 2, 1e-8, cap, 1e-6, 50)
+    vel = [cl.vel_bc[0].copy(), cl.vel_bc[1].copy()]
+    p = np.zeros(f.nsys)
+    for it in range(args.warmup):
+        f.step(vel, p, it)
+    t0 = time.time()
+    for it in range(args.steps):
+        f.step(vel, p, args.warmup + it)
+    ms = (time.time() - t0) * 1e3 / args.steps
+    cores = os.cpu_count() or 1
+    sample = (f"{args.steps} timesteps of the {cl.nv}-node cavity, C restatement of "
+              f"FRACTIONAL_STEP_1 + BiCGSTAB/ILUT capped at {cap} iterations per step "
+              f"(a lower bound of a converged step); weights on {cores} threads "
+              f"({t_setup:.0f} s setup)")
+    return {"metric": "ms/fractional-step at 1M pts (learned+mixed vs plain FP64 GPU); SpMV HBM GB/s",
+            "impl": "reference", "value": round(ms, 2), "unit": "ms/step", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 2),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"cavity_2d {args.nx}x{args.nx} jittered, {cl.nv} nodes",
+                       "nodes": cl.nv, "stencil": n},
+            "cpu_baseline": {"value": round(ms, 2), "unit": "ms/step", "cores": 1, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(ms, 2), "unit": "ms/step", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def parallel_weights(xyz, nb):
+    """Oracle weights over stencil chunks on all host cores (ctypes releases the GIL)."""
+    import concurrent.futures as cf
+    import oracle
+    nthreads = max(1, os.cpu_count() or 1)
+    chunks = [c for c in np.array_split(np.arange(len(nb)), nthreads) if len(c)]
+    with cf.ThreadPoolExecutor(nthreads) as ex:
+        parts = list(ex.map(lambda c: oracle.cloud_weights(xyz, nb[c], 3, 3, cond=False), chunks))
+    # each chunk's stencils index the full cloud, so the rows are already global
+    return {k: np.concatenate([p[k] for p in parts]) for k in ("gx", "gy", "lap")}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        # rank 0 alone times the CPU path; other ranks exit without work
+        ws = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        if rank == 0:
+            print(json.dumps(run_reference(args, ws, rank)), flush=True)
+        return
+    ws, rank, local, pg = dist_setup(args)
+    out = run_ours(args, ws, rank, local, pg)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

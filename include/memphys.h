@@ -49,6 +49,7 @@ typedef void *mp_stream; /* a cudaStream_t; NULL is the legacy default stream */
 int mp_last_error(char *buf, size_t len);
 int mp_version(void);
 int mp_device_info(int *sm_count, int *cc_major, int *cc_minor, size_t *total_mem);
+int mp_set_device(int device); /* the calling host thread's current device */
 int mp_malloc(void **ptr, size_t bytes);
 int mp_free(void *ptr);
 int mp_malloc_host(void **ptr, size_t bytes); /* pinned */
@@ -235,6 +236,9 @@ int mp_fs1_last_stats(mp_fs1 f, int *iters, double *relres, double *abs_res, dou
  * iterations, relative residual, absolute residual, regularisation alpha); the
  * device keeps the last 4096 steps */
 int mp_fs1_log(mp_fs1 f, int first, int count, double *out);
+/* kernels in one graph step: `fixed` once per step, `per_sweep` per BiCGSTAB
+ * sweep, `per_refine` per iterative-refinement sweep (mixed precision) */
+int mp_fs1_kernel_counts(mp_fs1 f, int *fixed, int *per_sweep, int *per_refine);
 int mp_fs1_destroy(mp_fs1 f);
 
 #ifdef __cplusplus

@@ -29,7 +29,7 @@ STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "NAN_DETECTED",
 
 # every entry point declared in include/memphys.h
 EXPORTS = [
-    "mp_last_error", "mp_version", "mp_device_info", "mp_malloc", "mp_free", "mp_malloc_host",
+    "mp_last_error", "mp_version", "mp_device_info", "mp_set_device", "mp_malloc", "mp_free", "mp_malloc_host",
     "mp_free_host", "mp_memcpy", "mp_memset", "mp_stream_create", "mp_stream_destroy",
     "mp_stream_sync", "mp_timer_start", "mp_timer_stop", "mp_launch_count", "mp_num_poly_terms",
     "mp_cloud_size", "mp_poly_exponents", "mp_knn_stencils", "mp_stencil_weights",
@@ -38,7 +38,8 @@ EXPORTS = [
     "mp_op_apply_multi", "mp_op_info", "mp_op_destroy", "mp_solver_cfg_default", "mp_ppe_create",
     "mp_ppe_system_size", "mp_ppe_solve", "mp_ppe_destroy", "mp_fs1_create",
     "mp_fs1_system_size", "mp_fs1_set_state", "mp_fs1_get_state", "mp_fs1_step",
-    "mp_fs1_single_timestep", "mp_fs1_last_stats", "mp_fs1_log", "mp_fs1_destroy",
+    "mp_fs1_single_timestep", "mp_fs1_last_stats", "mp_fs1_log", "mp_fs1_kernel_counts",
+    "mp_fs1_destroy",
 ]
 
 
@@ -74,7 +75,7 @@ def lib() -> C.CDLL:
         sig = {
             "mp_last_error": [C.c_char_p, sz], "mp_version": [],
             "mp_device_info": [C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(sz)],
-            "mp_malloc": [C.POINTER(vp), sz], "mp_free": [vp],
+            "mp_set_device": [i], "mp_malloc": [C.POINTER(vp), sz], "mp_free": [vp],
             "mp_malloc_host": [C.POINTER(vp), sz], "mp_free_host": [vp],
             "mp_memcpy": [vp, vp, sz, vp], "mp_memset": [vp, i, sz, vp],
             "mp_stream_create": [C.POINTER(vp)], "mp_stream_destroy": [vp],
@@ -104,7 +105,9 @@ def lib() -> C.CDLL:
             "mp_fs1_get_state": [vp, vp, vp, vp], "mp_fs1_step": [vp, i, i, vp],
             "mp_fs1_single_timestep": [vp, vp, vp, vp, vp, i, vp],
             "mp_fs1_last_stats": [vp, C.POINTER(i), C.POINTER(d), C.POINTER(d), C.POINTER(d)],
-            "mp_fs1_log": [vp, i, i, vp], "mp_fs1_destroy": [vp],
+            "mp_fs1_log": [vp, i, i, vp],
+            "mp_fs1_kernel_counts": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)],
+            "mp_fs1_destroy": [vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)

@@ -15,6 +15,7 @@
 // same steps.  Each kernel streams the stencil indices once for all the
 // operators it applies.  With graphs enabled the whole step (including the
 // solver's device-controlled while loop) is a single graph launch.
+#include <cmath>
 #include "mp_cloud.cuh"
 #include "mp_ppe.cuh"
 
@@ -241,7 +242,8 @@ __global__ void k_step_log(int *step, const BicgScalars *S, double *log, int cap
                            int nv, int bordered, int mixed) {
     const int s = *step;
     double *e = log + 4 * (size_t)(s % cap);
-    e[0] = mixed ? S->total_inner : S->it;
+    // mixed precision: inner sweeps + 1e6 * refinement sweeps (decoded by the caller)
+    e[0] = mixed ? S->total_inner + 1.0e6 * S->outer_it : S->it;
     e[1] = S->b64_sq > 0 ? sqrt(S->rr_true / S->b64_sq) : 0.0;
     e[2] = sqrt(S->rr_true);
     e[3] = bordered ? x[nv] : 0.0;
@@ -266,6 +268,7 @@ struct mp_fs1_s {
     dbuf<double> log;
     int log_cap = 4096;
     GraphExec graph[2];
+    int kcounts[3] = {0, 0, 0};  // kernels per step / per sweep / per refinement sweep
     int cur = 0;
     int use_graph = 1;
 };
@@ -344,6 +347,8 @@ static int fs1_step_once(mp_fs1_s *f, bool graph, cudaStream_t s) {
         if (!G.e) {
             GraphBuilder gb;
             MP_TRY(gb.init_root(f->P.cap_stream()));
+            int counts[3] = {0, 0, 0};
+            gb.counts = counts;
             int rc = gb.captured([&](cudaStream_t cs) { return fs1_issue_pre(f, cur, cs); });
             if (rc == MP_OK)
                 rc = f->P.build_solve_graph(gb);
@@ -355,6 +360,8 @@ static int fs1_step_once(mp_fs1_s *f, bool graph, cudaStream_t s) {
                 return rc;
             }
             MP_TRY(G.instantiate(gb));
+            for (int q = 0; q < 3; q++)
+                f->kcounts[q] = counts[q];
         }
         MP_TRY(G.launch(s));
     } else {
@@ -537,7 +544,7 @@ extern "C" int mp_fs1_last_stats(mp_fs1 f, int *iters, double *relres, double *a
     MP_CUDA(cudaMemcpy(e, f->log.p + 4 * (size_t)((step - 1) % f->log_cap), sizeof(e),
                        cudaMemcpyDeviceToHost));
     if (iters)
-        *iters = (int)e[0];
+        *iters = (int)std::fmod(e[0], 1.0e6);
     if (relres)
         *relres = e[1];
     if (abs_res)
@@ -559,6 +566,20 @@ extern "C" int mp_fs1_log(mp_fs1 f, int first, int count, double *out) {
     for (int i = 0; i < count; i++)
         MP_CUDA(cudaMemcpy(out + 4 * (size_t)i, f->log.p + 4 * (size_t)((first + i) % f->log_cap),
                            4 * sizeof(double), cudaMemcpyDeviceToHost));
+    return MP_OK;
+}
+
+extern "C" int mp_fs1_kernel_counts(mp_fs1 f, int *fixed, int *per_sweep, int *per_refine) {
+    if (!f)
+        return fail(MP_BAD_ARG, "null fractional-step handle");
+    // FP64: fixed + iters * per_sweep; mixed: fixed + outer * per_refine + inner * per_sweep
+    const bool mixed = f->P.cfg.precision == MP_FP32;
+    if (fixed)
+        *fixed = f->kcounts[0];
+    if (per_sweep)
+        *per_sweep = mixed ? f->kcounts[2] : f->kcounts[1];
+    if (per_refine)
+        *per_refine = mixed ? f->kcounts[1] : 0;
     return MP_OK;
 }
 

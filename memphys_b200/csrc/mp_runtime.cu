@@ -25,6 +25,7 @@ int fail(int status, const char *fmt, ...) {
 }
 
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launch_counter() { return g_launches.load(std::memory_order_relaxed); }
 
 int sm_count() {
     static int cached[64] = {0};
@@ -86,6 +87,11 @@ int mp_device_info(int *sm, int *major, int *minor, size_t *total_mem) {
     if (p.major != 10)
         return fail(MP_NO_DEVICE, "device is sm_%d%d; this build runs on sm_100 (B200) only",
                     p.major, p.minor);
+    return MP_OK;
+}
+
+int mp_set_device(int device) {
+    MP_CUDA(cudaSetDevice(device));
     return MP_OK;
 }
 
@@ -192,7 +198,8 @@ int mp_num_poly_terms(int dim, int poly_deg) {
         return (int)(0.5 * (poly_deg + 1) * (poly_deg + 2));
     if (dim == 3)
         return (poly_deg + 1) * (poly_deg + 2) * (poly_deg + 3) / 6;
-    return fail(-MP_BAD_ARG, "dimension must be 2 or 3"), -1;
+    fail(MP_BAD_ARG, "dimension must be 2 or 3");
+    return -1;
 }
 
 int mp_cloud_size(int dim, int poly_deg, double mult) {

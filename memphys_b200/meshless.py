@@ -376,6 +376,38 @@ def cavity_setup(nx: int, solver_type="cuda_bicgstab_amg", dt=None, rho=1.0, mu=
     return cl, prm, pts, cld, fs
 
 
+def largest_eig_magnitude(op: "Operator", iters: int = 60, seed: int = 1) -> float:
+    """|lambda_max| of an operator by power iteration on the GPU (SpMV through the C ABI).
+    Stands in for the Arnoldi eigensolve of general_functions.cpp:4-24; the ratio
+    ||A^2 x|| / ||x|| is used so that a complex-conjugate dominant pair converges too."""
+    n = op.nrows
+    x = np.random.default_rng(seed).random(n) + 0.5
+    dx = capi.DeviceArray.from_host(x / np.linalg.norm(x))
+    dy = capi.DeviceArray((n,))
+    lam = 0.0
+    for _ in range(iters):
+        op.apply(dx, dy)
+        op.apply(dy, dx)
+        v = dx.to_host()
+        nv2 = np.linalg.norm(v)
+        if nv2 == 0 or not np.isfinite(nv2):
+            break
+        lam = np.sqrt(nv2)
+        dx.upload(v / nv2)
+    return float(lam)
+
+
+def calc_dt(cloud: CLOUD, u0: float, v0: float, w0: float, alpha: float, courant: float) -> float:
+    """PARAMETERS::calc_dt (parameters.cpp:269-296): dt = Courant * 2 /
+    (u0|l_x| + v0|l_y| [+ w0|l_z|] + alpha|l_L|) from the largest-magnitude eigenvalues."""
+    ev = u0 * largest_eig_magnitude(cloud.operator(capi.MP_GRAD_X))
+    ev += v0 * largest_eig_magnitude(cloud.operator(capi.MP_GRAD_Y))
+    if cloud.dim == 3:
+        ev += w0 * largest_eig_magnitude(cloud.operator(capi.MP_GRAD_Z))
+    ev += alpha * largest_eig_magnitude(cloud.operator(capi.MP_LAPLACIAN))
+    return courant * 2.0 / ev
+
+
 def stable_dt(h: float, nu: float, lid: float = 1.0, safety: float = 0.5) -> float:
     """Explicit-step limit of the AB2 projection step used by the benchmark cavities:
     min(0.5 h / u, 0.1 h^2 / nu) times `safety`; 1e-3 at the 100 x 100 cavity."""

@@ -138,9 +138,11 @@ def cloud_weights(xyz, nb_col, phs=3, poly_deg=3, cond=True):
     """cloud.cpp:207-279.  nb_col: (nv, n) stencils.  Returns dict of CSR-aligned
     (nv, n) arrays gx, gy, [gz], lap and per-node cond_est / cond_exact."""
     xyz = np.ascontiguousarray(xyz, np.float64)
-    nv, dim = xyz.shape
+    dim = xyz.shape[1]
     nb_col = np.ascontiguousarray(nb_col, np.int32)
-    n = nb_col.shape[1]
+    nv, n = nb_col.shape  # stencils to solve (may be a subset of the cloud's nodes)
+    if nb_col.size and (nb_col.min() < 0 or nb_col.max() >= xyz.shape[0]):
+        raise IndexError("stencil index outside the cloud")
     rp = (np.arange(nv + 1, dtype=np.int32) * n)
     gx, gy, lap = (np.zeros(nv * n) for _ in range(3))
     gz = np.zeros(nv * n) if dim == 3 else None

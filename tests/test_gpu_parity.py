@@ -1,0 +1,338 @@
+"""GPU parity: every kernel through the C ABI against the CPU oracle.
+
+Tolerances (relative, stated per check):
+  kNN stencils            exact (sets exact where the golden mesh has ties)
+  stencil weights         1e-9 normwise per stencil (condition ~1e4-1e6 x eps)
+  condition numbers       1e-9 vs the oracle's Eigen-rcond restatement
+  FP64 SpMV               1e-13 per row; FP32 SpMV 2e-6
+  pressure solve          ||b - A x|| / ||b|| <= tol recomputed in FP64 on the host
+  fractional step fields  1e-7 vs the direct-LU oracle after several steps
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as sla
+
+import oracle
+from oracle import fs1 as ofs1
+from memphys_b200 import capi, clouds, meshless
+from memphys_b200.capi import ptr
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_knn(xyz, bnd, n):
+    import ctypes as C
+    nv, dim = xyz.shape
+    out = np.zeros((nv, n), np.int32)
+    capi.check(capi.lib().mp_knn_stencils(ptr(np.ascontiguousarray(xyz)),
+                                          ptr(np.ascontiguousarray(bnd, np.uint8)), nv, dim, n,
+                                          ptr(out), None))
+    return out
+
+
+def gpu_weights(xyz, nb, phs=3, poly=3, cond=True):
+    nv, dim = xyz.shape
+    n = nb.shape[1]
+    w = {k: np.zeros((nv, n)) for k in ["gx", "gy", "lap"] + (["gz"] if dim == 3 else [])}
+    c = np.zeros(nv) if cond else None
+    capi.check(capi.lib().mp_stencil_weights(ptr(np.ascontiguousarray(xyz)), nv, dim,
+                                             ptr(np.ascontiguousarray(nb, np.int32)), n, phs, poly,
+                                             ptr(w["gx"]), ptr(w["gy"]), ptr(w.get("gz")),
+                                             ptr(w["lap"]), ptr(c), None))
+    if cond:
+        w["cond"] = c
+    return w
+
+
+def rowwise_rel(a, b):
+    return (np.abs(a - b).max(1) / np.maximum(np.abs(b).max(1), 1e-300)).max()
+
+
+@pytest.mark.parametrize("maker", [lambda: clouds.cavity_2d(40, seed=5),
+                                   lambda: clouds.cube_3d(8, seed=5),
+                                   lambda: clouds.channel_2d(0.05, seed=5)])
+def test_knn_matches_oracle(mp_lib, maker):
+    cl = maker()
+    n = oracle.cloud_size(cl.dim, 3, 2.0)
+    assert np.array_equal(gpu_knn(cl.xyz, cl.boundary, n),
+                          oracle.knn_stencils(cl.xyz, cl.boundary, n))
+
+
+def test_knn_matches_nanoflann_golden(mp_lib, golden_dir):
+    c = np.load(os.path.join(golden_dir, "knn_cavity.npz"))
+    assert np.array_equal(gpu_knn(c["xyz"], c["boundary"], 20), c["nb_col_nanoflann"])
+    g = np.load(os.path.join(golden_dir, "ecc_cloud.npz"))
+    nb = gpu_knn(g["xyz"], g["boundary"], 20)
+    assert all(set(a) == set(b) for a, b in zip(nb.tolist(), g["nb_col_nanoflann"].tolist()))
+
+
+@pytest.mark.parametrize("dim,phs", [(2, 3), (3, 3), (2, 5), (2, 7)])
+def test_weights_match_oracle(mp_lib, dim, phs):
+    cl = clouds.cavity_2d(30, seed=2) if dim == 2 else clouds.cube_3d(7, seed=2)
+    n = oracle.cloud_size(dim, 3, 2.0)
+    nb = oracle.knn_stencils(cl.xyz, cl.boundary, n)
+    ref = oracle.cloud_weights(cl.xyz, nb, phs, 3)
+    got = gpu_weights(cl.xyz, nb, phs, 3)
+    for k in ["gx", "gy", "lap"] + (["gz"] if dim == 3 else []):
+        assert rowwise_rel(got[k], ref[k]) <= 1e-9, k
+    assert np.abs(got["cond"] / ref["cond_est"] - 1).max() <= 1e-9
+
+
+def test_weights_higher_degree(mp_lib):
+    cl = clouds.cavity_2d(16, seed=4)
+    n = oracle.cloud_size(2, 4, 2.0)  # 30 nodes, 15 monomials: 45 x 45 systems
+    nb = oracle.knn_stencils(cl.xyz, cl.boundary, n)
+    ref = oracle.cloud_weights(cl.xyz, nb, 3, 4)
+    got = gpu_weights(cl.xyz, nb, 3, 4)
+    for k in ("gx", "gy", "lap"):
+        assert rowwise_rel(got[k], ref[k]) <= 1e-8, k
+
+
+def test_sample_statistics_on_gpu(mp_lib, golden_dir):
+    """The reference's sample-run statistics reproduced by the GPU path end to end."""
+    g = np.load(os.path.join(golden_dir, "ecc_cloud.npz"))
+    st = json.load(open(os.path.join(golden_dir, "sample_stats.json")))
+    cl = clouds.from_arrays("ecc", g["xyz"], g["boundary"], g["normal"])
+    prm = meshless.PARAMETERS(poly_deg=3, phs_deg=3, cloud_size_multiplier=2.0)
+    cld = meshless.CLOUD(meshless.POINTS(cl), prm, compute_cond=True).fetch()
+    assert cld.nv == st["nv"] and int(g["boundary"].sum()) == st["nv_boundary"]
+    assert cld.cond_num_RBF_max == pytest.approx(st["cond_max"], rel=1e-8)
+    assert cld.cond_num_RBF_min == pytest.approx(st["cond_min"], rel=1e-8)
+    assert cld.cond_num_RBF_avg == pytest.approx(st["cond_avg"], rel=1e-8)
+    nv, n = cld.nv, cld.n
+    rows = np.repeat(np.arange(nv), n)
+    for key, name in [("laplacian_coeff", "laplace_eig"), ("grad_x_coeff", "grad_x_eig")]:
+        A = sp.csr_matrix((getattr(cld, key).ravel(), (rows, cld.nb_points_col.ravel())),
+                          shape=(nv, nv))
+        ev = sla.eigs(A, k=1, which="LM", ncv=20, return_eigenvectors=False)[0]
+        assert ev.real == pytest.approx(st[name][0], rel=1e-7)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_batched_weights_match_lapack(mp_lib, golden_dir, dim):
+    L = np.load(os.path.join(golden_dir, "lapack_stencils.npz"))
+    sizes = L[f"sizes{dim}"].astype(np.int32)
+    off = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    pts = np.ascontiguousarray(L[f"pts{dim}"])
+    w = np.zeros((dim + 1) * int(sizes.sum()))
+    cond = np.zeros(len(sizes))
+    capi.check(capi.lib().mp_stencil_weights_batched(len(sizes), ptr(sizes), ptr(off), ptr(pts),
+                                                     dim, 3, 3, ptr(w), ptr(cond), None))
+    ref = L[f"w{dim}"]
+    _, cx, _ = oracle.batched_weights(sizes, off, pts, dim, cond=False)
+    for n, o in zip(sizes, off):
+        a = w[(dim + 1) * o:(dim + 1) * (o + n)]
+        b = ref[(dim + 1) * o:(dim + 1) * (o + n)]
+        assert np.abs(a - b).max() <= 1e-8 * np.abs(b).max()
+    # condition estimates agree with the oracle's rcond restatement
+    e = np.zeros(len(sizes))
+    for i, (n, o) in enumerate(zip(sizes, off)):
+        _, e[i], _ = oracle.stencil_single(pts[o:o + n], 3, 3)
+    assert np.abs(cond / e - 1).max() <= 1e-8
+
+
+def test_batched_uneven_sizes_one_call(mp_lib):
+    rng = np.random.default_rng(11)
+    sizes = rng.choice([20, 30, 40, 60], size=500).astype(np.int32)
+    off = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    pts = []
+    for n in sizes:
+        d = rng.normal(size=(n, 2))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        d *= rng.uniform(0, 1, size=(n, 1)) ** 0.5
+        d[0] = 0
+        pts.append(d * rng.uniform(1e-3, 1e-2))
+    pts = np.ascontiguousarray(np.concatenate(pts))
+    w = np.zeros(3 * int(sizes.sum()))
+    capi.check(capi.lib().mp_stencil_weights_batched(len(sizes), ptr(sizes), ptr(off), ptr(pts), 2,
+                                                     3, 3, ptr(w), None, None))
+    ref, _, bad = oracle.batched_weights(sizes, off, pts, 2)
+    assert bad == 0
+    for n, o in zip(sizes, off):
+        a, b = w[3 * o:3 * (o + n)], ref[3 * o:3 * (o + n)]
+        assert np.abs(a - b).max() <= 1e-8 * np.abs(b).max()
+
+
+@pytest.fixture(scope="module")
+def cav(mp_lib):
+    cl = clouds.cavity_2d(48, seed=9)
+    prm = meshless.PARAMETERS()
+    pts = meshless.POINTS(cl)
+    cld = meshless.CLOUD(pts, prm, compute_cond=False).fetch()
+    return cl, prm, pts, cld
+
+
+def csr_of(cld, coeff, rows_mask=None):
+    nv, n = cld.nv, cld.n
+    v = coeff.copy()
+    if rows_mask is not None:
+        v[~rows_mask] = 0.0
+    return sp.csr_matrix((v.ravel(), (np.repeat(np.arange(nv), n), cld.nb_points_col.ravel())),
+                         shape=(nv, nv))
+
+
+def test_cloud_matches_oracle(cav):
+    cl, prm, pts, cld = cav
+    nb = oracle.knn_stencils(cl.xyz, cl.boundary, 20)
+    assert np.array_equal(cld.nb_points_col, nb)
+    ref = oracle.cloud_weights(cl.xyz, nb, 3, 3, cond=False)
+    assert rowwise_rel(cld.grad_x_coeff, ref["gx"]) <= 1e-9
+    assert rowwise_rel(cld.laplacian_coeff, ref["lap"]) <= 1e-9
+
+
+@pytest.mark.parametrize("which,key", [(capi.MP_GRAD_X, "grad_x_coeff"),
+                                       (capi.MP_GRAD_Y, "grad_y_coeff"),
+                                       (capi.MP_LAPLACIAN, "laplacian_coeff")])
+@pytest.mark.parametrize("rows", [capi.MP_ROWS_ALL, capi.MP_ROWS_INTERNAL, capi.MP_ROWS_BOUNDARY])
+def test_spmv_fp64(cav, which, key, rows):
+    cl, prm, pts, cld = cav
+    mask = {capi.MP_ROWS_ALL: None, capi.MP_ROWS_INTERNAL: ~cl.boundary,
+            capi.MP_ROWS_BOUNDARY: cl.boundary}[rows]
+    A = csr_of(cld, getattr(cld, key), mask)
+    x = np.random.default_rng(1).standard_normal(cld.nv)
+    y = cld.operator(which, rows).apply(x)
+    ref = A @ x
+    scale = np.abs(A).max(1).toarray().ravel() * np.abs(x).max() * 20
+    assert np.all(np.abs(y - ref) <= 1e-13 * np.maximum(scale, 1e-300))
+
+
+def test_spmv_fp32_and_axpby(cav):
+    cl, prm, pts, cld = cav
+    A = csr_of(cld, cld.laplacian_coeff)
+    x = np.random.default_rng(2).standard_normal(cld.nv)
+    op32 = cld.operator(capi.MP_LAPLACIAN, precision=capi.MP_FP32)
+    y32 = op32.apply(x.astype(np.float32))
+    ref = A @ x
+    assert np.abs(y32 - ref).max() <= 2e-6 * np.abs(A).sum(1).max() * np.abs(x).max()
+    y0 = np.random.default_rng(3).standard_normal(cld.nv)
+    y = cld.operator(capi.MP_LAPLACIAN).apply(x, y0.copy(), alpha=2.0, beta=-0.5)
+    assert np.allclose(y, 2.0 * ref - 0.5 * y0, rtol=1e-12, atol=1e-9 * np.abs(ref).max())
+
+
+def test_spmv_multi_shares_indices(cav):
+    import ctypes as C
+    cl, prm, pts, cld = cav
+    ops = [cld.operator(w) for w in (capi.MP_GRAD_X, capi.MP_GRAD_Y, capi.MP_LAPLACIAN)]
+    x = np.random.default_rng(4).standard_normal(cld.nv)
+    dx = capi.DeviceArray.from_host(x)
+    outs = [capi.DeviceArray((cld.nv,)) for _ in ops]
+    harr = (C.c_void_p * 3)(*[o.handle.value for o in ops])
+    yarr = (C.c_void_p * 3)(*[o.ptr for o in outs])
+    capi.check(capi.lib().mp_op_apply_multi(3, harr, ptr(dx), yarr, None))
+    for o, key in zip(outs, ("grad_x_coeff", "grad_y_coeff", "laplacian_coeff")):
+        ref = csr_of(cld, getattr(cld, key)) @ x
+        assert np.abs(o.to_host() - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def ppe_direct(cl, cld):
+    w = {"gx": cld.grad_x_coeff, "gy": cld.grad_y_coeff, "lap": cld.laplacian_coeff}
+    rp, ci, val, ns = oracle.ppe_assemble(cld.nb_points_col, w, cl.boundary, cl.p_dirichlet,
+                                          cl.normal)
+    return sp.csr_matrix((val, ci, rp), shape=(ns, ns))
+
+
+@pytest.mark.parametrize("solver_type", ["cuda_bicgstab_amg", "cuda_bicgstab_jacobi",
+                                         "cuda_bicgstab_amg_mixed"])
+def test_pressure_solve(cav, solver_type):
+    cl, prm, pts, cld = cav
+    A = ppe_direct(cl, cld)
+    ns = A.shape[0]
+    b = np.random.default_rng(5).standard_normal(ns)
+    b[-1] = 0.0
+    p = meshless.PARAMETERS(solver_type=solver_type, solver_tolerance=1e-8, n_iter=4000)
+    s = meshless.SOLVER().init(pts, cld, p, cl.p_dirichlet, 0.0, 0.0, 1.0, True)
+    assert s.system_size == ns
+    x_old = np.zeros(ns)
+    x = np.zeros(ns)
+    it, rr = s.general_solve(pts, p, x, x_old, b)
+    true = np.linalg.norm(A @ x - b) / np.linalg.norm(b)
+    assert true <= 1e-8 and rr == pytest.approx(true, rel=1e-3)
+    xd = sla.spsolve(A.tocsc(), b)
+    assert np.linalg.norm(x - xd) <= 1e-4 * np.linalg.norm(xd)
+    assert p.n_iter_actual[-1] == it and x_old[-1] == x[-1]
+
+
+def run_fs1_pair(cl, dt, nsteps, solver_type="cuda_bicgstab_amg", tol=1e-11, use_graph=True):
+    prm = meshless.PARAMETERS(solver_type=solver_type, solver_tolerance=tol, n_iter=5000)
+    prm.rho, prm.mu, prm.dt = 1.0, 0.01, dt
+    pts = meshless.POINTS(cl)
+    cld = meshless.CLOUD(pts, prm, compute_cond=False).fetch()
+    fs = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                    cl.p_dirichlet, 2, w_dirichlet_flag=cl.w_dirichlet,
+                                    use_graph=use_graph)
+    w = {"gx": cld.grad_x_coeff, "gy": cld.grad_y_coeff, "lap": cld.laplacian_coeff}
+    if cl.dim == 3:
+        w["gz"] = cld.grad_z_coeff
+    ref = ofs1.FS1(cl, cld.nb_points_col, w, 1.0, 0.01, dt, 2)
+    vel = [cl.vel_bc[d].copy() for d in range(cl.dim)]
+    p = np.zeros(fs.system_size)
+    fs.set_state(vel, p, 0)
+    fs.step(nsteps)
+    for it in range(nsteps):
+        ref.step(vel, p, it)
+    gv, gp = fs.get_state()
+    log = fs.log(0, nsteps)
+    return gv, gp, vel, p, log
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_fs1_cavity_matches_oracle(mp_lib, use_graph):
+    cl = clouds.cavity_2d(32, seed=3)
+    gv, gp, rv, rp_, log = run_fs1_pair(cl, 2e-4, 8, use_graph=use_graph)
+    for d in range(2):
+        assert np.abs(gv[d] - rv[d]).max() <= 1e-7 * np.abs(rv[d]).max()
+    assert np.abs(gp - rp_).max() <= 1e-6 * np.abs(rp_).max()
+    assert np.all(log[:, 1] <= 1e-11)
+
+
+def test_fs1_mixed_precision_matches_fp64(mp_lib):
+    cl = clouds.cavity_2d(32, seed=3)
+    gv, gp, rv, rp_, log = run_fs1_pair(cl, 2e-4, 6, solver_type="cuda_bicgstab_amg_mixed",
+                                        tol=1e-10)
+    for d in range(2):
+        assert np.abs(gv[d] - rv[d]).max() <= 1e-7 * np.abs(rv[d]).max()
+    assert np.all(log[:, 1] <= 1e-10)
+
+
+def test_fs1_channel_with_outlet_and_neumann_velocity(mp_lib):
+    # p Dirichlet outlet (no border), u/v Neumann outlet rows (fractional_step_1.cpp:166-181)
+    cl = clouds.channel_2d(0.04, seed=1)
+    gv, gp, rv, rp_, log = run_fs1_pair(cl, 1e-4, 5)
+    assert len(gp) == cl.nv
+    for d in range(2):
+        assert np.abs(gv[d] - rv[d]).max() <= 1e-7 * max(np.abs(rv[d]).max(), 1e-12)
+
+
+def test_fs1_3d_matches_oracle(mp_lib):
+    cl = clouds.cube_3d(7, seed=2)
+    gv, gp, rv, rp_, log = run_fs1_pair(cl, 2e-4, 3)
+    for d in range(3):
+        assert np.abs(gv[d] - rv[d]).max() <= 1e-7 * max(np.abs(rv[d]).max(), 1e-12)
+
+
+def test_single_timestep_drop_in(mp_lib):
+    """FRACTIONAL_STEP_1::single_timestep_2d with the reference's argument order."""
+    cl = clouds.cavity_2d(24, seed=8)
+    prm = meshless.PARAMETERS(solver_type="cuda_bicgstab_amg", solver_tolerance=1e-10)
+    prm.rho, prm.mu, prm.dt = 1.0, 0.01, 2e-4
+    pts = meshless.POINTS(cl)
+    cld = meshless.CLOUD(pts, prm, compute_cond=False).fetch()
+    fs = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                    cl.p_dirichlet, 2)
+    w = {"gx": cld.grad_x_coeff, "gy": cld.grad_y_coeff, "lap": cld.laplacian_coeff}
+    ref = ofs1.FS1(cl, cld.nb_points_col, w, 1.0, 0.01, 2e-4, 2)
+    u_old, v_old = cl.vel_bc[0].copy(), cl.vel_bc[1].copy()
+    p_old = np.zeros(fs.system_size)
+    rv = [u_old.copy(), v_old.copy()]
+    rp_ = p_old.copy()
+    for it in range(4):
+        u_new, v_new, p_new = np.zeros(cl.nv), np.zeros(cl.nv), np.zeros(fs.system_size)
+        fs.single_timestep_2d(pts, cld, prm, u_new, v_new, p_new, u_old, v_old, p_old, it)
+        ref.step(rv, rp_, it)
+        u_old, v_old, p_old = u_new, v_new, p_new
+    assert np.abs(u_old - rv[0]).max() <= 1e-7 * np.abs(rv[0]).max()
+    assert len(prm.rel_res_log) == 4 and max(prm.rel_res_log) <= 1e-10
