@@ -45,6 +45,13 @@ def parse():
     ap.add_argument("--courant", type=float, default=0.25)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch the step's kernels one by one instead of as a CUDA graph")
+    ap.add_argument("--inner-tol", type=float, default=1e-5,
+                    help="mixed precision: relative reduction of each FP32 refinement solve")
+    ap.add_argument("--profile", default=None, choices=["steps", "spmv"],
+                    help="set up, warm up, then run `--steps` steps (or SpMV launches) inside a "
+                         "profiler capture range and exit (for ncu --profile-from-start off)")
     return ap.parse_args()
 
 
@@ -167,12 +174,14 @@ def run_ours(args, ws, rank, local, pg):
     prm.dt = meshless.calc_dt(cld, 1.0, 1.0, 0.0, prm.mu / prm.rho, args.courant)
     t0 = time.time()
     fs = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
-                                    cl.p_dirichlet, 2, use_graph=True)
+                                    cl.p_dirichlet, 2, use_graph=not args.no_graph)
     t_setup = time.time() - t0
     ns = fs.system_size
     vel0 = [cl.vel_bc[0].copy(), cl.vel_bc[1].copy()]
     p0 = np.zeros(ns)
     stream = capi.Stream()
+    if args.profile:
+        return profile_range(args, cld, fs, vel0, p0, stream)
 
     def timed_steps(f, K, W):
         f.set_state(vel0, p0, 0)
@@ -191,11 +200,12 @@ def run_ours(args, ws, rank, local, pg):
         ms64 = timed_steps(fs, args.steps, args.warmup)
     clocks = clk.summary()
     log64 = fs.log(args.warmup, args.steps)
-    fixed, per_sweep, per_ref = (np.zeros(1, np.int32) for _ in range(3))
-    capi.check(L.mp_fs1_kernel_counts(fs.handle, capi.ptr(fixed), capi.ptr(per_sweep),
-                                      capi.ptr(per_ref)))
+    import ctypes as C
+    fixed, per_sweep, per_ref = C.c_int(), C.c_int(), C.c_int()
+    capi.check(L.mp_fs1_kernel_counts(fs.handle, C.byref(fixed), C.byref(per_sweep),
+                                      C.byref(per_ref)), "mp_fs1_kernel_counts")
     iters64 = log64[:, 0]
-    launches = int(args.steps * fixed[0] + iters64.sum() * per_sweep[0])
+    launches = int(args.steps * fixed.value + iters64.sum() * per_sweep.value)
     vel64, p64 = fs.get_state()
     ms64_max = max_over_ranks(pg, ms64)
 
@@ -203,8 +213,8 @@ def run_ours(args, ws, rank, local, pg):
     mixed = None
     if not args.no_mixed:
         fsm = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
-                                         cl.p_dirichlet, 2, use_graph=True,
-                                         precision=capi.MP_FP32, inner_tol=1e-5)
+                                         cl.p_dirichlet, 2, use_graph=not args.no_graph,
+                                         precision=capi.MP_FP32, inner_tol=args.inner_tol)
         msm = timed_steps(fsm, args.steps, args.warmup)
         logm = fsm.log(args.warmup, args.steps)
         velm, pm = fsm.get_state()
@@ -227,7 +237,6 @@ def run_ours(args, ws, rank, local, pg):
     u_h.array[:] = vel64[0]
     v_h.array[:] = vel64[1]
     p_h.array[:] = p64
-    import ctypes as C
     vo = (C.c_void_p * 2)(u_h.ptr, v_h.ptr)
     vn = (C.c_void_p * 2)(un_h.ptr, vn_h.ptr)
     step0 = args.warmup + args.steps
@@ -286,6 +295,35 @@ def run_ours(args, ws, rank, local, pg):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(cl, cld)
     return out
+
+
+def profile_range(args, cld, fs, vel0, p0, stream):
+    """Warm-up outside, `--steps` steps (or SpMV launches) inside the capture range."""
+    from memphys_b200 import capi
+    L = capi.lib()
+    if args.profile == "steps":
+        fs.set_state(vel0, p0, 0)
+        fs.step(args.warmup, stream.handle)
+        stream.sync()
+        capi.check(L.mp_profiler(1))
+        fs.step(args.steps, stream.handle)
+        stream.sync()
+        capi.check(L.mp_profiler(0))
+        log = fs.log(args.warmup, args.steps)
+        return {"profile": "steps", "iters": log[:, 0].tolist()}
+    op = cld.operator(capi.MP_LAPLACIAN)
+    nv = cld.nv
+    x = capi.DeviceArray.from_host(np.random.default_rng(0).standard_normal(nv))
+    y = capi.DeviceArray((nv,))
+    for _ in range(args.warmup):
+        op.apply(x, y, stream=stream.handle)
+    stream.sync()
+    capi.check(L.mp_profiler(1))
+    for _ in range(args.steps):
+        op.apply(x, y, stream=stream.handle)
+    stream.sync()
+    capi.check(L.mp_profiler(0))
+    return {"profile": "spmv", "launches": args.steps, "nodes": nv}
 
 
 def cpu_baseline(cl, cld, max_iters=40):

@@ -62,6 +62,8 @@ int mp_stream_sync(mp_stream s);
 /* CUDA-event timer on a stream: mp_timer_start / mp_timer_stop -> milliseconds */
 int mp_timer_start(mp_stream s, void **timer);
 int mp_timer_stop(void *timer, mp_stream s, double *ms);
+/* start (on != 0) / stop the profiler's capture range (cudaProfilerStart/Stop) */
+int mp_profiler(int on);
 /* launches of this library's kernels since the last reset (process-wide counter) */
 int mp_launch_count(int64_t *count, int reset);
 

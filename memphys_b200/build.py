@@ -70,7 +70,25 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
+    build_host_driver(force)
     return LIB
+
+
+DRIVER_SRC = os.path.join(HERE, "host", "cavity_driver.cpp")
+DRIVER = os.path.join(HERE, "host", "cavity_driver")
+
+
+def build_host_driver(force: bool = False) -> str:
+    """The C++ example driver over the C ABI (host code only: g++ and the .so)."""
+    deps = [DRIVER_SRC, os.path.join(HERE, "host", "memphys.hpp"), LIB]
+    if force or not os.path.exists(DRIVER) or os.path.getmtime(DRIVER) < max(
+            os.path.getmtime(d) for d in deps):
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", DRIVER_SRC, "-o", DRIVER,
+               "-L" + HERE, "-lmemphys_cuda", "-Wl,-rpath,$ORIGIN/.."]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"host driver build failed:\n{r.stderr}")
+    return DRIVER
 
 
 if __name__ == "__main__":

@@ -31,7 +31,7 @@ STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "NAN_DETECTED",
 EXPORTS = [
     "mp_last_error", "mp_version", "mp_device_info", "mp_set_device", "mp_malloc", "mp_free", "mp_malloc_host",
     "mp_free_host", "mp_memcpy", "mp_memset", "mp_stream_create", "mp_stream_destroy",
-    "mp_stream_sync", "mp_timer_start", "mp_timer_stop", "mp_launch_count", "mp_num_poly_terms",
+    "mp_stream_sync", "mp_timer_start", "mp_timer_stop", "mp_profiler", "mp_launch_count", "mp_num_poly_terms",
     "mp_cloud_size", "mp_poly_exponents", "mp_knn_stencils", "mp_stencil_weights",
     "mp_stencil_weights_batched", "mp_cloud_create", "mp_cloud_create_stencils", "mp_cloud_info",
     "mp_cloud_get", "mp_cloud_destroy", "mp_op_create_ell", "mp_op_from_cloud", "mp_op_apply",
@@ -81,7 +81,7 @@ def lib() -> C.CDLL:
             "mp_stream_create": [C.POINTER(vp)], "mp_stream_destroy": [vp],
             "mp_stream_sync": [vp], "mp_timer_start": [vp, C.POINTER(vp)],
             "mp_timer_stop": [vp, vp, C.POINTER(d)],
-            "mp_launch_count": [C.POINTER(C.c_int64), i],
+            "mp_profiler": [i], "mp_launch_count": [C.POINTER(C.c_int64), i],
             "mp_num_poly_terms": [i, i], "mp_cloud_size": [i, i, d], "mp_poly_exponents": [i, i, vp],
             "mp_knn_stencils": [vp, vp, i, i, i, vp, vp],
             "mp_stencil_weights": [vp, i, i, vp, i, i, i, vp, vp, vp, vp, vp, vp],
@@ -130,7 +130,8 @@ def check(rc: int, what: str = "") -> int:
 
 
 def ptr(a) -> C.c_void_p | None:
-    """Address of a numpy array, a DeviceArray, or any object with data_ptr() (torch)."""
+    """Address of a numpy array, a DeviceArray, or any object with data_ptr() (torch).
+    The caller must keep the object referenced until the C call returns."""
     if a is None:
         return None
     if isinstance(a, np.ndarray):

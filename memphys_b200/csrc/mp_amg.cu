@@ -213,18 +213,27 @@ static void transpose(const Csr &A, Csr &T) {
         }
 }
 
-// CSR -> ELL slices on the device; padded entries: column `self ? row : 0`, value 0
+// CSR -> sliced ELL on the device, each 64-row slice as wide as its longest
+// row; padded entries: column `self ? row : 0`, value 0
 static int upload_ell(const Csr &C, Ell &E, bool self_pad, cudaStream_t s) {
-    int K = 1;
-    for (int i = 0; i < C.n; i++)
-        K = std::max(K, C.rp[i + 1] - C.rp[i]);
-    const int np = ell_padded_rows(C.n);
-    std::vector<int> cols((size_t)np * K);
-    std::vector<double> vals((size_t)np * K, 0.0);
-    for (int i = 0; i < np; i++) {
+    const int ns = (C.n + SLICE - 1) / SLICE;
+    std::vector<int> soff(ns + 1, 0);
+    int kmax = 1;
+    for (int sl = 0; sl < ns; sl++) {
+        int w = 1;
+        for (int i = sl * SLICE; i < std::min(C.n, (sl + 1) * SLICE); i++)
+            w = std::max(w, C.rp[i + 1] - C.rp[i]);
+        soff[sl + 1] = soff[sl] + w;
+        kmax = std::max(kmax, w);
+    }
+    const size_t tot = (size_t)soff[ns] * SLICE;
+    std::vector<int> cols(tot);
+    std::vector<double> vals(tot, 0.0);
+    for (int i = 0; i < ns * SLICE; i++) {
+        const int sl = i / SLICE, r = i % SLICE, w = soff[sl + 1] - soff[sl];
         const int len = i < C.n ? C.rp[i + 1] - C.rp[i] : 0;
-        for (int k = 0; k < K; k++) {
-            const size_t o = ell_index(i, k, K);
+        for (int k = 0; k < w; k++) {
+            const size_t o = (size_t)soff[sl] * SLICE + (size_t)k * SLICE + r;
             if (k < len) {
                 cols[o] = C.ci[C.rp[i] + k];
                 vals[o] = C.v[C.rp[i] + k];
@@ -235,11 +244,28 @@ static int upload_ell(const Csr &C, Ell &E, bool self_pad, cudaStream_t s) {
     }
     E.nrows = C.n;
     E.ncols = C.m;
-    E.K = K;
+    E.K = kmax;
     MP_TRY(E.cols.alloc(cols.size()));
     MP_TRY(E.v64.alloc(vals.size()));
+    MP_TRY(E.soff.alloc(soff.size()));
     MP_CUDA(cudaMemcpyAsync(E.cols.p, cols.data(), sizeof(int) * cols.size(), cudaMemcpyHostToDevice, s));
     MP_CUDA(cudaMemcpyAsync(E.v64.p, vals.data(), sizeof(double) * vals.size(), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaMemcpyAsync(E.soff.p, soff.data(), sizeof(int) * soff.size(), cudaMemcpyHostToDevice, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    return MP_OK;
+}
+
+static int upload_csr(const Csr &C, DCsr &D, cudaStream_t s) {
+    D.n = C.n;
+    D.m = C.m;
+    MP_TRY(D.rp.alloc(C.rp.size()));
+    MP_TRY(D.ci.alloc(std::max<size_t>(C.ci.size(), 1)));
+    MP_TRY(D.v64.alloc(std::max<size_t>(C.v.size(), 1)));
+    MP_CUDA(cudaMemcpyAsync(D.rp.p, C.rp.data(), sizeof(int) * C.rp.size(), cudaMemcpyHostToDevice, s));
+    if (!C.ci.empty()) {
+        MP_CUDA(cudaMemcpyAsync(D.ci.p, C.ci.data(), sizeof(int) * C.ci.size(), cudaMemcpyHostToDevice, s));
+        MP_CUDA(cudaMemcpyAsync(D.v64.p, C.v.data(), sizeof(double) * C.v.size(), cudaMemcpyHostToDevice, s));
+    }
     MP_CUDA(cudaStreamSynchronize(s));
     return MP_OK;
 }
@@ -308,6 +334,8 @@ Amg::~Amg() {
         delete l;
 }
 
+static int amg_autotune(Amg &a, cudaStream_t s);
+
 int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, bool mixed, cudaStream_t s) {
     auto t0 = std::chrono::steady_clock::now();
     const double theta = 0.25;
@@ -335,7 +363,7 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, bool mixed, cudaStream_
             L->A64 = A0.view64();
             L->A32 = A0.view32();
         } else {
-            if ((rc = upload_ell(A, L->A, true, s)) != MP_OK)
+            if ((rc = upload_ell(A, L->A, true, s)) != MP_OK || (rc = upload_csr(A, L->Ac, s)) != MP_OK)
                 return bail(rc);
             L->A64 = L->A.view64();
         }
@@ -392,7 +420,8 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, bool mixed, cudaStream_
                 spgemm(A, P, AP);
                 spgemm(R, AP, Ac);
                 if ((rc = upload_ell(P, L->P, false, s)) != MP_OK ||
-                    (rc = upload_ell(R, L->R, false, s)) != MP_OK)
+                    (rc = upload_ell(R, L->R, false, s)) != MP_OK ||
+                    (rc = upload_csr(P, L->Pc, s)) != MP_OK || (rc = upload_csr(R, L->Rc, s)) != MP_OK)
                     return bail(rc);
                 if (lev > 0) {
                     if ((rc = L->b.alloc(A.n)) != MP_OK || (rc = L->x.alloc(A.n)) != MP_OK)
@@ -428,6 +457,9 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, bool mixed, cudaStream_
             }
             if (L->P.v64.p && ((rc = ell_make_fp32(L->P, s)) != MP_OK || (rc = ell_make_fp32(L->R, s)) != MP_OK))
                 return bail(rc);
+            for (DCsr *D : {&L->Ac, &L->Pc, &L->Rc})
+                if (D->v64.p && (rc = make_f32(D->v64, D->v32, s)) != MP_OK)
+                    return bail(rc);
             if ((rc = make_f32(L->dinv, L->dinv32, s)) != MP_OK)
                 return bail(rc);
             for (auto pr : {std::make_pair(&L->b, &L->b32), std::make_pair(&L->x, &L->x32),
@@ -438,9 +470,24 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, bool mixed, cudaStream_
         if ((rc = make_f32(a->cinv, a->cinv32, s)) != MP_OK)
             return bail(rc);
     }
+    if ((rc = amg_autotune(*a, s)) != MP_OK)
+        return bail(rc);
     MP_CUDA(cudaStreamSynchronize(s));
     a->setup_seconds =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (getenv("MP_VERBOSE")) {
+        for (size_t l = 0; l < a->L.size(); l++) {
+            const AmgLevel &L = *a->L[l];
+            fprintf(stderr, "[memphys amg] level %zu n=%d A.K=%d", l, L.n, L.A64.K);
+            if (L.Ac.n)
+                fprintf(stderr, " A.nnz/row=%.1f", (double)L.Ac.ci.n / L.n);
+            if (L.Pc.n)
+                fprintf(stderr, " P.nnz/row=%.1f R.nnz/row=%.1f", (double)L.Pc.ci.n / L.Pc.n,
+                        (double)L.Rc.ci.n / L.Rc.n);
+            fprintf(stderr, " sched A=%d P=%d R=%d\n", L.sA.mode, L.sP.mode, L.sR.mode);
+        }
+        fprintf(stderr, "[memphys amg] coarse n=%d setup %.2f s\n", a->nc, a->setup_seconds);
+    }
     *out = a;
     return MP_OK;
 }
@@ -456,11 +503,14 @@ template <class T>
 __device__ __forceinline__ void spmv_pair(const EllView<T> &A, int w, int lane,
                                           const T *__restrict__ x, T &a0, T &a1) {
     using V2 = typename V2a<T>::type;
-    const size_t base = (size_t)w * A.K * SLICE + 2 * lane;
+    size_t base;
+    int K;
+    slice_span(A, w, base, K);
+    base += 2 * lane;
     a0 = 0;
     a1 = 0;
 #pragma unroll 4
-    for (int k = 0; k < A.K; k++) {
+    for (int k = 0; k < K; k++) {
         const size_t o = base + (size_t)k * SLICE;
         const int2 c = __ldcs(reinterpret_cast<const int2 *>(A.cols + o));
         const V2 v = __ldcs(reinterpret_cast<const V2 *>(A.vals + o));
@@ -478,14 +528,40 @@ struct ChebC {
     double inv_theta, theta, c1, c2, c3, c4;
 };
 
-// One fused SpMV + epilogue over the rows of M (warp per slice, 2 rows/lane):
+template <class T> struct CsrView {
+    int nrows;
+    const int *rp, *ci;
+    const T *v;
+};
+
+// Row i of one fused SpMV (a = (M u)_i) followed by its epilogue:
 //   EP_CHEB_PRE  : x = c1 d + c2 dinv (b - M d)            (u = d)
-//   EP_RESID     : r = b - M x                              (u = x)
+//   EP_RESID     : y = b - M x                              (u = x)
 //   EP_PLAIN     : y = M u
 //   EP_PROLONG   : x = x + M u                              (M = P, u = coarse x)
 //   EP_CHEB_POST1: d = dinv (b - M x) / theta               (u = x)
 //   EP_CHEB_POST2: x = x + (1 + c3) d + c4 (theta d - dinv M d)   (u = d)
 // No kernel writes the vector it gathers.
+template <class T, int EP>
+__device__ __forceinline__ void level_epilogue(int i, T a, const T *b, const T *dinv, T *d, T *x,
+                                               T *y, const ChebC &c) {
+    if (EP == EP_CHEB_PRE) {
+        x[i] = (T)c.c1 * d[i] + (T)c.c2 * dinv[i] * (b[i] - a);
+    } else if (EP == EP_RESID) {
+        y[i] = b[i] - a;
+    } else if (EP == EP_PLAIN) {
+        y[i] = a;
+    } else if (EP == EP_PROLONG) {
+        x[i] = x[i] + a;
+    } else if (EP == EP_CHEB_POST1) {
+        d[i] = dinv[i] * (b[i] - a) * (T)c.inv_theta;
+    } else {
+        const T di = d[i];
+        x[i] = x[i] + (T)(1.0 + c.c3) * di + (T)c.c4 * ((T)c.theta * di - dinv[i] * a);
+    }
+}
+
+// sliced ELL: one warp per 64-row slice, two rows per lane
 template <class T, int EP>
 __global__ void __launch_bounds__(256)
     k_level(EllView<T> M, const T *__restrict__ u, const T *__restrict__ b,
@@ -499,25 +575,31 @@ __global__ void __launch_bounds__(256)
     spmv_pair(M, w, lane, u, a[0], a[1]);
     const int i0 = w * SLICE + 2 * lane;
 #pragma unroll
-    for (int q = 0; q < 2; q++) {
-        const int i = i0 + q;
-        if (i >= M.nrows)
-            continue;
-        if (EP == EP_CHEB_PRE) {
-            x[i] = (T)c.c1 * d[i] + (T)c.c2 * dinv[i] * (b[i] - a[q]);
-        } else if (EP == EP_RESID) {
-            y[i] = b[i] - a[q];
-        } else if (EP == EP_PLAIN) {
-            y[i] = a[q];
-        } else if (EP == EP_PROLONG) {
-            x[i] = x[i] + a[q];
-        } else if (EP == EP_CHEB_POST1) {
-            d[i] = dinv[i] * (b[i] - a[q]) * (T)c.inv_theta;
-        } else {
-            const T di = d[i];
-            x[i] = x[i] + (T)(1.0 + c.c3) * di + (T)c.c4 * ((T)c.theta * di - dinv[i] * a[q]);
-        }
+    for (int q = 0; q < 2; q++)
+        if (i0 + q < M.nrows)
+            level_epilogue<T, EP>(i0 + q, a[q], b, dinv, d, x, y, c);
+}
+
+// CSR: G lanes per row, partial sums combined with shuffles inside the group
+template <class T, int G, int EP>
+__global__ void __launch_bounds__(256)
+    k_level_csr(CsrView<T> M, const T *__restrict__ u, const T *__restrict__ b,
+                const T *__restrict__ dinv, T *d, T *x, T *y, ChebC c, const int *done) {
+    if (*done)
+        return;
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = gid / G, li = gid % G;
+    T acc = 0;
+    if (row < M.nrows) {
+        const int e = M.rp[row + 1];
+        for (int t = M.rp[row] + li; t < e; t += G)
+            acc = fma(__ldcs(M.v + t), __ldg(u + __ldcs(M.ci + t)), acc);
     }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1)
+        acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (row < M.nrows && li == 0)
+        level_epilogue<T, EP>(row, acc, b, dinv, d, x, y, c);
 }
 
 // d = dinv b / theta (start of the pre-smoother from a zero guess)
@@ -567,6 +649,7 @@ template <> struct LvlPtr<double> {
     static EllView<double> A(const AmgLevel &L) { return L.A64; }
     static EllView<double> P(const AmgLevel &L) { return L.P.view64(); }
     static EllView<double> R(const AmgLevel &L) { return L.R.view64(); }
+    static CsrView<double> csr(const DCsr &D) { return {D.n, D.rp.p, D.ci.p, D.v64.p}; }
     static const double *dinv(const AmgLevel &L) { return L.dinv.p; }
     static double *b(AmgLevel &L) { return L.b.p; }
     static double *x(AmgLevel &L) { return L.x.p; }
@@ -578,6 +661,7 @@ template <> struct LvlPtr<float> {
     static EllView<float> A(const AmgLevel &L) { return L.A32; }
     static EllView<float> P(const AmgLevel &L) { return L.P.view32(); }
     static EllView<float> R(const AmgLevel &L) { return L.R.view32(); }
+    static CsrView<float> csr(const DCsr &D) { return {D.n, D.rp.p, D.ci.p, D.v32.p}; }
     static const float *dinv(const AmgLevel &L) { return L.dinv32.p; }
     static float *b(AmgLevel &L) { return L.b32.p; }
     static float *x(AmgLevel &L) { return L.x32.p; }
@@ -587,6 +671,23 @@ template <> struct LvlPtr<float> {
 };
 
 static unsigned sblocks(int n) { return (unsigned)(((n + SLICE - 1) / SLICE + 7) / 8); }
+
+// launch one fused level operation with the operator's tuned schedule
+template <class T, int EP>
+static int level_op(int mode, const EllView<T> &E, const CsrView<T> &Cv, const T *u, const T *b,
+                    const T *dinv, T *d, T *x, T *y, const ChebC &c, const int *done,
+                    cudaStream_t s) {
+    const int n = E.nrows;
+    switch (mode) {
+    case 0: k_level<T, EP><<<sblocks(n), 256, 0, s>>>(E, u, b, dinv, d, x, y, c, done); break;
+    case 1: k_level_csr<T, 4, EP><<<(unsigned)((n * 4 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
+    case 2: k_level_csr<T, 8, EP><<<(unsigned)((n * 8 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
+    case 3: k_level_csr<T, 16, EP><<<(unsigned)((n * 16 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
+    default: k_level_csr<T, 32, EP><<<(unsigned)(((size_t)n * 32 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
+    }
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
 
 template <class T>
 static int vcycle(const Amg &a, size_t l, const T *b, T *x, const int *done, cudaStream_t s) {
@@ -600,27 +701,22 @@ static int vcycle(const Amg &a, size_t l, const T *b, T *x, const int *done, cud
     AmgLevel &N = *a.L[l + 1];
     const ChebC c = cheb_consts(L.lmax);
     const EllView<T> A = LP::A(L);
+    const CsrView<T> Ac = LP::csr(L.Ac), Pc = LP::csr(L.Pc), Rc = LP::csr(L.Rc);
     const T *dinv = LP::dinv(L);
     T *d = LP::d(L), *r = LP::r(L);
-    const unsigned nb = sblocks(L.n);
     const unsigned vb = (unsigned)std::min((L.n + 255) / 256, sm_count() * 8);
+    const int mA = l == 0 ? 0 : L.sA.mode;
     k_cheb_start<T><<<vb, 256, 0, s>>>(L.n, b, dinv, d, (T)c.inv_theta, done);
     MP_CHECK_LAUNCH();
-    k_level<T, EP_CHEB_PRE><<<nb, 256, 0, s>>>(A, d, b, dinv, d, x, nullptr, c, done);
-    MP_CHECK_LAUNCH();
-    k_level<T, EP_RESID><<<nb, 256, 0, s>>>(A, x, b, dinv, d, x, r, c, done);
-    MP_CHECK_LAUNCH();
-    k_level<T, EP_PLAIN><<<sblocks(N.n), 256, 0, s>>>(LP::R(L), r, nullptr, nullptr, nullptr,
-                                                      nullptr, LP::b(N), c, done);
-    MP_CHECK_LAUNCH();
+    MP_TRY((level_op<T, EP_CHEB_PRE>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
+    MP_TRY((level_op<T, EP_RESID>(mA, A, Ac, x, b, dinv, d, x, r, c, done, s)));
+    MP_TRY((level_op<T, EP_PLAIN>(L.sR.mode, LP::R(L), Rc, r, nullptr, nullptr, nullptr, nullptr,
+                                  LP::b(N), c, done, s)));
     MP_TRY(vcycle<T>(a, l + 1, LP::b(N), LP::x(N), done, s));
-    k_level<T, EP_PROLONG><<<nb, 256, 0, s>>>(LP::P(L), LP::x(N), nullptr, nullptr, nullptr, x,
-                                              nullptr, c, done);
-    MP_CHECK_LAUNCH();
-    k_level<T, EP_CHEB_POST1><<<nb, 256, 0, s>>>(A, x, b, dinv, d, x, nullptr, c, done);
-    MP_CHECK_LAUNCH();
-    k_level<T, EP_CHEB_POST2><<<nb, 256, 0, s>>>(A, d, b, dinv, d, x, nullptr, c, done);
-    MP_CHECK_LAUNCH();
+    MP_TRY((level_op<T, EP_PROLONG>(L.sP.mode, LP::P(L), Pc, LP::x(N), nullptr, nullptr, nullptr,
+                                    x, nullptr, c, done, s)));
+    MP_TRY((level_op<T, EP_CHEB_POST1>(mA, A, Ac, x, b, dinv, d, x, nullptr, c, done, s)));
+    MP_TRY((level_op<T, EP_CHEB_POST2>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
     return MP_OK;
 }
 
@@ -630,5 +726,63 @@ int amg_apply(const Amg &a, const T *in, T *out, const int *done, cudaStream_t s
 }
 template int amg_apply<double>(const Amg &, const double *, double *, const int *, cudaStream_t);
 template int amg_apply<float>(const Amg &, const float *, float *, const int *, cudaStream_t);
+
+// ------------------------------------------------------------- autotuner
+// For each level operator and transfer, time y = M u with every schedule
+// (sliced ELL, CSR with 4/8/16/32 lanes per row) and keep the fastest.  The
+// same schedule is used for the FP64 and FP32 copies.
+static int tune_one(const Ell &E, const DCsr &D, bool allow_sell, OpSched &out, const int *zero,
+                    cudaStream_t s) {
+    if (!D.n) {
+        out.mode = 0;
+        return MP_OK;
+    }
+    dbuf<double> u, y;
+    MP_TRY(u.alloc(std::max(D.m, 1)));
+    MP_TRY(y.alloc(std::max(D.n, 1)));
+    MP_CUDA(cudaMemsetAsync(u.p, 0, sizeof(double) * u.n, s));
+    cudaEvent_t e0, e1;
+    MP_CUDA(cudaEventCreate(&e0));
+    MP_CUDA(cudaEventCreate(&e1));
+    const ChebC c{};
+    const CsrView<double> Cv{D.n, D.rp.p, D.ci.p, D.v64.p};
+    float best = 1e30f;
+    int rc = MP_OK;
+    for (int mode = allow_sell ? 0 : 1; mode <= 4 && rc == MP_OK; mode++) {
+        float ms_best = 1e30f;
+        for (int rep = 0; rep < 4 && rc == MP_OK; rep++) {
+            cudaEventRecord(e0, s);
+            rc = level_op<double, EP_PLAIN>(mode, E.view64(), Cv, u.p, nullptr, nullptr, nullptr,
+                                            nullptr, y.p, c, zero, s);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0 && ms < ms_best)
+                ms_best = ms;
+        }
+        out.us[mode] = ms_best * 1e3f;
+        if (ms_best < best) {
+            best = ms_best;
+            out.mode = mode;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+static int amg_autotune(Amg &a, cudaStream_t s) {
+    MP_TRY(a.zero_flag.alloc(1));
+    MP_CUDA(cudaMemsetAsync(a.zero_flag.p, 0, sizeof(int), s));
+    for (size_t l = 0; l + 1 < a.L.size(); l++) {
+        AmgLevel &L = *a.L[l];
+        if (l > 0)
+            MP_TRY(tune_one(L.A, L.Ac, true, L.sA, a.zero_flag.p, s));
+        MP_TRY(tune_one(L.P, L.Pc, true, L.sP, a.zero_flag.p, s));
+        MP_TRY(tune_one(L.R, L.Rc, true, L.sR, a.zero_flag.p, s));
+    }
+    return MP_OK;
+}
 
 }  // namespace mp

@@ -22,6 +22,21 @@ namespace mp {
 
 struct Cfg;
 
+// CSR copy of a multigrid operator for the row-group kernels (G lanes per row)
+struct DCsr {
+    int n = 0, m = 0;
+    dbuf<int> rp, ci;
+    dbuf<double> v64;
+    dbuf<float> v32;
+};
+
+// kernel schedule of one operator, chosen by the setup-time autotuner:
+// 0 = sliced ELL (2 rows per lane), 1..4 = CSR with 4, 8, 16, 32 lanes per row
+struct OpSched {
+    int mode = 0;
+    float us[5] = {0, 0, 0, 0, 0};
+};
+
 struct AmgLevel {
     int n = 0;
     Ell A;                   // level operator (level 0 borrows the PPE operator)
@@ -29,6 +44,8 @@ struct AmgLevel {
     EllView<double> A64;
     EllView<float> A32;
     Ell P, R;                // prolongation (n x n_next), restriction (n_next x n)
+    DCsr Ac, Pc, Rc;         // CSR copies (A only for levels >= 1)
+    OpSched sA, sP, sR;
     dbuf<double> dinv;
     dbuf<float> dinv32;
     double lmax = 2.0;
@@ -43,6 +60,7 @@ struct Amg {
     dbuf<double> cinv;                // (nc+1)^2 bordered inverse, row-major
     dbuf<float> cinv32;
     double setup_seconds = 0;
+    dbuf<int> zero_flag;              // a device 0 used as `done` while autotuning
     ~Amg();
 };
 

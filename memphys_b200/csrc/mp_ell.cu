@@ -68,7 +68,7 @@ int ell_create(Ell &E, int nrows, int ncols, int K, const int *cols, const doubl
 }
 
 int ell_make_fp32(Ell &E, cudaStream_t s) {
-    const size_t tot = (size_t)ell_padded_rows(E.nrows) * E.K;
+    const size_t tot = E.v64.n;
     MP_TRY(E.v32.alloc(tot));
     f64_to_f32<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(E.v64.p, E.v32.p, tot);
     MP_CHECK_LAUNCH();
@@ -84,10 +84,13 @@ __global__ void __launch_bounds__(256)
     const int nslices = (A.nrows + SLICE - 1) / SLICE;
     if (warp >= nslices)
         return;
-    const size_t base = (size_t)warp * A.K * SLICE + 2 * lane;
+    size_t base;
+    int K;
+    slice_span(A, warp, base, K);
+    base += 2 * lane;
     T a0 = 0, a1 = 0;
 #pragma unroll 4
-    for (int k = 0; k < A.K; k++) {
+    for (int k = 0; k < K; k++) {
         const int2 c = __ldcs(reinterpret_cast<const int2 *>(A.cols + base + (size_t)k * SLICE));
         const V2 v = __ldcs(reinterpret_cast<const V2 *>(A.vals + base + (size_t)k * SLICE));
         a0 = fma(v.x, __ldg(x + c.x), a0);
@@ -268,7 +271,8 @@ static int op_apply_t(mp_op op, const void *x, void *y, double alpha, double bet
         dy = ty.p;
     }
     EllView<T> A{op->E.nrows, op->E.ncols, op->E.K, op->cols(),
-                 std::is_same<T, double>::value ? (const T *)op->E.v64.p : (const T *)op->E.v32.p};
+                 std::is_same<T, double>::value ? (const T *)op->E.v64.p : (const T *)op->E.v32.p,
+                 nullptr};
     MP_TRY(ell_spmv<T>(A, dx, dy, alpha, beta, s));
     if (host_y) {
         MP_CUDA(cudaMemcpyAsync(y, dy, sizeof(T) * op->E.nrows, cudaMemcpyDeviceToHost, s));

@@ -22,21 +22,40 @@ __host__ __device__ inline size_t ell_index(int row, int k, int K) {
 
 __host__ __device__ inline int ell_padded_rows(int nrows) { return (nrows + SLICE - 1) / SLICE * SLICE; }
 
-// Device ELL matrix (non-owning view)
+// Device ELL matrix (non-owning view).  With soff == nullptr every slice has
+// width K; otherwise slice s spans entries [soff[s], soff[s+1]) of width
+// soff[s+1] - soff[s] (sliced ELL with a width per 64-row slice, used for the
+// multigrid operators whose row lengths vary).
 template <class T> struct EllView {
     int nrows, ncols, K;
     const int *cols;
     const T *vals;
+    const int *soff;
 };
+
+// start offset and width of slice w
+template <class T>
+__device__ __forceinline__ void slice_span(const EllView<T> &A, int w, size_t &base, int &K) {
+    if (A.soff) {
+        const int o0 = A.soff[w], o1 = A.soff[w + 1];
+        base = (size_t)o0 * SLICE;
+        K = o1 - o0;
+    } else {
+        base = (size_t)w * A.K * SLICE;
+        K = A.K;
+    }
+}
 
 // Owning ELL storage
 struct Ell {
-    int nrows = 0, ncols = 0, K = 0;
+    int nrows = 0, ncols = 0, K = 0;  // K: uniform width, or the widest slice when soff is set
     dbuf<int> cols;
     dbuf<double> v64;
     dbuf<float> v32;
-    EllView<double> view64() const { return {nrows, ncols, K, cols.p, v64.p}; }
-    EllView<float> view32() const { return {nrows, ncols, K, cols.p, v32.p}; }
+    dbuf<int> soff;
+    size_t entries() const { return v64.p ? v64.n : (v32.p ? v32.n : cols.n); }
+    EllView<double> view64() const { return {nrows, ncols, K, cols.p, v64.p, soff.p}; }
+    EllView<float> view32() const { return {nrows, ncols, K, cols.p, v32.p, soff.p}; }
 };
 
 // Build an Ell from row-major host or device arrays (copied).

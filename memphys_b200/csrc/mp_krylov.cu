@@ -24,7 +24,10 @@ template <class T>
 __device__ __forceinline__ void ell_pair(const EllView<T> &A, int w, int lane,
                                          const T *__restrict__ x, T &a0, T &a1, T &xs0, T &xs1) {
     using V2 = typename V2t<T>::type;
-    const size_t base = (size_t)w * A.K * SLICE + 2 * lane;
+    size_t base;
+    int K;
+    slice_span(A, w, base, K);
+    base += 2 * lane;
     int2 c = __ldcs(reinterpret_cast<const int2 *>(A.cols + base));
     V2 v = __ldcs(reinterpret_cast<const V2 *>(A.vals + base));
     xs0 = __ldg(x + c.x);
@@ -32,7 +35,7 @@ __device__ __forceinline__ void ell_pair(const EllView<T> &A, int w, int lane,
     a0 = v.x * xs0;
     a1 = v.y * xs1;
 #pragma unroll 4
-    for (int k = 1; k < A.K; k++) {
+    for (int k = 1; k < K; k++) {
         const size_t o = base + (size_t)k * SLICE;
         c = __ldcs(reinterpret_cast<const int2 *>(A.cols + o));
         v = __ldcs(reinterpret_cast<const V2 *>(A.vals + o));
@@ -55,10 +58,10 @@ __global__ void __launch_bounds__(KT)
     k_init(EllView<T> A, int bordered, const T *x, const T *b, T *r, T *r0, T *p, T *v,
            BicgScalars *S, RedBuf R, double tol, int maxit, cudaGraphConditionalHandle h) {
     KRYLOV_SMEM
-    const int nv = A.nrows, w = gwarp(), lane = threadIdx.x & 31;
+    const int nv = A.nrows, lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nsl = (nv + SLICE - 1) / SLICE;
     double acc[3] = {0, 0, 0};
-    if (w < nsl) {
+    for (int w = gwarp(); w < nsl; w += nwarps) {
         T a0 = 0, a1 = 0, s0 = 0, s1 = 0;
         if (!ZERO_X)
             ell_pair(A, w, lane, x, a0, a1, s0, s1);
@@ -124,10 +127,10 @@ __global__ void __launch_bounds__(KT)
     KRYLOV_SMEM
     if (S->done || !S->need_restart)
         return;
-    const int nv = A.nrows, w = gwarp(), lane = threadIdx.x & 31;
+    const int nv = A.nrows, lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nsl = (nv + SLICE - 1) / SLICE;
     double acc[2] = {0, 0};
-    if (w < nsl) {
+    for (int w = gwarp(); w < nsl; w += nwarps) {
         T a0, a1, s0, s1;
         ell_pair(A, w, lane, x, a0, a1, s0, s1);
         const T xb = bordered ? x[nv] : T(0);
@@ -193,10 +196,10 @@ __global__ void __launch_bounds__(KT)
     KRYLOV_SMEM
     if (S->done)
         return;
-    const int nv = A.nrows, w = gwarp(), lane = threadIdx.x & 31;
+    const int nv = A.nrows, lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nsl = (nv + SLICE - 1) / SLICE;
     double acc[2] = {0, 0};
-    if (w < nsl) {
+    for (int w = gwarp(); w < nsl; w += nwarps) {
         T a0, a1, s0, s1;
         ell_pair(A, w, lane, y, a0, a1, s0, s1);
         const T yb = bordered ? y[nv] : T(0);
@@ -256,10 +259,10 @@ __global__ void __launch_bounds__(KT)
     KRYLOV_SMEM
     if (S->done)
         return;
-    const int nv = A.nrows, w = gwarp(), lane = threadIdx.x & 31;
+    const int nv = A.nrows, lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nsl = (nv + SLICE - 1) / SLICE;
     double acc[3] = {0, 0, 0};
-    if (w < nsl) {
+    for (int w = gwarp(); w < nsl; w += nwarps) {
         T a0, a1, s0, s1;
         ell_pair(A, w, lane, z, a0, a1, s0, s1);
         const T zb = bordered ? z[nv] : T(0);
@@ -333,11 +336,11 @@ __global__ void __launch_bounds__(KT)
     k_true_residual(EllView<double> A, int bordered, double *x, const double *b, double *r64,
                     BicgScalars *S, RedBuf R, int refine, cudaGraphConditionalHandle h) {
     KRYLOV_SMEM
-    const int nv = A.nrows, w = gwarp(), lane = threadIdx.x & 31;
+    const int nv = A.nrows, lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nsl = (nv + SLICE - 1) / SLICE;
     const bool zx = S->zero_x && !refine;
     double acc[3] = {0, 0, 0};
-    if (w < nsl) {
+    for (int w = gwarp(); w < nsl; w += nwarps) {
         double a0 = 0, a1 = 0, s0 = 0, s1 = 0;
         if (!zx)
             ell_pair(A, w, lane, x, a0, a1, s0, s1);
@@ -474,12 +477,15 @@ __global__ void k_assemble_ppe(int nv, int K, int dim, const int *cols, const do
 // ------------------------------------------------------------ host side
 static unsigned vec_blocks(int n) {
     int b = (n + KT - 1) / KT;
-    int cap = sm_count() * 8;
+    int cap = sm_count() * 4;
     return (unsigned)(b < cap ? (b < 1 ? 1 : b) : cap);
 }
+// reduction kernels walk the slices with a grid of a few blocks per SM, so the
+// last-block ticket sees few atomics
 static unsigned slice_blocks(int nv) {
     int ns = (nv + SLICE - 1) / SLICE;
-    return (unsigned)((ns + 7) / 8);
+    int b = (ns + 7) / 8, cap = sm_count() * 4;
+    return (unsigned)(b < cap ? b : cap);
 }
 
 int Krylov::alloc(int nv_, int bordered_, bool mixed, bool external_pc) {
@@ -813,7 +819,7 @@ Cfg Cfg::from(const mp_solver_cfg &c) {
     o.inner_tol = c.inner_tol > 0 ? c.inner_tol : 1e-5;
     o.max_refine = 12;
     o.amg_max_levels = c.amg_max_levels > 0 ? c.amg_max_levels : 12;
-    o.amg_coarse_size = c.amg_coarse_size > 0 ? c.amg_coarse_size : 256;
+    o.amg_coarse_size = c.amg_coarse_size > 0 ? c.amg_coarse_size : 512;
     o.smoother_sweeps = c.smoother_sweeps > 0 ? c.smoother_sweeps : 1;
     o.smoother_omega = c.smoother_omega > 0 ? c.smoother_omega : 0.7;
     return o;
@@ -833,7 +839,7 @@ extern "C" int mp_solver_cfg_default(mp_solver_cfg *c) {
     c->guess = MP_GUESS_PREVIOUS;
     c->inner_tol = 1e-5;
     c->amg_max_levels = 12;
-    c->amg_coarse_size = 256;
+    c->amg_coarse_size = 512;
     c->smoother_sweeps = 1;
     c->smoother_omega = 0.7;
     return MP_OK;

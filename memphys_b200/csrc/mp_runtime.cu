@@ -2,6 +2,7 @@
 #include <atomic>
 #include <cstdarg>
 #include <cmath>
+#include <cuda_profiler_api.h>
 #include "mp_common.cuh"
 
 namespace mp {
@@ -181,6 +182,11 @@ int mp_timer_stop(void *timer, mp_stream s, double *ms) {
     cudaEventDestroy(t->a);
     cudaEventDestroy(t->b);
     delete t;
+    return MP_OK;
+}
+
+int mp_profiler(int on) {
+    MP_CUDA(on ? cudaProfilerStart() : cudaProfilerStop());
     return MP_OK;
 }
 

@@ -326,10 +326,13 @@ class FRACTIONAL_STEP_1:
         """fractional_step_1.cpp:52-63 with the reference's argument order."""
         if len(p_new) != self.system_size:
             raise capi.MemphysError(capi.MP_BAD_ARG, "p_new must have system_size entries")
+        # keep every converted array referenced until the call returns
+        uo = np.ascontiguousarray(u_old, np.float64)
+        vo_ = np.ascontiguousarray(v_old, np.float64)
+        po = np.ascontiguousarray(p_old, np.float64)
         vn = self._vec_ptrs([u_new, v_new])
-        vo = self._vec_ptrs([np.ascontiguousarray(u_old), np.ascontiguousarray(v_old)])
-        rc = capi.lib().mp_fs1_single_timestep(self.handle, vn, ptr(p_new), vo,
-                                               ptr(np.ascontiguousarray(p_old)), it, None)
+        vo = self._vec_ptrs([uo, vo_])
+        rc = capi.lib().mp_fs1_single_timestep(self.handle, vn, ptr(p_new), vo, ptr(po), it, None)
         iters, rr, ar, al = self.last_stats()
         parameters.rel_res_log.append(rr)
         parameters.abs_res_log.append(ar)

@@ -70,7 +70,8 @@ def test_duplicate_nodes_are_singular(mp_lib):
 def test_bad_parameters(mp_lib, phs, poly, dim):
     cl = clouds.cavity_2d(10)
     h = __import__("ctypes").c_void_p()
-    rc = capi.lib().mp_cloud_create(ptr(cl.xyz), ptr(cl.boundary.astype(np.uint8)), cl.nv, dim,
+    bnd = cl.boundary.astype(np.uint8)
+    rc = capi.lib().mp_cloud_create(ptr(cl.xyz), ptr(bnd), cl.nv, dim,
                                     phs, poly, 2.0, 0, None, __import__("ctypes").byref(h))
     assert rc == capi.MP_BAD_ARG
 

@@ -25,22 +25,23 @@ pytestmark = pytest.mark.gpu
 
 
 def gpu_knn(xyz, bnd, n):
-    import ctypes as C
+    # arrays passed by address must stay referenced until the call returns
+    xyz = np.ascontiguousarray(xyz, np.float64)
+    bnd = np.ascontiguousarray(bnd, np.uint8)
     nv, dim = xyz.shape
     out = np.zeros((nv, n), np.int32)
-    capi.check(capi.lib().mp_knn_stencils(ptr(np.ascontiguousarray(xyz)),
-                                          ptr(np.ascontiguousarray(bnd, np.uint8)), nv, dim, n,
-                                          ptr(out), None))
+    capi.check(capi.lib().mp_knn_stencils(ptr(xyz), ptr(bnd), nv, dim, n, ptr(out), None))
     return out
 
 
 def gpu_weights(xyz, nb, phs=3, poly=3, cond=True):
+    xyz = np.ascontiguousarray(xyz, np.float64)
+    nb = np.ascontiguousarray(nb, np.int32)
     nv, dim = xyz.shape
     n = nb.shape[1]
     w = {k: np.zeros((nv, n)) for k in ["gx", "gy", "lap"] + (["gz"] if dim == 3 else [])}
     c = np.zeros(nv) if cond else None
-    capi.check(capi.lib().mp_stencil_weights(ptr(np.ascontiguousarray(xyz)), nv, dim,
-                                             ptr(np.ascontiguousarray(nb, np.int32)), n, phs, poly,
+    capi.check(capi.lib().mp_stencil_weights(ptr(xyz), nv, dim, ptr(nb), n, phs, poly,
                                              ptr(w["gx"]), ptr(w["gy"]), ptr(w.get("gz")),
                                              ptr(w["lap"]), ptr(c), None))
     if cond:
