@@ -136,7 +136,12 @@ int mp_cloud_destroy(mp_cloud c);
 /* -------------------------------------------------------------- operators */
 typedef struct mp_op_s *mp_op;
 
-enum { MP_FP64 = 0, MP_FP32 = 1 };
+/* operator precision; for the pressure solve (mp_solver_cfg.precision) also
+ * MP_MG32: FP64 BiCGSTAB whose multigrid preconditioner stores its level
+ * operators, prolongations and restrictions in FP32 (level operators in the
+ * difference form (A u)_i = s_i u_i + sum_j a_ij (u_j - u_i), s_i the exact
+ * row sum) and works on FP64 vectors */
+enum { MP_FP64 = 0, MP_FP32 = 1, MP_MG32 = 2 };
 enum { MP_GRAD_X = 0, MP_GRAD_Y = 1, MP_GRAD_Z = 2, MP_LAPLACIAN = 3 };
 enum { MP_ROWS_ALL = 0, MP_ROWS_INTERNAL = 1, MP_ROWS_BOUNDARY = 2 };
 
@@ -162,13 +167,16 @@ int mp_op_destroy(mp_op op);
 typedef struct mp_ppe_s *mp_ppe;
 
 enum { MP_PRECOND_NONE = 0, MP_PRECOND_JACOBI = 1, MP_PRECOND_AMG = 2 };
-enum { MP_GUESS_PREVIOUS = 0, MP_GUESS_ZERO = 1, MP_GUESS_LEARNED = 2 };
+/* initial guess of each fractional-step pressure solve: the previous pressure
+ * (the reference's solveWithGuess(rhs, p_old)), zero, the linear extrapolation
+ * 2 p^n - p^(n-1), or p^n plus the learned network's predicted increment */
+enum { MP_GUESS_PREVIOUS = 0, MP_GUESS_ZERO = 1, MP_GUESS_LEARNED = 2, MP_GUESS_EXTRAPOLATE = 3 };
 
 typedef struct {
     double tol;        /* relative residual ||b - A x|| / ||b||, solver.cpp:154 */
     int maxit;         /* solver.cpp:155 */
     int precond;       /* MP_PRECOND_* */
-    int precision;     /* MP_FP64, or MP_FP32 = FP32 Krylov + FP64 iterative refinement */
+    int precision;     /* MP_FP64; MP_FP32 = FP32 Krylov + FP64 iterative refinement; MP_MG32 */
     int guess;         /* MP_GUESS_* */
     double inner_tol;  /* mixed precision: relative reduction per refinement sweep */
     int amg_max_levels;
@@ -234,14 +242,57 @@ int mp_fs1_single_timestep(mp_fs1 f, double *const *vel_new, double *p_new,
 /* per-solve logs of the last step (class.hpp:83-84: rel_res_log, abs_res_log,
  * n_iter_actual, regul_alpha_log) */
 int mp_fs1_last_stats(mp_fs1 f, int *iters, double *relres, double *abs_res, double *alpha);
-/* the same four logs for `count` steps starting at step `first` (4 doubles per step:
- * iterations, relative residual, absolute residual, regularisation alpha); the
- * device keeps the last 4096 steps */
+/* the logs of `count` steps starting at step `first`, MP_LOG_FIELDS doubles per
+ * step: iterations (mixed: inner sweeps), relative residual, absolute residual,
+ * regularisation alpha, relative residual of the initial guess, refinement
+ * sweeps (mixed), and two reserved fields; the device keeps the last 4096 steps */
+#define MP_LOG_FIELDS 8
 int mp_fs1_log(mp_fs1 f, int first, int count, double *out);
 /* kernels in one graph step: `fixed` once per step, `per_sweep` per BiCGSTAB
  * sweep, `per_refine` per iterative-refinement sweep (mixed precision) */
 int mp_fs1_kernel_counts(mp_fs1 f, int *fixed, int *per_sweep, int *per_refine);
 int mp_fs1_destroy(mp_fs1 f);
+
+/* ------------------------------------------------------- learned guess */
+/*
+ * Per-node network predicting the pressure increment of a fractional step
+ * (no counterpart in the reference; its Python CNN surrogate
+ * NN_functions.py:17-51 is a different model).  64 features -> 128 -> 128 ->
+ * 128 (ReLU) -> 1; BF16 weights and activations, FP32 accumulation on the
+ * tensor cores (tcgen05); FP32 master weights trained with Adam on the GPU.
+ * Feature layout and parameter order: memphys_b200/csrc/mp_mlp.cuh.
+ */
+typedef struct mp_mlp_s *mp_mlp;
+
+int mp_mlp_create(uint64_t seed, mp_mlp *out);
+int mp_mlp_num_params(void);
+int mp_mlp_get_params(mp_mlp m, float *theta);
+int mp_mlp_set_params(mp_mlp m, const float *theta);
+/* y = net(X) for n rows of 64 features (FP32 in, rounded to BF16) */
+int mp_mlp_forward(mp_mlp m, const float *X, int n, float *y);
+/* mean squared error over n rows and its gradient w.r.t. the parameters */
+int mp_mlp_gradient(mp_mlp m, const float *X, const float *t, int n, double *loss, float *grad);
+/* Adam, `epochs` passes over n rows in shuffled batches (batch a multiple of 128) */
+int mp_mlp_train(mp_mlp m, const float *X, const float *t, int n, int epochs, int batch,
+                 double lr, uint64_t seed, double *loss);
+int mp_mlp_destroy(mp_mlp m);
+
+/*
+ * Attach a network to a fractional step: every step then records, for
+ * `sample_nodes` fixed nodes, the features and the solved increment (up to
+ * `capacity_steps` steps, oldest overwritten).  mp_fs1_train_mlp trains the
+ * network on the recorded samples; mp_fs1_set_guess selects the pressure
+ * solve's initial guess (MP_GUESS_*).  The solve always runs to the same
+ * tolerance, so a poor prediction costs iterations, never accuracy.
+ */
+int mp_fs1_attach_mlp(mp_fs1 f, mp_mlp m, int sample_nodes, int capacity_steps, int collect);
+int mp_fs1_train_mlp(mp_fs1 f, int epochs, int batch, double lr, uint64_t seed, double *loss);
+int mp_fs1_set_guess(mp_fs1 f, int guess);
+/* The recorded samples, in ring-slot order: X (n x 64 row-major features, the
+ * BF16 values widened to float), t (n targets) and nodes (n sampled node
+ * indices); any may be NULL.  cap is the number of rows the outputs hold; *n
+ * returns the number of rows recorded (at most cap are written). */
+int mp_fs1_samples(mp_fs1 f, float *X, float *t, int *nodes, int cap, int *n);
 
 #ifdef __cplusplus
 }

@@ -17,11 +17,12 @@ LIB_PATH = os.path.join(HERE, "libmemphys_cuda.so")
 
 MP_OK, MP_NOT_CONVERGED, MP_BREAKDOWN, MP_NAN_DETECTED, MP_SINGULAR_STENCIL, MP_BAD_ARG, \
     MP_CUDA_ERROR, MP_NO_DEVICE, MP_TIMEOUT, MP_KNN_FAILED = range(10)
-MP_FP64, MP_FP32 = 0, 1
+MP_FP64, MP_FP32, MP_MG32 = 0, 1, 2
 MP_GRAD_X, MP_GRAD_Y, MP_GRAD_Z, MP_LAPLACIAN = range(4)
 MP_ROWS_ALL, MP_ROWS_INTERNAL, MP_ROWS_BOUNDARY = range(3)
 MP_PRECOND_NONE, MP_PRECOND_JACOBI, MP_PRECOND_AMG = range(3)
-MP_GUESS_PREVIOUS, MP_GUESS_ZERO, MP_GUESS_LEARNED = range(3)
+MP_GUESS_PREVIOUS, MP_GUESS_ZERO, MP_GUESS_LEARNED, MP_GUESS_EXTRAPOLATE = range(4)
+MP_LOG_FIELDS = 8
 
 STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "NAN_DETECTED",
                 4: "SINGULAR_STENCIL", 5: "BAD_ARG", 6: "CUDA_ERROR", 7: "NO_DEVICE",
@@ -39,7 +40,9 @@ EXPORTS = [
     "mp_ppe_system_size", "mp_ppe_solve", "mp_ppe_destroy", "mp_fs1_create",
     "mp_fs1_system_size", "mp_fs1_set_state", "mp_fs1_get_state", "mp_fs1_step",
     "mp_fs1_single_timestep", "mp_fs1_last_stats", "mp_fs1_log", "mp_fs1_kernel_counts",
-    "mp_fs1_destroy",
+    "mp_fs1_destroy", "mp_mlp_create", "mp_mlp_num_params", "mp_mlp_get_params",
+    "mp_mlp_set_params", "mp_mlp_forward", "mp_mlp_gradient", "mp_mlp_train", "mp_mlp_destroy",
+    "mp_fs1_attach_mlp", "mp_fs1_train_mlp", "mp_fs1_set_guess", "mp_fs1_samples",
 ]
 
 
@@ -108,6 +111,16 @@ def lib() -> C.CDLL:
             "mp_fs1_log": [vp, i, i, vp],
             "mp_fs1_kernel_counts": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)],
             "mp_fs1_destroy": [vp],
+            "mp_mlp_create": [C.c_uint64, C.POINTER(vp)], "mp_mlp_num_params": [],
+            "mp_mlp_get_params": [vp, vp], "mp_mlp_set_params": [vp, vp],
+            "mp_mlp_forward": [vp, vp, i, vp],
+            "mp_mlp_gradient": [vp, vp, vp, i, C.POINTER(d), vp],
+            "mp_mlp_train": [vp, vp, vp, i, i, i, d, C.c_uint64, C.POINTER(d)],
+            "mp_mlp_destroy": [vp],
+            "mp_fs1_attach_mlp": [vp, vp, i, i, i],
+            "mp_fs1_train_mlp": [vp, i, i, d, C.c_uint64, C.POINTER(d)],
+            "mp_fs1_set_guess": [vp, i],
+            "mp_fs1_samples": [vp, vp, vp, vp, i, C.POINTER(i)],
         }
         for name, args in sig.items():
             f = getattr(L, name)

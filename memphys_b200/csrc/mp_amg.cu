@@ -1,6 +1,7 @@
 // mp_amg.cu -- smoothed-aggregation multigrid: host setup, GPU V-cycle.
 #include <algorithm>
 #include <chrono>
+#include <type_traits>
 #include <cmath>
 #include <unordered_map>
 #include "mp_amg.cuh"
@@ -63,6 +64,31 @@ static std::vector<double> diag_of(const Csr &A) {
             if (A.ci[t] == i)
                 d[i] += A.v[t];
     return d;
+}
+
+// difference form of a square operator: self entry first holding the row sum,
+// then the off-diagonal entries, so that (A u)_i = s_i u_i + sum_j a_ij (u_j - u_i)
+static Csr diff_form(const Csr &A) {
+    Csr D;
+    D.n = A.n;
+    D.m = A.m;
+    D.rp.assign(A.n + 1, 0);
+    D.ci.reserve(A.ci.size() + A.n);
+    D.v.reserve(A.v.size() + A.n);
+    for (int i = 0; i < A.n; i++) {
+        double sum = 0.0;
+        for (int t = A.rp[i]; t < A.rp[i + 1]; t++)
+            sum += A.v[t];
+        D.ci.push_back(i);
+        D.v.push_back(sum);
+        for (int t = A.rp[i]; t < A.rp[i + 1]; t++)
+            if (A.ci[t] != i) {
+                D.ci.push_back(A.ci[t]);
+                D.v.push_back(A.v[t]);
+            }
+        D.rp[i + 1] = (int)D.ci.size();
+    }
+    return D;
 }
 
 // largest |eigenvalue| of D^-1 A by power iteration (deterministic start)
@@ -329,6 +355,61 @@ static int make_f32(const dbuf<double> &a, dbuf<float> &b, cudaStream_t s) {
     return MP_OK;
 }
 
+// level 0 in FP32 difference form, in the PPE operator's own sliced layout
+// (its stencil rows start with the node itself); one thread per row
+__global__ void k_diff_level0(EllView<double> A, float *out, int *bad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int np = ell_padded_rows(A.nrows);
+    if (i >= np)
+        return;
+    size_t base;
+    int K;
+    slice_span(A, i / SLICE, base, K);
+    base += i % SLICE;
+    double sum = 0.0;
+    for (int k = 0; k < K; k++)
+        sum += A.vals[base + (size_t)k * SLICE];
+    if (i < A.nrows && K > 0 && A.cols[base] != i)
+        atomicAdd(bad, 1);
+    for (int k = 1; k < K; k++)
+        out[base + (size_t)k * SLICE] = (float)A.vals[base + (size_t)k * SLICE];
+    if (K > 0)
+        out[base] = i < A.nrows ? (float)sum : 0.f;
+}
+
+static int diff_level0(const Ell &A0, AmgLevel &L, cudaStream_t s) {
+    const EllView<double> A = A0.view64();
+    MP_TRY(L.Ad.v32.alloc(A0.v64.n));
+    dbuf<int> bad;
+    MP_TRY(bad.alloc(1));
+    MP_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+    const int np = ell_padded_rows(A0.nrows);
+    k_diff_level0<<<(np + 255) / 256, 256, 0, s>>>(A, L.Ad.v32.p, bad.p);
+    MP_CHECK_LAUNCH();
+    int hb = 0;
+    MP_CUDA(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    if (hb)
+        return fail(MP_BAD_ARG, "FP32 multigrid storage needs every stencil row to start with its "
+                                "own node (%d rows do not)", hb);
+    L.Ad32 = EllView<float>{A0.nrows, A0.ncols, A0.K, A0.cols.p, L.Ad.v32.p, A0.soff.p};
+    return MP_OK;
+}
+
+// levels >= 1: difference-form copies (sliced ELL and CSR), FP32 values
+static int diff_level(const Csr &A, AmgLevel &L, cudaStream_t s) {
+    const Csr D = diff_form(A);
+    MP_TRY(upload_ell(D, L.Ad, true, s));
+    MP_TRY(ell_make_fp32(L.Ad, s));
+    MP_TRY(upload_csr(D, L.Acd, s));
+    MP_TRY(make_f32(L.Acd.v64, L.Acd.v32, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    L.Ad.v64.release();
+    L.Acd.v64.release();
+    L.Ad32 = L.Ad.view32();
+    return MP_OK;
+}
+
 Amg::~Amg() {
     for (auto *l : L)
         delete l;
@@ -336,10 +417,12 @@ Amg::~Amg() {
 
 static int amg_autotune(Amg &a, cudaStream_t s);
 
-int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, bool mixed, cudaStream_t s) {
+int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t s) {
     auto t0 = std::chrono::steady_clock::now();
     const double theta = 0.25;
+    const bool mixed = store == AMG_F32;
     Amg *a = new Amg;
+    a->store = store;
     Csr A;
     int rc = csr_from_ell(A0, A);
     if (rc != MP_OK) {
@@ -362,10 +445,14 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, bool mixed, cudaStream_
             L->borrowed = true;
             L->A64 = A0.view64();
             L->A32 = A0.view32();
+            if (store == AMG_MG32 && (rc = diff_level0(A0, *L, s)) != MP_OK)
+                return bail(rc);
         } else {
             if ((rc = upload_ell(A, L->A, true, s)) != MP_OK || (rc = upload_csr(A, L->Ac, s)) != MP_OK)
                 return bail(rc);
             L->A64 = L->A.view64();
+            if (store == AMG_MG32 && (rc = diff_level(A, *L, s)) != MP_OK)
+                return bail(rc);
         }
         if ((rc = L->dinv.alloc(A.n)) != MP_OK)
             return bail(rc);
@@ -470,6 +557,16 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, bool mixed, cudaStream_
         if ((rc = make_f32(a->cinv, a->cinv32, s)) != MP_OK)
             return bail(rc);
     }
+    if (store == AMG_MG32) {  // FP32 transfers; vectors, diagonal and coarse inverse stay FP64
+        for (AmgLevel *L : a->L) {
+            if (L->P.v64.p && ((rc = ell_make_fp32(L->P, s)) != MP_OK ||
+                               (rc = ell_make_fp32(L->R, s)) != MP_OK))
+                return bail(rc);
+            for (DCsr *D : {&L->Pc, &L->Rc})
+                if (D->v64.p && (rc = make_f32(D->v64, D->v32, s)) != MP_OK)
+                    return bail(rc);
+        }
+    }
     if ((rc = amg_autotune(*a, s)) != MP_OK)
         return bail(rc);
     MP_CUDA(cudaStreamSynchronize(s));
@@ -499,23 +596,38 @@ template <class T> struct V2a;
 template <> struct V2a<double> { using type = double2; };
 template <> struct V2a<float> { using type = float2; };
 
-template <class T>
-__device__ __forceinline__ void spmv_pair(const EllView<T> &A, int w, int lane,
+// Two rows of (M u): T is the vector type, V the stored value type.  With DIFF
+// the first entry of each row is the self entry holding the row sum, and the
+// others multiply (u_j - u_i): a = s_i u_i + sum_k a_ik (u_k - u_i).
+template <class T, class V, bool DIFF>
+__device__ __forceinline__ void spmv_pair(const EllView<V> &A, int w, int lane,
                                           const T *__restrict__ x, T &a0, T &a1) {
-    using V2 = typename V2a<T>::type;
+    using V2 = typename V2a<V>::type;
     size_t base;
     int K;
     slice_span(A, w, base, K);
     base += 2 * lane;
     a0 = 0;
     a1 = 0;
+    T s0 = 0, s1 = 0;
+    int k0 = 0;
+    if (DIFF && K > 0) {
+        const int i0 = w * SLICE + 2 * lane;
+        s0 = i0 < A.nrows ? __ldg(x + i0) : T(0);
+        s1 = i0 + 1 < A.nrows ? __ldg(x + i0 + 1) : T(0);
+        const V2 v = __ldcs(reinterpret_cast<const V2 *>(A.vals + base));
+        a0 = (T)v.x * s0;
+        a1 = (T)v.y * s1;
+        k0 = 1;
+    }
 #pragma unroll 4
-    for (int k = 0; k < K; k++) {
+    for (int k = k0; k < K; k++) {
         const size_t o = base + (size_t)k * SLICE;
         const int2 c = __ldcs(reinterpret_cast<const int2 *>(A.cols + o));
         const V2 v = __ldcs(reinterpret_cast<const V2 *>(A.vals + o));
-        a0 = fma(v.x, __ldg(x + c.x), a0);
-        a1 = fma(v.y, __ldg(x + c.y), a1);
+        const T x0 = __ldg(x + c.x), x1 = __ldg(x + c.y);
+        a0 = fma((T)v.x, DIFF ? x0 - s0 : x0, a0);
+        a1 = fma((T)v.y, DIFF ? x1 - s1 : x1, a1);
     }
 }
 
@@ -528,10 +640,10 @@ struct ChebC {
     double inv_theta, theta, c1, c2, c3, c4;
 };
 
-template <class T> struct CsrView {
+template <class V> struct CsrView {
     int nrows;
     const int *rp, *ci;
-    const T *v;
+    const V *v;
 };
 
 // Row i of one fused SpMV (a = (M u)_i) followed by its epilogue:
@@ -562,9 +674,9 @@ __device__ __forceinline__ void level_epilogue(int i, T a, const T *b, const T *
 }
 
 // sliced ELL: one warp per 64-row slice, two rows per lane
-template <class T, int EP>
+template <class T, class V, bool DIFF, int EP>
 __global__ void __launch_bounds__(256)
-    k_level(EllView<T> M, const T *__restrict__ u, const T *__restrict__ b,
+    k_level(EllView<V> M, const T *__restrict__ u, const T *__restrict__ b,
             const T *__restrict__ dinv, T *d, T *x, T *y, ChebC c, const int *done) {
     if (*done)
         return;
@@ -572,7 +684,7 @@ __global__ void __launch_bounds__(256)
     if (w >= (M.nrows + SLICE - 1) / SLICE)
         return;
     T a[2];
-    spmv_pair(M, w, lane, u, a[0], a[1]);
+    spmv_pair<T, V, DIFF>(M, w, lane, u, a[0], a[1]);
     const int i0 = w * SLICE + 2 * lane;
 #pragma unroll
     for (int q = 0; q < 2; q++)
@@ -581,9 +693,10 @@ __global__ void __launch_bounds__(256)
 }
 
 // CSR: G lanes per row, partial sums combined with shuffles inside the group
-template <class T, int G, int EP>
+// (DIFF: the row's first entry is its self entry, see spmv_pair)
+template <class T, class V, int G, bool DIFF, int EP>
 __global__ void __launch_bounds__(256)
-    k_level_csr(CsrView<T> M, const T *__restrict__ u, const T *__restrict__ b,
+    k_level_csr(CsrView<V> M, const T *__restrict__ u, const T *__restrict__ b,
                 const T *__restrict__ dinv, T *d, T *x, T *y, ChebC c, const int *done) {
     if (*done)
         return;
@@ -591,9 +704,12 @@ __global__ void __launch_bounds__(256)
     const int row = gid / G, li = gid % G;
     T acc = 0;
     if (row < M.nrows) {
-        const int e = M.rp[row + 1];
-        for (int t = M.rp[row] + li; t < e; t += G)
-            acc = fma(__ldcs(M.v + t), __ldg(u + __ldcs(M.ci + t)), acc);
+        const int b0 = M.rp[row], e = M.rp[row + 1];
+        const T ui = DIFF ? __ldg(u + row) : T(0);
+        for (int t = b0 + li; t < e; t += G) {
+            const T ut = __ldg(u + __ldcs(M.ci + t));
+            acc = fma((T)__ldcs(M.v + t), (DIFF && t != b0) ? ut - ui : ut, acc);
+        }
     }
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1)
@@ -644,12 +760,9 @@ static ChebC cheb_consts(double lmax) {
     return c;
 }
 
-template <class T> struct LvlPtr;
-template <> struct LvlPtr<double> {
-    static EllView<double> A(const AmgLevel &L) { return L.A64; }
-    static EllView<double> P(const AmgLevel &L) { return L.P.view64(); }
-    static EllView<double> R(const AmgLevel &L) { return L.R.view64(); }
-    static CsrView<double> csr(const DCsr &D) { return {D.n, D.rp.p, D.ci.p, D.v64.p}; }
+// Work vectors of one vector precision
+template <class T> struct LvlVec;
+template <> struct LvlVec<double> {
     static const double *dinv(const AmgLevel &L) { return L.dinv.p; }
     static double *b(AmgLevel &L) { return L.b.p; }
     static double *x(AmgLevel &L) { return L.x.p; }
@@ -657,11 +770,7 @@ template <> struct LvlPtr<double> {
     static double *r(AmgLevel &L) { return L.r.p; }
     static const double *cinv(const Amg &a) { return a.cinv.p; }
 };
-template <> struct LvlPtr<float> {
-    static EllView<float> A(const AmgLevel &L) { return L.A32; }
-    static EllView<float> P(const AmgLevel &L) { return L.P.view32(); }
-    static EllView<float> R(const AmgLevel &L) { return L.R.view32(); }
-    static CsrView<float> csr(const DCsr &D) { return {D.n, D.rp.p, D.ci.p, D.v32.p}; }
+template <> struct LvlVec<float> {
     static const float *dinv(const AmgLevel &L) { return L.dinv32.p; }
     static float *b(AmgLevel &L) { return L.b32.p; }
     static float *x(AmgLevel &L) { return L.x32.p; }
@@ -670,59 +779,90 @@ template <> struct LvlPtr<float> {
     static const float *cinv(const Amg &a) { return a.cinv32.p; }
 };
 
+// Stored operators of one value precision (DIFF: level operators in difference form)
+template <class V, bool DIFF> struct LvlOps;
+template <> struct LvlOps<double, false> {
+    static EllView<double> A(const AmgLevel &L) { return L.A64; }
+    static CsrView<double> Ac(const AmgLevel &L) { return {L.Ac.n, L.Ac.rp.p, L.Ac.ci.p, L.Ac.v64.p}; }
+    static EllView<double> P(const AmgLevel &L) { return L.P.view64(); }
+    static EllView<double> R(const AmgLevel &L) { return L.R.view64(); }
+    static CsrView<double> Pc(const AmgLevel &L) { return {L.Pc.n, L.Pc.rp.p, L.Pc.ci.p, L.Pc.v64.p}; }
+    static CsrView<double> Rc(const AmgLevel &L) { return {L.Rc.n, L.Rc.rp.p, L.Rc.ci.p, L.Rc.v64.p}; }
+};
+template <> struct LvlOps<float, false> {
+    static EllView<float> A(const AmgLevel &L) { return L.A32; }
+    static CsrView<float> Ac(const AmgLevel &L) { return {L.Ac.n, L.Ac.rp.p, L.Ac.ci.p, L.Ac.v32.p}; }
+    static EllView<float> P(const AmgLevel &L) { return L.P.view32(); }
+    static EllView<float> R(const AmgLevel &L) { return L.R.view32(); }
+    static CsrView<float> Pc(const AmgLevel &L) { return {L.Pc.n, L.Pc.rp.p, L.Pc.ci.p, L.Pc.v32.p}; }
+    static CsrView<float> Rc(const AmgLevel &L) { return {L.Rc.n, L.Rc.rp.p, L.Rc.ci.p, L.Rc.v32.p}; }
+};
+template <> struct LvlOps<float, true> : LvlOps<float, false> {
+    static EllView<float> A(const AmgLevel &L) { return L.Ad32; }
+    static CsrView<float> Ac(const AmgLevel &L) { return {L.Acd.n, L.Acd.rp.p, L.Acd.ci.p, L.Acd.v32.p}; }
+};
+
 static unsigned sblocks(int n) { return (unsigned)(((n + SLICE - 1) / SLICE + 7) / 8); }
 
 // launch one fused level operation with the operator's tuned schedule
-template <class T, int EP>
-static int level_op(int mode, const EllView<T> &E, const CsrView<T> &Cv, const T *u, const T *b,
+template <class T, class V, bool DIFF, int EP>
+static int level_op(int mode, const EllView<V> &E, const CsrView<V> &Cv, const T *u, const T *b,
                     const T *dinv, T *d, T *x, T *y, const ChebC &c, const int *done,
                     cudaStream_t s) {
     const int n = E.nrows;
     switch (mode) {
-    case 0: k_level<T, EP><<<sblocks(n), 256, 0, s>>>(E, u, b, dinv, d, x, y, c, done); break;
-    case 1: k_level_csr<T, 4, EP><<<(unsigned)((n * 4 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
-    case 2: k_level_csr<T, 8, EP><<<(unsigned)((n * 8 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
-    case 3: k_level_csr<T, 16, EP><<<(unsigned)((n * 16 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
-    default: k_level_csr<T, 32, EP><<<(unsigned)(((size_t)n * 32 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
+    case 0: k_level<T, V, DIFF, EP><<<sblocks(n), 256, 0, s>>>(E, u, b, dinv, d, x, y, c, done); break;
+    case 1: k_level_csr<T, V, 4, DIFF, EP><<<(unsigned)((n * 4 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
+    case 2: k_level_csr<T, V, 8, DIFF, EP><<<(unsigned)((n * 8 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
+    case 3: k_level_csr<T, V, 16, DIFF, EP><<<(unsigned)((n * 16 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
+    default: k_level_csr<T, V, 32, DIFF, EP><<<(unsigned)(((size_t)n * 32 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
     }
     MP_CHECK_LAUNCH();
     return MP_OK;
 }
 
-template <class T>
+// V(1,1) cycle from level l: T vectors, V stored values, DIFF level operators
+template <class T, class V, bool DIFF>
 static int vcycle(const Amg &a, size_t l, const T *b, T *x, const int *done, cudaStream_t s) {
-    using LP = LvlPtr<T>;
+    using LV = LvlVec<T>;
+    using LO = LvlOps<V, DIFF>;
     AmgLevel &L = *a.L[l];
     if (l + 1 == a.L.size()) {
-        k_coarse<T><<<(unsigned)((a.nc + 7) / 8), 256, 0, s>>>(a.nc, LP::cinv(a), b, x, done);
+        k_coarse<T><<<(unsigned)((a.nc + 7) / 8), 256, 0, s>>>(a.nc, LV::cinv(a), b, x, done);
         MP_CHECK_LAUNCH();
         return MP_OK;
     }
     AmgLevel &N = *a.L[l + 1];
     const ChebC c = cheb_consts(L.lmax);
-    const EllView<T> A = LP::A(L);
-    const CsrView<T> Ac = LP::csr(L.Ac), Pc = LP::csr(L.Pc), Rc = LP::csr(L.Rc);
-    const T *dinv = LP::dinv(L);
-    T *d = LP::d(L), *r = LP::r(L);
+    const EllView<V> A = LO::A(L);
+    const CsrView<V> Ac = LO::Ac(L), Pc = LO::Pc(L), Rc = LO::Rc(L);
+    const T *dinv = LV::dinv(L);
+    T *d = LV::d(L), *r = LV::r(L);
     const unsigned vb = (unsigned)std::min((L.n + 255) / 256, sm_count() * 8);
     const int mA = l == 0 ? 0 : L.sA.mode;
     k_cheb_start<T><<<vb, 256, 0, s>>>(L.n, b, dinv, d, (T)c.inv_theta, done);
     MP_CHECK_LAUNCH();
-    MP_TRY((level_op<T, EP_CHEB_PRE>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
-    MP_TRY((level_op<T, EP_RESID>(mA, A, Ac, x, b, dinv, d, x, r, c, done, s)));
-    MP_TRY((level_op<T, EP_PLAIN>(L.sR.mode, LP::R(L), Rc, r, nullptr, nullptr, nullptr, nullptr,
-                                  LP::b(N), c, done, s)));
-    MP_TRY(vcycle<T>(a, l + 1, LP::b(N), LP::x(N), done, s));
-    MP_TRY((level_op<T, EP_PROLONG>(L.sP.mode, LP::P(L), Pc, LP::x(N), nullptr, nullptr, nullptr,
-                                    x, nullptr, c, done, s)));
-    MP_TRY((level_op<T, EP_CHEB_POST1>(mA, A, Ac, x, b, dinv, d, x, nullptr, c, done, s)));
-    MP_TRY((level_op<T, EP_CHEB_POST2>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
+    MP_TRY((level_op<T, V, DIFF, EP_CHEB_PRE>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
+    MP_TRY((level_op<T, V, DIFF, EP_RESID>(mA, A, Ac, x, b, dinv, d, x, r, c, done, s)));
+    MP_TRY((level_op<T, V, false, EP_PLAIN>(L.sR.mode, LO::R(L), Rc, r, nullptr, nullptr, nullptr,
+                                            nullptr, LV::b(N), c, done, s)));
+    MP_TRY((vcycle<T, V, DIFF>(a, l + 1, LV::b(N), LV::x(N), done, s)));
+    MP_TRY((level_op<T, V, false, EP_PROLONG>(L.sP.mode, LO::P(L), Pc, LV::x(N), nullptr, nullptr,
+                                              nullptr, x, nullptr, c, done, s)));
+    MP_TRY((level_op<T, V, DIFF, EP_CHEB_POST1>(mA, A, Ac, x, b, dinv, d, x, nullptr, c, done, s)));
+    MP_TRY((level_op<T, V, DIFF, EP_CHEB_POST2>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
     return MP_OK;
 }
 
 template <class T>
 int amg_apply(const Amg &a, const T *in, T *out, const int *done, cudaStream_t s) {
-    return vcycle<T>(a, 0, in, out, done, s);
+    if constexpr (std::is_same<T, double>::value) {
+        if (a.store == AMG_MG32)
+            return vcycle<double, float, true>(a, 0, in, out, done, s);
+        return vcycle<double, double, false>(a, 0, in, out, done, s);
+    } else {
+        return vcycle<float, float, false>(a, 0, in, out, done, s);
+    }
 }
 template int amg_apply<double>(const Amg &, const double *, double *, const int *, cudaStream_t);
 template int amg_apply<float>(const Amg &, const float *, float *, const int *, cudaStream_t);
@@ -752,8 +892,8 @@ static int tune_one(const Ell &E, const DCsr &D, bool allow_sell, OpSched &out, 
         float ms_best = 1e30f;
         for (int rep = 0; rep < 4 && rc == MP_OK; rep++) {
             cudaEventRecord(e0, s);
-            rc = level_op<double, EP_PLAIN>(mode, E.view64(), Cv, u.p, nullptr, nullptr, nullptr,
-                                            nullptr, y.p, c, zero, s);
+            rc = level_op<double, double, false, EP_PLAIN>(mode, E.view64(), Cv, u.p, nullptr,
+                                                           nullptr, nullptr, nullptr, y.p, c, zero, s);
             cudaEventRecord(e1, s);
             cudaEventSynchronize(e1);
             float ms = 0;

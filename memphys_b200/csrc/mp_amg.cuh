@@ -52,7 +52,16 @@ struct AmgLevel {
     // work vectors (b, x, d, r) per precision
     dbuf<double> b, x, d, r;
     dbuf<float> b32, x32, d32, r32;
+    // AMG_MG32: the level operator in FP32 difference form, self entry first in
+    // every row holding the row sum s_i: (A u)_i = s_i u_i + sum_k a_ik (u_k - u_i).
+    // Level 0 shares the PPE operator's columns and stores only values.
+    Ell Ad;
+    EllView<float> Ad32{};
+    DCsr Acd;
 };
+
+// storage of the multigrid hierarchy
+enum { AMG_F64 = 0, AMG_F32 = 1, AMG_MG32 = 2 };
 
 struct Amg {
     std::vector<AmgLevel *> L;
@@ -60,14 +69,16 @@ struct Amg {
     dbuf<double> cinv;                // (nc+1)^2 bordered inverse, row-major
     dbuf<float> cinv32;
     double setup_seconds = 0;
+    int store = AMG_F64;
     dbuf<int> zero_flag;              // a device 0 used as `done` while autotuning
     ~Amg();
 };
 
-int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, bool mixed, cudaStream_t s);
+int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t s);
 void amg_destroy(Amg *a);
 // out = V-cycle(in) on the first n0 entries (the border entry is handled by
-// the caller); kernels return immediately while *done is set
+// the caller); kernels return immediately while *done is set.  FP64 vectors use
+// the FP32 difference-form operators when the hierarchy was built with AMG_MG32.
 template <class T>
 int amg_apply(const Amg &a, const T *in, T *out, const int *done, cudaStream_t s);
 

@@ -72,6 +72,8 @@ CloudView cloud_view(mp_cloud_s *c) {
     return v;
 }
 
+const double *cloud_xyz(mp_cloud_s *c) { return c->xyz.p; }
+
 const Ell *cloud_operator(mp_cloud_s *c, int which) {
     if (which < 0 || which > 3 || !c->ops[which].v64.p)
         return nullptr;

@@ -16,6 +16,7 @@ struct CloudView {
 };
 
 CloudView cloud_view(mp_cloud_s *c);
+const double *cloud_xyz(mp_cloud_s *c);
 const Ell *cloud_operator(mp_cloud_s *c, int which);
 std::shared_ptr<Ell> cloud_cols(mp_cloud_s *c);
 // copy operator `which` (sliced) into dst, zeroing rows outside the mask

@@ -16,7 +16,9 @@
 // operators it applies.  With graphs enabled the whole step (including the
 // solver's device-controlled while loop) is a single graph launch.
 #include <cmath>
+#include <cstring>
 #include "mp_cloud.cuh"
+#include "mp_mlp.cuh"
 #include "mp_ppe.cuh"
 
 namespace mp {
@@ -241,13 +243,60 @@ __global__ void k_vel_neumann(int nb, const int *__restrict__ rows, const int *_
 __global__ void k_step_log(int *step, const BicgScalars *S, double *log, int cap, const double *x,
                            int nv, int bordered, int mixed) {
     const int s = *step;
-    double *e = log + 4 * (size_t)(s % cap);
-    // mixed precision: inner sweeps + 1e6 * refinement sweeps (decoded by the caller)
-    e[0] = mixed ? S->total_inner + 1.0e6 * S->outer_it : S->it;
+    double *e = log + MP_LOG_FIELDS * (size_t)(s % cap);
+    e[0] = mixed ? S->total_inner : S->it;
     e[1] = S->b64_sq > 0 ? sqrt(S->rr_true / S->b64_sq) : 0.0;
     e[2] = sqrt(S->rr_true);
     e[3] = bordered ? x[nv] : 0.0;
+    e[4] = S->relres0;
+    e[5] = mixed ? S->outer_it : 0;
+    e[6] = 0.0;
+    e[7] = 0.0;
     *step = s + 1;
+}
+
+// start of the guess stage: pcur = p^n (x on entry), then the non-learned guesses
+__global__ void k_guess(int nsys, int mode, double *x, double *pcur, const double *ph1,
+                        const int *step) {
+    const int stride = gridDim.x * blockDim.x;
+    const bool have_prev = *step >= 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += stride) {
+        const double pn = x[i];
+        pcur[i] = pn;
+        if (mode == MP_GUESS_ZERO)
+            x[i] = 0.0;
+        else if (mode == MP_GUESS_EXTRAPOLATE && have_prev)
+            x[i] = 2.0 * pn - ph1[i];
+    }
+}
+
+// end of a step: p^{n-2} <- p^{n-1}, p^{n-1} <- p^n
+__global__ void k_hist_rotate(int nsys, const double *pcur, double *ph1, double *ph2) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += stride) {
+        ph2[i] = ph1[i];
+        ph1[i] = pcur[i];
+    }
+}
+
+// distance from each node to its nearest stencil member
+__global__ void k_spacing(int nv, int dim, int K, const int *cols, const double *xyz, float *h) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv)
+        return;
+    double best = 1e300;
+    for (int k = 0; k < K; k++) {
+        const int j = cols[ell_index(i, k, K)];
+        if (j == i)
+            continue;
+        double d2 = 0;
+        for (int e = 0; e < dim; e++) {
+            const double t = xyz[(size_t)i * dim + e] - xyz[(size_t)j * dim + e];
+            d2 += t * t;
+        }
+        best = fmin(best, d2);
+    }
+    h[i] = (float)sqrt(best);
 }
 
 }  // namespace mp
@@ -267,6 +316,16 @@ struct mp_fs1_s {
     dbuf<int> step;
     dbuf<double> log;
     int log_cap = 4096;
+    int guess = MP_GUESS_PREVIOUS;
+    // pressure history for the extrapolated and learned guesses
+    dbuf<double> pcur, ph1, ph2, norms;
+    // learned guess
+    Mlp *mlp = nullptr;
+    dbuf<float> hloc;
+    dbuf<int> sidx;
+    int nsample = 0, cap_steps = 0, collect = 0;
+    dbuf<uint16_t> sX;
+    dbuf<float> st;
     GraphExec graph[2];
     int kcounts[3] = {0, 0, 0};  // kernels per step / per sweep / per refinement sweep
     int cur = 0;
@@ -274,6 +333,22 @@ struct mp_fs1_s {
 };
 
 namespace mp {
+
+static MlpFields fs1_fields(mp_fs1_s *f) {
+    const CloudView cv = cloud_view(f->c);
+    MlpFields F;
+    F.nv = f->nv;
+    F.K = f->K;
+    F.cols = cv.cols;
+    F.b = f->P.W.b64.p;
+    F.pcur = f->pcur.p;
+    F.ph1 = f->ph1.p;
+    F.ph2 = f->ph2.p;
+    F.hloc = f->hloc.p;
+    F.bflag = f->bflag.p;
+    F.norms = f->norms.p;
+    return F;
+}
 
 static int fs1_issue_pre(mp_fs1_s *f, int cur, cudaStream_t s) {
     CloudView cv = cloud_view(f->c);
@@ -300,6 +375,18 @@ static int fs1_issue_pre(mp_fs1_s *f, int cur, cudaStream_t s) {
                                        f->pdir.p, f->normal.p, f->P.W.x.p, f->P.W.b64.p, f->k);
     }
     MP_CHECK_LAUNCH();
+    if (f->guess != MP_GUESS_PREVIOUS || f->collect) {
+        const int ns = f->P.sys.nsys;
+        const int gmode = f->guess == MP_GUESS_LEARNED ? MP_GUESS_PREVIOUS : f->guess;
+        k_guess<<<(unsigned)std::min((ns + 255) / 256, sm_count() * 4), 256, 0, s>>>(
+            ns, gmode, f->P.W.x.p, f->pcur.p, f->ph1.p, f->step.p);
+        MP_CHECK_LAUNCH();
+        if (f->guess == MP_GUESS_LEARNED) {
+            const MlpFields F = fs1_fields(f);
+            MP_TRY(mlp_norms(F, f->norms.p, f->P.W.partials.p, f->P.W.ticket.p, s));
+            MP_TRY(mlp_predict_fields(*f->mlp, F, f->P.W.x.p, f->step.p, s));
+        }
+    }
     return MP_OK;
 }
 
@@ -332,6 +419,19 @@ static int fs1_issue_post(mp_fs1_s *f, int cur, cudaStream_t s) {
             k_vel_neumann<3><<<bb, 128, 0, s>>>(f->n_neumann, f->nrows.p, cv.cols, cv.w[0], cv.w[1],
                                                  cv.w[2], f->normal.p, f->vdir[0].p, f->vdir[1].p,
                                                  d2, vn, f->K);
+        MP_CHECK_LAUNCH();
+    }
+    if (f->collect) {  // samples for the learned guess: features of this step, solved increment
+        const MlpFields F = fs1_fields(f);
+        if (f->guess != MP_GUESS_LEARNED)
+            MP_TRY(mlp_norms(F, f->norms.p, f->P.W.partials.p, f->P.W.ticket.p, s));
+        MP_TRY(mlp_collect(F, f->sidx.p, f->nsample, f->P.W.x.p, f->sX.p, f->st.p, f->step.p,
+                           f->cap_steps, s));
+    }
+    if (f->guess != MP_GUESS_PREVIOUS || f->collect) {
+        const int ns = f->P.sys.nsys;
+        k_hist_rotate<<<(unsigned)std::min((ns + 255) / 256, sm_count() * 4), 256, 0, s>>>(
+            ns, f->pcur.p, f->ph1.p, f->ph2.p);
         MP_CHECK_LAUNCH();
     }
     k_step_log<<<1, 1, 0, s>>>(f->step.p, f->P.W.scal.p, f->log.p, f->log_cap, f->P.W.x.p, f->nv,
@@ -412,6 +512,7 @@ extern "C" int mp_fs1_create(mp_cloud c, const uint8_t *boundary, const double *
                     cfg->temporal_order);
     if (!(cfg->dt > 0))
         return fail(MP_BAD_ARG, "dt must be positive");
+    MP_TRY(solver_cfg_check(*solver));
     mp_fs1 f = new mp_fs1_s;
     f->c = c;
     f->nv = nv;
@@ -464,8 +565,19 @@ extern "C" int mp_fs1_create(mp_cloud c, const uint8_t *boundary, const double *
             return bail(rc);
         cudaMemcpy(f->nrows.p, rows.data(), sizeof(int) * rows.size(), cudaMemcpyHostToDevice);
     }
-    if ((rc = f->step.alloc(1)) || (rc = f->log.alloc(4 * (size_t)f->log_cap)))
+    const int ns = f->P.sys.nsys;
+    if ((rc = f->step.alloc(1)) || (rc = f->log.alloc(MP_LOG_FIELDS * (size_t)f->log_cap)) ||
+        (rc = f->pcur.alloc(ns)) || (rc = f->ph1.alloc(ns)) || (rc = f->ph2.alloc(ns)) ||
+        (rc = f->norms.alloc(2)))
         return bail(rc);
+    for (dbuf<double> *b : {&f->pcur, &f->ph1, &f->ph2})
+        cudaMemset(b->p, 0, sizeof(double) * ns);
+    f->guess = solver->guess;
+    if (f->guess < MP_GUESS_PREVIOUS || f->guess > MP_GUESS_EXTRAPOLATE)
+        return bail(fail(MP_BAD_ARG, "unknown initial-guess mode %d", f->guess));
+    if (f->guess == MP_GUESS_LEARNED)
+        return bail(fail(MP_BAD_ARG, "the learned guess needs a network: mp_fs1_attach_mlp, then "
+                                     "mp_fs1_set_guess"));
     cudaMemset(f->step.p, 0, sizeof(int));
     cudaMemset(f->P.W.x.p, 0, sizeof(double) * f->P.sys.nsys);
     if (cudaDeviceSynchronize() != cudaSuccess)
@@ -540,11 +652,11 @@ extern "C" int mp_fs1_last_stats(mp_fs1 f, int *iters, double *relres, double *a
     MP_CUDA(cudaMemcpy(&step, f->step.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (step <= 0)
         return fail(MP_BAD_ARG, "no step has been taken");
-    double e[4];
-    MP_CUDA(cudaMemcpy(e, f->log.p + 4 * (size_t)((step - 1) % f->log_cap), sizeof(e),
+    double e[MP_LOG_FIELDS];
+    MP_CUDA(cudaMemcpy(e, f->log.p + MP_LOG_FIELDS * (size_t)((step - 1) % f->log_cap), sizeof(e),
                        cudaMemcpyDeviceToHost));
     if (iters)
-        *iters = (int)std::fmod(e[0], 1.0e6);
+        *iters = (int)e[0];
     if (relres)
         *relres = e[1];
     if (abs_res)
@@ -564,8 +676,122 @@ extern "C" int mp_fs1_log(mp_fs1 f, int first, int count, double *out) {
         return fail(MP_BAD_ARG, "mp_fs1_log: steps %d..%d not in the log (last step %d)", first,
                     first + count - 1, step - 1);
     for (int i = 0; i < count; i++)
-        MP_CUDA(cudaMemcpy(out + 4 * (size_t)i, f->log.p + 4 * (size_t)((first + i) % f->log_cap),
-                           4 * sizeof(double), cudaMemcpyDeviceToHost));
+        MP_CUDA(cudaMemcpy(out + MP_LOG_FIELDS * (size_t)i,
+                           f->log.p + MP_LOG_FIELDS * (size_t)((first + i) % f->log_cap),
+                           MP_LOG_FIELDS * sizeof(double), cudaMemcpyDeviceToHost));
+    return MP_OK;
+}
+
+static void fs1_invalidate(mp_fs1 f) {
+    f->graph[0].reset();
+    f->graph[1].reset();
+    for (int q = 0; q < 3; q++)
+        f->kcounts[q] = 0;
+}
+
+extern "C" int mp_fs1_attach_mlp(mp_fs1 f, mp_mlp m, int sample_nodes, int capacity_steps,
+                                 int collect) {
+    if (!f || !m || sample_nodes <= 0 || capacity_steps <= 0)
+        return fail(MP_BAD_ARG, "mp_fs1_attach_mlp: bad arguments");
+    MP_CUDA(cudaDeviceSynchronize());
+    f->mlp = mlp_of(m);
+    const int nv = f->nv;
+    // node spacing feature: distance to the nearest stencil member over its mean
+    MP_TRY(f->hloc.alloc(nv));
+    {
+        CloudView cv = cloud_view(f->c);
+        k_spacing<<<(nv + 255) / 256, 256>>>(nv, f->dim, f->K, cv.cols, cloud_xyz(f->c), f->hloc.p);
+        MP_CHECK_LAUNCH();
+        std::vector<float> h(nv);
+        MP_CUDA(cudaMemcpy(h.data(), f->hloc.p, sizeof(float) * nv, cudaMemcpyDeviceToHost));
+        double mean = 0;
+        for (float v : h)
+            mean += v;
+        mean /= nv;
+        for (float &v : h)
+            v = (float)(v / mean);
+        MP_CUDA(cudaMemcpy(f->hloc.p, h.data(), sizeof(float) * nv, cudaMemcpyHostToDevice));
+    }
+    // a fixed pseudo-random sample of nodes whose features are recorded each step
+    f->nsample = std::min(sample_nodes, nv);
+    std::vector<int> all(nv);
+    for (int i = 0; i < nv; i++)
+        all[i] = i;
+    uint64_t st = 0x2545F4914F6CDD1Dull;
+    for (int i = 0; i < f->nsample; i++) {  // partial Fisher-Yates
+        st ^= st << 13;
+        st ^= st >> 7;
+        st ^= st << 17;
+        const int j = i + (int)(st % (uint64_t)(nv - i));
+        std::swap(all[i], all[j]);
+    }
+    std::sort(all.begin(), all.begin() + f->nsample);
+    MP_TRY(f->sidx.alloc(f->nsample));
+    MP_CUDA(cudaMemcpy(f->sidx.p, all.data(), sizeof(int) * f->nsample, cudaMemcpyHostToDevice));
+    f->cap_steps = capacity_steps;
+    MP_TRY(f->sX.alloc((size_t)capacity_steps * f->nsample * MLP_IN));
+    MP_TRY(f->st.alloc((size_t)capacity_steps * f->nsample));
+    f->collect = collect ? 1 : 0;
+    fs1_invalidate(f);
+    return MP_OK;
+}
+
+extern "C" int mp_fs1_set_guess(mp_fs1 f, int guess) {
+    if (!f || guess < MP_GUESS_PREVIOUS || guess > MP_GUESS_EXTRAPOLATE)
+        return fail(MP_BAD_ARG, "mp_fs1_set_guess: unknown mode %d", guess);
+    if (guess == MP_GUESS_LEARNED && !f->mlp)
+        return fail(MP_BAD_ARG, "the learned guess needs mp_fs1_attach_mlp first");
+    if (guess != f->guess) {
+        f->guess = guess;
+        fs1_invalidate(f);
+    }
+    return MP_OK;
+}
+
+extern "C" int mp_fs1_train_mlp(mp_fs1 f, int epochs, int batch, double lr, uint64_t seed,
+                                double *loss) {
+    if (!f || !f->mlp)
+        return fail(MP_BAD_ARG, "mp_fs1_train_mlp: no network attached");
+    MP_CUDA(cudaDeviceSynchronize());
+    int step = 0;
+    MP_CUDA(cudaMemcpy(&step, f->step.p, sizeof(int), cudaMemcpyDeviceToHost));
+    const int steps = std::min(std::max(step - 2, 0), f->cap_steps);
+    const int n = steps * f->nsample;
+    if (n < batch)
+        return fail(MP_BAD_ARG, "only %d samples recorded (batch %d)", n, batch);
+    return mlp_train(*f->mlp, f->sX.p, f->st.p, n, epochs, batch, lr, seed, loss, 0);
+}
+
+extern "C" int mp_fs1_samples(mp_fs1 f, float *X, float *t, int *nodes, int cap, int *n) {
+    if (!f || !n || cap < 0)
+        return fail(MP_BAD_ARG, "mp_fs1_samples: bad arguments");
+    if (!f->mlp)
+        return fail(MP_BAD_ARG, "mp_fs1_samples: no network attached");
+    MP_CUDA(cudaDeviceSynchronize());
+    int step = 0;
+    MP_CUDA(cudaMemcpy(&step, f->step.p, sizeof(int), cudaMemcpyDeviceToHost));
+    const int rows = std::min(std::max(step - 2, 0), f->cap_steps) * f->nsample;
+    *n = rows;
+    const int m = std::min(rows, cap);
+    if (m == 0)
+        return MP_OK;
+    if (X) {
+        std::vector<uint16_t> h((size_t)m * MLP_IN);
+        MP_CUDA(cudaMemcpy(h.data(), f->sX.p, h.size() * 2, cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < h.size(); q++) {
+            const uint32_t u = (uint32_t)h[q] << 16;
+            std::memcpy(X + q, &u, 4);
+        }
+    }
+    if (t)
+        MP_CUDA(cudaMemcpy(t, f->st.p, sizeof(float) * m, cudaMemcpyDefault));
+    if (nodes) {
+        std::vector<int> idx(f->nsample);
+        MP_CUDA(cudaMemcpy(idx.data(), f->sidx.p, sizeof(int) * f->nsample,
+                           cudaMemcpyDeviceToHost));
+        for (int r = 0; r < m; r++)
+            nodes[r] = idx[r % f->nsample];
+    }
     return MP_OK;
 }
 

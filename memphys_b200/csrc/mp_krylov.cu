@@ -95,6 +95,8 @@ __global__ void __launch_bounds__(KT)
             bb += (double)b[nv] * b[nv];
         }
         S->b_sq = bb;
+        if (!ZERO_X)  // FP64 solves: the initial guess's residual (mixed: set by the outer residual)
+            S->relres0 = bb > 0 ? sqrt(rr / bb) : 0.0;
         S->r0_sq = rr;
         S->rr = rr;
         S->rho_old = 1.0;
@@ -375,6 +377,8 @@ __global__ void __launch_bounds__(KT)
         }
         S->rr_true = rr;
         S->b64_sq = bb;
+        if (refine && S->outer_it == 0)
+            S->relres0 = bb > 0 ? sqrt(rr / bb) : 0.0;
         if (refine) {  // iterative-refinement loop control
             int done = !(rr > S->tol_outer2 * bb && S->outer_it < S->outer_max);
             if (bb == 0.0)
@@ -623,7 +627,7 @@ int Ppe::issue_ir_setup(cudaStream_t st) {
 
 // Build the whole solve (prologue, while loop(s), epilogue) into `gb`.
 int Ppe::build_solve_graph(GraphBuilder &gb) {
-    if (cfg.precision == MP_FP64) {
+    if (cfg.precision != MP_FP32) {
         cudaGraphConditionalHandle h;
         MP_TRY(gb.make_handle(&h));
         MP_TRY(gb.captured([&](cudaStream_t s) { return issue_prologue64(h, s); }));
@@ -662,7 +666,7 @@ int Ppe::solve_eager(cudaStream_t st) {
         MP_CUDA(cudaStreamSynchronize(st));
         return MP_OK;
     };
-    if (cfg.precision == MP_FP64) {
+    if (cfg.precision != MP_FP32) {
         MP_TRY(issue_prologue64(0, st));
         for (int it = 0;; it++) {
             if (it % poll == 0) {
@@ -723,7 +727,7 @@ int Ppe::read_stats(cudaStream_t st, SolveStats *out) {
     BicgScalars hs;
     MP_CUDA(cudaMemcpyAsync(&hs, W.scal.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
     MP_CUDA(cudaStreamSynchronize(st));
-    out->iters = cfg.precision == MP_FP64 ? hs.it : hs.total_inner;
+    out->iters = cfg.precision != MP_FP32 ? hs.it : hs.total_inner;
     out->outer = hs.outer_it;
     out->abs_res = std::sqrt(hs.rr_true);
     out->relres = hs.b64_sq > 0 ? std::sqrt(hs.rr_true / hs.b64_sq) : 0.0;
@@ -784,7 +788,7 @@ int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet
     MP_CUDA(cudaStreamSynchronize(st));
     if (hbad)
         return fail(MP_BAD_ARG, "%d stencils do not start with their own node", hbad);
-    const bool mixed = cfg.precision == MP_FP32;
+    const bool mixed = cfg.precision == MP_FP32;  // FP32 Krylov + FP64 refinement
     if (mixed)
         MP_TRY(ell_make_fp32(sys.A, st));
     MP_TRY(sys.dinv.alloc(nv));
@@ -794,7 +798,8 @@ int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet
                                                    mixed ? sys.dinv32.p : nullptr);
     MP_CHECK_LAUNCH();
     if (cfg.precond == MP_PRECOND_AMG) {
-        MP_TRY(amg_create(&sys.amg, sys.A, cfg, mixed, st));
+        MP_TRY(amg_create(&sys.amg, sys.A, cfg,
+                          mixed ? AMG_F32 : (cfg.precision == MP_MG32 ? AMG_MG32 : AMG_F64), st));
     }
     MP_TRY(W.alloc(nv, bordered, mixed, cfg.precond == MP_PRECOND_AMG));
     MP_CUDA(cudaStreamSynchronize(st));
@@ -807,6 +812,19 @@ Ppe::~Ppe() {
         amg_destroy(sys.amg);
     if (capture_stream)
         cudaStreamDestroy(capture_stream);
+}
+
+int solver_cfg_check(const mp_solver_cfg &c) {
+    if (c.tol <= 0 || c.maxit <= 0)
+        return fail(MP_BAD_ARG, "solver tolerance and maxit must be positive");
+    if (c.precision != MP_FP64 && c.precision != MP_FP32 && c.precision != MP_MG32)
+        return fail(MP_BAD_ARG, "precision must be MP_FP64, MP_FP32 or MP_MG32");
+    if (c.precond < MP_PRECOND_NONE || c.precond > MP_PRECOND_AMG)
+        return fail(MP_BAD_ARG, "unknown preconditioner %d", c.precond);
+    if (c.precision == MP_MG32 && c.precond != MP_PRECOND_AMG)
+        return fail(MP_BAD_ARG, "MP_MG32 stores the multigrid preconditioner in FP32: it needs "
+                                "MP_PRECOND_AMG");
+    return MP_OK;
 }
 
 Cfg Cfg::from(const mp_solver_cfg &c) {
@@ -850,12 +868,7 @@ extern "C" int mp_ppe_create(mp_cloud c, const uint8_t *boundary, const uint8_t 
                              const mp_solver_cfg *cfg, mp_ppe *out) {
     if (!c || !boundary || !dirichlet || !normal || !cfg || !out)
         return fail(MP_BAD_ARG, "mp_ppe_create: null argument");
-    if (cfg->tol <= 0 || cfg->maxit <= 0)
-        return fail(MP_BAD_ARG, "solver tolerance and maxit must be positive");
-    if (cfg->precision != MP_FP64 && cfg->precision != MP_FP32)
-        return fail(MP_BAD_ARG, "precision must be MP_FP64 or MP_FP32 (mixed)");
-    if (cfg->precond < MP_PRECOND_NONE || cfg->precond > MP_PRECOND_AMG)
-        return fail(MP_BAD_ARG, "unknown preconditioner %d", cfg->precond);
+    MP_TRY(solver_cfg_check(*cfg));
     mp_ppe p = new mp_ppe_s;
     int rc = p->P.create(c, boundary, dirichlet, normal, unsteady, conv, diff, *cfg, 0);
     if (rc != MP_OK) {

@@ -29,6 +29,7 @@ struct BicgScalars {
     // iterative refinement (outer) state
     int outer_it, outer_max, outer_done, total_inner;
     double tol_outer2, b64_sq;
+    double relres0;     // ||b - A x0|| / ||b|| of the initial guess (first residual of a solve)
 };
 
 struct PpeSystem {

@@ -1,0 +1,764 @@
+// mp_mlp.cu -- the learned pressure-increment network on sm_100a.
+//
+// Forward: one CTA (128 threads) owns a tile of 128 nodes.  The BF16 weights
+// (transposed) and the tile's features sit in shared memory in the canonical
+// K-major, non-swizzled core-matrix layout (8 rows x 16 bytes per core
+// matrix; the two 8-element halves of a 16-wide K step 128 bytes apart, the
+// 8-row groups K*16 bytes apart).  One elected thread issues
+// tcgen05.mma.cta_group::1.kind::f16 (M = N = 128, K = 16 per instruction)
+// into a 128-column FP32 accumulator in tensor memory and commits to an
+// mbarrier; every thread then reads its own row back with tcgen05.ld
+// (thread 32w + l owns TMEM lane 32w + l), applies bias + ReLU and writes the
+// BF16 activations back to shared memory as the next layer's A operand.  The
+// output layer is a per-thread dot product on the FP32 activations.
+//
+// Backward (training): CUDA-core kernels on the stored activations (weight
+// gradients reduce over the batch), Adam on FP32 master weights, then the
+// BF16 operand copies are repacked.
+#include <cuda_bf16.h>
+#include <algorithm>
+#include <cmath>
+#include <random>
+#include "mp_mlp.cuh"
+
+namespace mp {
+
+struct Mlp {
+    dbuf<float> theta, m1, m2, grad;
+    dbuf<uint16_t> pack;  // W1t | W2t | W3t in core-matrix layout
+    int adam_t = 0;
+    // training scratch (sized for the largest batch seen)
+    int cap = 0;
+    dbuf<uint16_t> h1, h2;
+    dbuf<float> h3, y, d3, d2, d1, lossbuf;
+    dbuf<int> idx;
+    dbuf<int> err;  // device flag: an mbarrier wait ran out
+};
+
+// ------------------------------------------------------------ layout helpers
+__host__ __device__ __forceinline__ int cm_off(int r, int k, int K) {
+    return (r >> 3) * (K * 8) + (k >> 3) * 64 + (r & 7) * 8 + (k & 7);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// K-major, no swizzle: LBO = 128 B (next K half), SBO = K*16 B (next 8 rows)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, int K) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)(128 >> 4) << 16;
+    d |= (uint64_t)(((uint32_t)K * 16u) >> 4) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+    return d;
+}
+
+// kind::f16 instruction descriptor: FP32 accumulate, BF16 A and B, both
+// K-major, N = 128 (>> 3), M = 128 (>> 4)
+constexpr uint32_t MLP_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) |
+                               ((128u >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db,
+                                          uint32_t accumulate) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+            tmem_d),
+        "l"(da), "l"(db), "r"(MLP_IDESC), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+        smem_u32(mbar)));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
+    const uint32_t a = smem_u32(mbar);
+    for (int i = 0; i < (1 << 22); i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(parity));
+        if (ok)
+            return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+        v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t *>(&h);
+}
+
+__device__ __forceinline__ float bf16_round(float a) {
+    return __bfloat162float(__float2bfloat16_rn(a));
+}
+
+// ---------------------------------------------------------- forward kernel
+enum { MLP_MODE_FIELDS = 0, MLP_MODE_ROWS = 1, MLP_MODE_TRAIN = 2 };
+
+struct MlpFwdArgs {
+    int n;                   // rows
+    const uint16_t *pack;    // packed BF16 weights
+    const float *theta;      // biases and output weights
+    // rows mode: row-major BF16 features, optional index list
+    const uint16_t *X;
+    const int *idx;
+    float *y;                // output (rows/train)
+    // train mode: stored activations
+    uint16_t *h1, *h2;
+    float *h3;
+    // fields mode
+    MlpFields F;
+    double *x;               // initial guess written here
+    const int *step;         // fields mode: skip while *step < 2
+    int *err;
+};
+
+struct MlpSmem {
+    uint16_t w1[MLP_H * MLP_IN];
+    uint16_t w2[MLP_H * MLP_H];
+    uint16_t w3[MLP_H * MLP_H];
+    uint16_t xa[MLP_TILE * MLP_IN];
+    uint16_t ha[MLP_TILE * MLP_H];
+    float bias[3][MLP_H];
+    float w4[MLP_H];
+    uint64_t mbar;
+    uint32_t tmem;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpFwdArgs A) {
+    extern __shared__ __align__(1024) unsigned char mlp_smem_raw[];
+    MlpSmem &S = *reinterpret_cast<MlpSmem *>(mlp_smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (MODE == MLP_MODE_FIELDS && *A.step < 2)
+        return;  // no pressure history yet: the guess stays p^n
+    // weights (already in operand layout) and vectors into shared memory
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(A.pack);
+        uint4 *dst = reinterpret_cast<uint4 *>(S.w1);  // w1, w2, w3 are contiguous
+        for (int i = tid; i < MLP_PACK / 8; i += blockDim.x)
+            dst[i] = src[i];
+        for (int i = tid; i < MLP_H; i += blockDim.x) {
+            S.bias[0][i] = A.theta[MLP_OFF_B1 + i];
+            S.bias[1][i] = A.theta[MLP_OFF_B2 + i];
+            S.bias[2][i] = A.theta[MLP_OFF_B3 + i];
+            S.w4[i] = A.theta[MLP_OFF_W4 + i];
+        }
+    }
+    if (tid == 0)
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&S.mbar)));
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_u32(&S.tmem)),
+                     "r"(MLP_H));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = S.tmem;
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    const float b4 = A.theta[MLP_OFF_B4];
+    uint32_t phase = 0;
+    bool ok = true;
+    const int ntiles = (A.n + MLP_TILE - 1) / MLP_TILE;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int row = tile * MLP_TILE + tid;
+        const bool live = row < A.n;
+        // ---- features of this thread's row into the A operand
+        if (MODE == MLP_MODE_FIELDS) {
+            const MlpFields &F = A.F;
+            float f[MLP_IN];
+#pragma unroll
+            for (int k = 0; k < MLP_IN; k++)
+                f[k] = 0.f;
+            if (live) {
+                const double sb = F.norms[0], sp = F.norms[1];
+                const size_t base = (size_t)(row / 64) * F.K * 64 + (row % 64);
+#pragma unroll 4
+                for (int k = 0; k < MLP_STENCIL; k++) {
+                    const int j = F.cols[base + (size_t)k * 64];
+                    const double pc = F.pcur[j], p1 = F.ph1[j];
+                    f[3 * k] = (float)(F.b[j] * sb);
+                    f[3 * k + 1] = (float)((pc - p1) * sp);
+                    f[3 * k + 2] = (float)((p1 - F.ph2[j]) * sp);
+                }
+                f[60] = F.hloc[row];
+                f[61] = F.bflag[row] ? 1.f : 0.f;
+                f[62] = 1.f;
+            }
+#pragma unroll
+            for (int c = 0; c < MLP_IN; c += 8) {
+                uint4 v;
+                v.x = pack_bf16x2(f[c], f[c + 1]);
+                v.y = pack_bf16x2(f[c + 2], f[c + 3]);
+                v.z = pack_bf16x2(f[c + 4], f[c + 5]);
+                v.w = pack_bf16x2(f[c + 6], f[c + 7]);
+                *reinterpret_cast<uint4 *>(&S.xa[cm_off(tid, c, MLP_IN)]) = v;
+            }
+        } else {
+            const int src = live ? (A.idx ? A.idx[row] : row) : 0;
+            const uint4 *xr = reinterpret_cast<const uint4 *>(A.X + (size_t)src * MLP_IN);
+#pragma unroll
+            for (int c = 0; c < MLP_IN; c += 8) {
+                uint4 v = live ? xr[c / 8] : make_uint4(0, 0, 0, 0);
+                *reinterpret_cast<uint4 *>(&S.xa[cm_off(tid, c, MLP_IN)]) = v;
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncthreads();
+        float out = b4;
+        for (int layer = 0; layer < 3; layer++) {
+            const int K = layer == 0 ? MLP_IN : MLP_H;
+            const uint16_t *Ab = layer == 0 ? S.xa : S.ha;
+            const uint16_t *Bw = layer == 0 ? S.w1 : (layer == 1 ? S.w2 : S.w3);
+            if (tid == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t a0 = smem_u32(Ab), b0 = smem_u32(Bw);
+                for (int k0 = 0; k0 < K; k0 += 16) {
+                    const uint32_t koff = (uint32_t)(k0 / 8) * 128u;
+                    umma_bf16(tmem, umma_desc(a0 + koff, K), umma_desc(b0 + koff, K), k0 > 0);
+                }
+                umma_commit(&S.mbar);
+            }
+            if (!mbar_wait(&S.mbar, phase))
+                ok = false;
+            phase ^= 1u;
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            // ---- epilogue: this thread's row of the accumulator
+#pragma unroll 1
+            for (int c0 = 0; c0 < MLP_H; c0 += 16) {
+                float v[16];
+                tmem_ld16(lane_addr + (uint32_t)c0, v);
+#pragma unroll
+                for (int i = 0; i < 16; i++)
+                    v[i] = fmaxf(v[i] + S.bias[layer][c0 + i], 0.f);
+                if (layer < 2) {
+#pragma unroll
+                    for (int h = 0; h < 16; h += 8) {
+                        uint4 q;
+                        q.x = pack_bf16x2(v[h], v[h + 1]);
+                        q.y = pack_bf16x2(v[h + 2], v[h + 3]);
+                        q.z = pack_bf16x2(v[h + 4], v[h + 5]);
+                        q.w = pack_bf16x2(v[h + 6], v[h + 7]);
+                        *reinterpret_cast<uint4 *>(&S.ha[cm_off(tid, c0 + h, MLP_H)]) = q;
+                        if (MODE == MLP_MODE_TRAIN && live) {
+                            uint16_t *hg = (layer == 0 ? A.h1 : A.h2) + (size_t)row * MLP_H + c0 + h;
+                            *reinterpret_cast<uint4 *>(hg) = q;
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; i++)
+                        out = fmaf(v[i], S.w4[c0 + i], out);
+                    if (MODE == MLP_MODE_TRAIN && live) {
+                        float4 *hg = reinterpret_cast<float4 *>(A.h3 + (size_t)row * MLP_H + c0);
+#pragma unroll
+                        for (int i = 0; i < 4; i++)
+                            hg[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                    }
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            __syncthreads();
+        }
+        if (live) {
+            if (MODE == MLP_MODE_FIELDS)
+                A.x[row] = A.F.pcur[row] + (double)out / A.F.norms[1];
+            else
+                A.y[row] = out;
+        }
+    }
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(MLP_H));
+    if (!ok && tid == 0 && A.err)
+        atomicExch(A.err, 1);
+}
+
+// ------------------------------------------------------------ small kernels
+// FP32 master weights -> transposed BF16 operand copies
+__global__ void k_mlp_pack(const float *theta, uint16_t *pack) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= MLP_PACK)
+        return;
+    int n, k, K, off;
+    float w;
+    if (i < MLP_H * MLP_IN) {  // W1t[n][k] = W1[k][n]
+        n = i / MLP_IN;
+        k = i % MLP_IN;
+        K = MLP_IN;
+        w = theta[MLP_OFF_W1 + k * MLP_H + n];
+        off = 0;
+    } else {
+        const int j = i - MLP_H * MLP_IN;
+        const int which = j / (MLP_H * MLP_H), r = j % (MLP_H * MLP_H);
+        n = r / MLP_H;
+        k = r % MLP_H;
+        K = MLP_H;
+        w = theta[(which == 0 ? MLP_OFF_W2 : MLP_OFF_W3) + k * MLP_H + n];
+        off = MLP_H * MLP_IN + which * MLP_H * MLP_H;
+    }
+    __nv_bfloat16 h = __float2bfloat16_rn(w);
+    pack[off + cm_off(n, k, K)] = *reinterpret_cast<uint16_t *>(&h);
+}
+
+__device__ __forceinline__ float bf(uint16_t u) {
+    return __uint_as_float((uint32_t)u << 16);
+}
+
+// BF16-rounded weight W_l[k][n] as the forward pass used it
+__device__ __forceinline__ float wq(const float *theta, int off, int k, int n) {
+    return bf16_round(theta[off + k * MLP_H + n]);
+}
+
+// loss, output-layer gradients and dL/dh3 (pre-activation, masked by ReLU)
+__global__ void k_mlp_out_grad(int B, const float *y, const float *t, const int *tidx,
+                               const float *h3, const float *theta, float *d3, float *grad,
+                               float *lossbuf) {
+    const int b = blockIdx.x, c = threadIdx.x;  // blockDim = 128
+    const float tb = t[tidx ? tidx[b] : b];
+    const float dy = 2.f * (y[b] - tb) / (float)B;
+    const float h = h3[(size_t)b * MLP_H + c];
+    d3[(size_t)b * MLP_H + c] = h > 0.f ? dy * theta[MLP_OFF_W4 + c] : 0.f;
+    atomicAdd(&grad[MLP_OFF_W4 + c], dy * h);
+    if (c == 0) {
+        atomicAdd(&grad[MLP_OFF_B4], dy);
+        atomicAdd(lossbuf, (y[b] - tb) * (y[b] - tb) / (float)B);
+    }
+}
+
+// gW[k][n] = sum_b a[b][k] d[b][n], gb[n] = sum_b d[b][n]; a BF16 rows of width Kin
+__global__ void k_mlp_wgrad(int B, int Kin, const uint16_t *a, const int *aidx, const float *d,
+                            float *gW, float *gb) {
+    const int n = threadIdx.x;  // 128
+    const int k = blockIdx.x;   // Kin (+1 row for the bias)
+    float acc = 0.f;
+    if (k < Kin) {
+        for (int b = 0; b < B; b++) {
+            const int r = aidx ? aidx[b] : b;
+            acc = fmaf(bf(a[(size_t)r * Kin + k]), d[(size_t)b * MLP_H + n], acc);
+        }
+        gW[k * MLP_H + n] += acc;
+    } else {
+        for (int b = 0; b < B; b++)
+            acc += d[(size_t)b * MLP_H + n];
+        gb[n] += acc;
+    }
+}
+
+// dprev[b][k] = (sum_n W[k][n] d[b][n]) * (h_prev[b][k] > 0)
+__global__ void k_mlp_dgrad(int B, const float *theta, int woff, const float *d,
+                            const uint16_t *hprev, float *dprev) {
+    const int b = blockIdx.x, k = threadIdx.x;  // blockDim 128
+    __shared__ float ds[MLP_H];
+    ds[k] = d[(size_t)b * MLP_H + k];
+    __syncthreads();
+    float acc = 0.f;
+    for (int n = 0; n < MLP_H; n++)
+        acc = fmaf(wq(theta, woff, k, n), ds[n], acc);
+    dprev[(size_t)b * MLP_H + k] = bf(hprev[(size_t)b * MLP_H + k]) > 0.f ? acc : 0.f;
+}
+
+__global__ void k_mlp_adam(float *theta, float *m1, float *m2, const float *g, int n, float lr,
+                           float bc1, float bc2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float gi = g[i];
+    const float a = b1 * m1[i] + (1.f - b1) * gi;
+    const float v = b2 * m2[i] + (1.f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = v;
+    theta[i] -= lr * (a / bc1) / (sqrtf(v / bc2) + eps);
+}
+
+// spacing feature, norms, sample collection
+__global__ void k_mlp_norms(MlpFields F, double *partials, unsigned *ticket, double *norms) {
+    __shared__ double red[32 * 2];
+    double acc[2] = {0, 0};
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.nv; i += stride) {
+        acc[0] += F.b[i] * F.b[i];
+        const double d = F.pcur[i] - F.ph1[i];
+        acc[1] += d * d;
+    }
+    if (grid_reduce<2>(acc, partials, ticket, red) && threadIdx.x == 0) {
+        const double rb = sqrt(acc[0] / F.nv), rp = sqrt(acc[1] / F.nv);
+        norms[0] = rb > 0 ? 1.0 / rb : 0.0;
+        norms[1] = rp > 0 ? 1.0 / rp : 0.0;
+    }
+}
+
+__global__ void k_mlp_collect(MlpFields F, const int *idx, int nidx, const double *xnew,
+                              uint16_t *X, float *t, const int *step, int cap_steps) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nidx || *step < 2)
+        return;
+    const size_t slot = (size_t)((*step - 2) % cap_steps) * nidx;
+    X += slot * MLP_IN;
+    t += slot;
+    const int i = idx[s];
+    const double sb = F.norms[0], sp = F.norms[1];
+    float f[MLP_IN];
+#pragma unroll
+    for (int k = 0; k < MLP_IN; k++)
+        f[k] = 0.f;
+    const size_t base = (size_t)(i / 64) * F.K * 64 + (i % 64);
+    for (int k = 0; k < MLP_STENCIL; k++) {
+        const int j = F.cols[base + (size_t)k * 64];
+        const double pc = F.pcur[j], p1 = F.ph1[j];
+        f[3 * k] = (float)(F.b[j] * sb);
+        f[3 * k + 1] = (float)((pc - p1) * sp);
+        f[3 * k + 2] = (float)((p1 - F.ph2[j]) * sp);
+    }
+    f[60] = F.hloc[i];
+    f[61] = F.bflag[i] ? 1.f : 0.f;
+    f[62] = 1.f;
+    uint4 *dst = reinterpret_cast<uint4 *>(X + (size_t)s * MLP_IN);
+#pragma unroll
+    for (int c = 0; c < MLP_IN; c += 8) {
+        uint4 v;
+        v.x = pack_bf16x2(f[c], f[c + 1]);
+        v.y = pack_bf16x2(f[c + 2], f[c + 3]);
+        v.z = pack_bf16x2(f[c + 4], f[c + 5]);
+        v.w = pack_bf16x2(f[c + 6], f[c + 7]);
+        dst[c / 8] = v;
+    }
+    t[s] = (float)((xnew[i] - F.pcur[i]) * sp);
+}
+
+__global__ void k_f32_to_bf16(const float *a, uint16_t *b, size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        __nv_bfloat16 h = __float2bfloat16_rn(a[i]);
+        b[i] = *reinterpret_cast<uint16_t *>(&h);
+    }
+}
+
+// --------------------------------------------------------------- host side
+static int fwd_smem() { return (int)sizeof(MlpSmem) + 1024; }
+
+template <int MODE> static int launch_forward(MlpFwdArgs &a, cudaStream_t s) {
+    const int sm = fwd_smem();
+    MP_CUDA(cudaFuncSetAttribute(k_mlp_forward<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    const int tiles = (a.n + MLP_TILE - 1) / MLP_TILE;
+    const int grid = std::max(1, std::min(tiles, sm_count()));
+    k_mlp_forward<MODE><<<grid, 128, sm, s>>>(a);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+static int repack(Mlp &m, cudaStream_t s) {
+    k_mlp_pack<<<(MLP_PACK + 255) / 256, 256, 0, s>>>(m.theta.p, m.pack.p);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+int mlp_create(Mlp **out, uint64_t seed) {
+    Mlp *m = new Mlp;
+    int rc;
+    if ((rc = m->theta.alloc(MLP_NPARAM)) || (rc = m->m1.alloc(MLP_NPARAM)) ||
+        (rc = m->m2.alloc(MLP_NPARAM)) || (rc = m->grad.alloc(MLP_NPARAM)) ||
+        (rc = m->pack.alloc(MLP_PACK)) || (rc = m->err.alloc(1))) {
+        delete m;
+        return rc;
+    }
+    // He-uniform initialisation from a fixed-seed generator (host)
+    std::vector<float> th(MLP_NPARAM, 0.f);
+    std::mt19937_64 g(seed);
+    auto init = [&](int off, int fan_in, int count) {
+        std::uniform_real_distribution<float> u(-std::sqrt(6.f / fan_in), std::sqrt(6.f / fan_in));
+        for (int i = 0; i < count; i++)
+            th[off + i] = u(g);
+    };
+    init(MLP_OFF_W1, MLP_IN, MLP_IN * MLP_H);
+    init(MLP_OFF_W2, MLP_H, MLP_H * MLP_H);
+    init(MLP_OFF_W3, MLP_H, MLP_H * MLP_H);
+    {
+        std::uniform_real_distribution<float> u(-1.f / std::sqrt((float)MLP_H), 1.f / std::sqrt((float)MLP_H));
+        for (int i = 0; i < MLP_H; i++)
+            th[MLP_OFF_W4 + i] = 0.1f * u(g);
+    }
+    MP_CUDA(cudaMemcpy(m->theta.p, th.data(), sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice));
+    MP_CUDA(cudaMemset(m->m1.p, 0, sizeof(float) * MLP_NPARAM));
+    MP_CUDA(cudaMemset(m->m2.p, 0, sizeof(float) * MLP_NPARAM));
+    MP_CUDA(cudaMemset(m->err.p, 0, sizeof(int)));
+    MP_TRY(repack(*m, 0));
+    MP_CUDA(cudaDeviceSynchronize());
+    *out = m;
+    return MP_OK;
+}
+
+void mlp_destroy(Mlp *m) { delete m; }
+
+static int mlp_check_err(Mlp &m, cudaStream_t s) {
+    int e = 0;
+    MP_CUDA(cudaMemcpyAsync(&e, m.err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    if (e)
+        return fail(MP_TIMEOUT, "tensor-core MLP: an mbarrier wait ran out");
+    return MP_OK;
+}
+
+int mlp_predict_fields(Mlp &m, const MlpFields &F, double *x, const int *step, cudaStream_t s) {
+    MlpFwdArgs a{};
+    a.step = step;
+    a.n = F.nv;
+    a.pack = m.pack.p;
+    a.theta = m.theta.p;
+    a.F = F;
+    a.x = x;
+    a.err = m.err.p;
+    return launch_forward<MLP_MODE_FIELDS>(a, s);
+}
+
+int mlp_norms(const MlpFields &F, double *norms, double *partials, unsigned *ticket,
+              cudaStream_t s) {
+    const unsigned g = (unsigned)std::min((F.nv + 255) / 256, sm_count() * 4);
+    k_mlp_norms<<<g, 256, 0, s>>>(F, partials, ticket, norms);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+int mlp_collect(const MlpFields &F, const int *idx, int nidx, const double *xnew, uint16_t *X,
+                float *t, const int *step, int cap_steps, cudaStream_t s) {
+    k_mlp_collect<<<(nidx + 127) / 128, 128, 0, s>>>(F, idx, nidx, xnew, X, t, step, cap_steps);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+static int ensure_cap(Mlp &m, int B) {
+    if (B <= m.cap)
+        return MP_OK;
+    const size_t n = (size_t)B * MLP_H;
+    MP_TRY(m.h1.alloc(n));
+    MP_TRY(m.h2.alloc(n));
+    MP_TRY(m.h3.alloc(n));
+    MP_TRY(m.d3.alloc(n));
+    MP_TRY(m.d2.alloc(n));
+    MP_TRY(m.d1.alloc(n));
+    MP_TRY(m.y.alloc(B));
+    MP_TRY(m.lossbuf.alloc(1));
+    m.cap = B;
+    return MP_OK;
+}
+
+// forward + backward of one batch: grad = dL/dtheta (accumulated from zero), loss to lossbuf
+static int batch_grad(Mlp &m, const uint16_t *X, const float *t, const int *idx, int B,
+                      cudaStream_t s) {
+    MP_TRY(ensure_cap(m, B));
+    MlpFwdArgs a{};
+    a.n = B;
+    a.pack = m.pack.p;
+    a.theta = m.theta.p;
+    a.X = X;
+    a.idx = idx;
+    a.y = m.y.p;
+    a.h1 = m.h1.p;
+    a.h2 = m.h2.p;
+    a.h3 = m.h3.p;
+    a.err = m.err.p;
+    MP_TRY(launch_forward<MLP_MODE_TRAIN>(a, s));
+    MP_CUDA(cudaMemsetAsync(m.grad.p, 0, sizeof(float) * MLP_NPARAM, s));
+    MP_CUDA(cudaMemsetAsync(m.lossbuf.p, 0, sizeof(float), s));
+    k_mlp_out_grad<<<B, MLP_H, 0, s>>>(B, m.y.p, t, idx, m.h3.p, m.theta.p, m.d3.p, m.grad.p,
+                                      m.lossbuf.p);
+    MP_CHECK_LAUNCH();
+    // layer 3: a = h2, d = d3
+    k_mlp_wgrad<<<MLP_H + 1, MLP_H, 0, s>>>(B, MLP_H, m.h2.p, nullptr, m.d3.p,
+                                            m.grad.p + MLP_OFF_W3, m.grad.p + MLP_OFF_B3);
+    MP_CHECK_LAUNCH();
+    k_mlp_dgrad<<<B, MLP_H, 0, s>>>(B, m.theta.p, MLP_OFF_W3, m.d3.p, m.h2.p, m.d2.p);
+    MP_CHECK_LAUNCH();
+    // layer 2: a = h1, d = d2
+    k_mlp_wgrad<<<MLP_H + 1, MLP_H, 0, s>>>(B, MLP_H, m.h1.p, nullptr, m.d2.p,
+                                            m.grad.p + MLP_OFF_W2, m.grad.p + MLP_OFF_B2);
+    MP_CHECK_LAUNCH();
+    k_mlp_dgrad<<<B, MLP_H, 0, s>>>(B, m.theta.p, MLP_OFF_W2, m.d2.p, m.h1.p, m.d1.p);
+    MP_CHECK_LAUNCH();
+    // layer 1: a = features
+    k_mlp_wgrad<<<MLP_IN + 1, MLP_H, 0, s>>>(B, MLP_IN, X, idx, m.d1.p, m.grad.p + MLP_OFF_W1,
+                                             m.grad.p + MLP_OFF_B1);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+int mlp_train(Mlp &m, const uint16_t *X, const float *t, int n, int epochs, int batch, double lr,
+              uint64_t seed, double *loss, cudaStream_t s) {
+    if (n < batch || batch < MLP_TILE || batch % MLP_TILE)
+        return fail(MP_BAD_ARG, "mlp_train: %d samples, batch %d (multiple of %d)", n, batch,
+                    MLP_TILE);
+    MP_TRY(ensure_cap(m, batch));
+    std::vector<int> perm(n);
+    for (int i = 0; i < n; i++)
+        perm[i] = i;
+    std::mt19937_64 g(seed);
+    MP_TRY(m.idx.alloc(n));
+    const int nb = n / batch;
+    double last = 0;
+    for (int e = 0; e < epochs; e++) {
+        std::shuffle(perm.begin(), perm.end(), g);
+        MP_CUDA(cudaMemcpyAsync(m.idx.p, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+        double ep = 0;
+        for (int bi = 0; bi < nb; bi++) {
+            const int *idx = m.idx.p + (size_t)bi * batch;
+            MP_TRY(batch_grad(m, X, t, idx, batch, s));
+            m.adam_t++;
+            const float bc1 = 1.f - std::pow(0.9f, (float)m.adam_t);
+            const float bc2 = 1.f - std::pow(0.999f, (float)m.adam_t);
+            k_mlp_adam<<<(MLP_NPARAM + 255) / 256, 256, 0, s>>>(m.theta.p, m.m1.p, m.m2.p, m.grad.p,
+                                                                MLP_NPARAM, (float)lr, bc1, bc2);
+            MP_CHECK_LAUNCH();
+            MP_TRY(repack(m, s));
+            if (e == epochs - 1) {
+                float l = 0;
+                MP_CUDA(cudaMemcpyAsync(&l, m.lossbuf.p, sizeof(float), cudaMemcpyDeviceToHost, s));
+                MP_CUDA(cudaStreamSynchronize(s));
+                ep += l;
+            }
+        }
+        last = ep / nb;
+    }
+    MP_TRY(mlp_check_err(m, s));
+    if (loss)
+        *loss = last;
+    return MP_OK;
+}
+
+}  // namespace mp
+
+using namespace mp;
+
+struct mp_mlp_s {
+    Mlp *m = nullptr;
+    ~mp_mlp_s() { mlp_destroy(m); }
+};
+
+// row-major FP32 (host or device) -> BF16 device rows
+static int to_bf16_rows(const float *X, size_t count, dbuf<uint16_t> &out, cudaStream_t s) {
+    dbuf<float> tmp;
+    const float *dX;
+    MP_TRY(stage_in(X, count, tmp, &dX, s));
+    MP_TRY(out.alloc(count));
+    k_f32_to_bf16<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(dX, out.p, count);
+    MP_CHECK_LAUNCH();
+    MP_CUDA(cudaStreamSynchronize(s));
+    return MP_OK;
+}
+
+extern "C" int mp_mlp_num_params(void) { return MLP_NPARAM; }
+
+extern "C" int mp_mlp_create(uint64_t seed, mp_mlp *out) {
+    if (!out)
+        return fail(MP_BAD_ARG, "mp_mlp_create: null out");
+    mp_mlp h = new mp_mlp_s;
+    int rc = mlp_create(&h->m, seed);
+    if (rc != MP_OK) {
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return MP_OK;
+}
+
+extern "C" int mp_mlp_get_params(mp_mlp h, float *theta) {
+    if (!h || !theta)
+        return fail(MP_BAD_ARG, "mp_mlp_get_params: null argument");
+    MP_CUDA(cudaMemcpy(theta, h->m->theta.p, sizeof(float) * MLP_NPARAM, cudaMemcpyDefault));
+    return MP_OK;
+}
+
+extern "C" int mp_mlp_set_params(mp_mlp h, const float *theta) {
+    if (!h || !theta)
+        return fail(MP_BAD_ARG, "mp_mlp_set_params: null argument");
+    MP_CUDA(cudaMemcpy(h->m->theta.p, theta, sizeof(float) * MLP_NPARAM, cudaMemcpyDefault));
+    MP_TRY(repack(*h->m, 0));
+    MP_CUDA(cudaDeviceSynchronize());
+    return MP_OK;
+}
+
+extern "C" int mp_mlp_forward(mp_mlp h, const float *X, int n, float *y) {
+    if (!h || !X || !y || n <= 0)
+        return fail(MP_BAD_ARG, "mp_mlp_forward: bad arguments");
+    dbuf<uint16_t> xb;
+    MP_TRY(to_bf16_rows(X, (size_t)n * MLP_IN, xb, 0));
+    dbuf<float> yd;
+    MP_TRY(yd.alloc(n));
+    MlpFwdArgs a{};
+    a.n = n;
+    a.pack = h->m->pack.p;
+    a.theta = h->m->theta.p;
+    a.X = xb.p;
+    a.y = yd.p;
+    a.err = h->m->err.p;
+    MP_TRY(launch_forward<MLP_MODE_ROWS>(a, 0));
+    MP_CUDA(cudaMemcpy(y, yd.p, sizeof(float) * n, cudaMemcpyDefault));
+    return mlp_check_err(*h->m, 0);
+}
+
+extern "C" int mp_mlp_gradient(mp_mlp h, const float *X, const float *t, int n, double *loss,
+                               float *grad) {
+    if (!h || !X || !t || !grad || n <= 0)
+        return fail(MP_BAD_ARG, "mp_mlp_gradient: bad arguments");
+    dbuf<uint16_t> xb;
+    dbuf<float> tt;
+    const float *dt;
+    MP_TRY(to_bf16_rows(X, (size_t)n * MLP_IN, xb, 0));
+    MP_TRY(stage_in(t, (size_t)n, tt, &dt, 0));
+    MP_TRY(batch_grad(*h->m, xb.p, dt, nullptr, n, 0));
+    float l = 0;
+    MP_CUDA(cudaMemcpy(&l, h->m->lossbuf.p, sizeof(float), cudaMemcpyDeviceToHost));
+    MP_CUDA(cudaMemcpy(grad, h->m->grad.p, sizeof(float) * MLP_NPARAM, cudaMemcpyDefault));
+    if (loss)
+        *loss = l;
+    return mlp_check_err(*h->m, 0);
+}
+
+extern "C" int mp_mlp_train(mp_mlp h, const float *X, const float *t, int n, int epochs, int batch,
+                            double lr, uint64_t seed, double *loss) {
+    if (!h || !X || !t)
+        return fail(MP_BAD_ARG, "mp_mlp_train: null argument");
+    dbuf<uint16_t> xb;
+    dbuf<float> tt;
+    const float *dt;
+    MP_TRY(to_bf16_rows(X, (size_t)n * MLP_IN, xb, 0));
+    MP_TRY(stage_in(t, (size_t)n, tt, &dt, 0));
+    return mlp_train(*h->m, xb.p, dt, n, epochs, batch, lr, seed, loss, 0);
+}
+
+extern "C" int mp_mlp_destroy(mp_mlp h) {
+    delete h;
+    return MP_OK;
+}
+
+namespace mp {
+Mlp *mlp_of(::mp_mlp_s *h) { return h ? h->m : nullptr; }
+}  // namespace mp

@@ -13,6 +13,8 @@ struct Cfg {
         smoother_sweeps;
     static Cfg from(const mp_solver_cfg &c);
 };
+// MP_OK, or MP_BAD_ARG with the reason for an inconsistent solver configuration
+int solver_cfg_check(const mp_solver_cfg &c);
 
 struct SolveStats {
     int iters = 0, outer = 0, status = MP_OK;

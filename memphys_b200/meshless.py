@@ -25,6 +25,7 @@ SOLVER_TYPES = {
     "eigen_direct": dict(precond=capi.MP_PRECOND_AMG, precision=capi.MP_FP64),
     "cuda_bicgstab_amg": dict(precond=capi.MP_PRECOND_AMG, precision=capi.MP_FP64),
     "cuda_bicgstab_amg_mixed": dict(precond=capi.MP_PRECOND_AMG, precision=capi.MP_FP32),
+    "cuda_bicgstab_amg_mg32": dict(precond=capi.MP_PRECOND_AMG, precision=capi.MP_MG32),
     "cuda_bicgstab_jacobi": dict(precond=capi.MP_PRECOND_JACOBI, precision=capi.MP_FP64),
     "cuda_bicgstab_jacobi_mixed": dict(precond=capi.MP_PRECOND_JACOBI, precision=capi.MP_FP32),
     "cuda_bicgstab": dict(precond=capi.MP_PRECOND_NONE, precision=capi.MP_FP64),
@@ -349,7 +350,8 @@ class FRACTIONAL_STEP_1:
         return it.value, rr.value, ar.value, al.value
 
     def log(self, first, count):
-        out = np.zeros((count, 4))
+        """Per-step logs: iterations, relres, abs res, alpha, initial relres, refinements."""
+        out = np.zeros((count, 8))
         check(capi.lib().mp_fs1_log(self.handle, first, count, ptr(out)), "mp_fs1_log")
         return out
 
@@ -360,6 +362,87 @@ class FRACTIONAL_STEP_1:
                 self.handle = None
         except Exception:
             pass
+
+
+class MLP:
+    """The learned pressure-increment network (mp_mlp): 64 -> 128 -> 128 -> 128 -> 1."""
+
+    def __init__(self, seed: int = 1):
+        h = C.c_void_p()
+        check(capi.lib().mp_mlp_create(seed, C.byref(h)), "mp_mlp_create")
+        self.handle = h
+        self.n_params = capi.lib().mp_mlp_num_params()
+
+    def params(self) -> np.ndarray:
+        th = np.zeros(self.n_params, np.float32)
+        check(capi.lib().mp_mlp_get_params(self.handle, ptr(th)), "mp_mlp_get_params")
+        return th
+
+    def set_params(self, theta):
+        th = np.ascontiguousarray(theta, np.float32)
+        check(capi.lib().mp_mlp_set_params(self.handle, ptr(th)), "mp_mlp_set_params")
+
+    def forward(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.zeros(X.shape[0], np.float32)
+        check(capi.lib().mp_mlp_forward(self.handle, ptr(X), X.shape[0], ptr(y)), "mp_mlp_forward")
+        return y
+
+    def gradient(self, X, t):
+        X = np.ascontiguousarray(X, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.zeros(self.n_params, np.float32)
+        loss = C.c_double()
+        check(capi.lib().mp_mlp_gradient(self.handle, ptr(X), ptr(t), X.shape[0], C.byref(loss),
+                                         ptr(g)), "mp_mlp_gradient")
+        return loss.value, g
+
+    def train(self, X, t, epochs=5, batch=1024, lr=1e-3, seed=0):
+        X = np.ascontiguousarray(X, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        loss = C.c_double()
+        check(capi.lib().mp_mlp_train(self.handle, ptr(X), ptr(t), X.shape[0], epochs, batch, lr,
+                                      seed, C.byref(loss)), "mp_mlp_train")
+        return loss.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                capi.lib().mp_mlp_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+def attach_mlp(fs: "FRACTIONAL_STEP_1", mlp: MLP, sample_nodes=8192, capacity_steps=500,
+               collect=True):
+    check(capi.lib().mp_fs1_attach_mlp(fs.handle, mlp.handle, sample_nodes, capacity_steps,
+                                       int(collect)), "mp_fs1_attach_mlp")
+    fs.mlp = mlp
+
+
+def train_mlp(fs: "FRACTIONAL_STEP_1", epochs=5, batch=4096, lr=1e-3, seed=0) -> float:
+    loss = C.c_double()
+    check(capi.lib().mp_fs1_train_mlp(fs.handle, epochs, batch, lr, seed, C.byref(loss)),
+          "mp_fs1_train_mlp")
+    return loss.value
+
+
+def samples(fs: "FRACTIONAL_STEP_1"):
+    """The recorded training samples (features X, targets t, node of each row)."""
+    n = C.c_int()
+    L = capi.lib()
+    check(L.mp_fs1_samples(fs.handle, None, None, None, 0, C.byref(n)), "mp_fs1_samples")
+    X = np.zeros((n.value, 64), np.float32)
+    t = np.zeros(n.value, np.float32)
+    nodes = np.zeros(n.value, np.int32)
+    check(L.mp_fs1_samples(fs.handle, capi.ptr(X), capi.ptr(t), capi.ptr(nodes), n.value,
+                           C.byref(n)), "mp_fs1_samples")
+    return X, t, nodes
+
+
+def set_guess(fs: "FRACTIONAL_STEP_1", guess: int):
+    check(capi.lib().mp_fs1_set_guess(fs.handle, guess), "mp_fs1_set_guess")
 
 
 def cavity_setup(nx: int, solver_type="cuda_bicgstab_amg", dt=None, rho=1.0, mu=0.01,
@@ -412,6 +495,9 @@ def calc_dt(cloud: CLOUD, u0: float, v0: float, w0: float, alpha: float, courant
 
 
 def stable_dt(h: float, nu: float, lid: float = 1.0, safety: float = 0.5) -> float:
-    """Explicit-step limit of the AB2 projection step used by the benchmark cavities:
-    min(0.5 h / u, 0.1 h^2 / nu) times `safety`; 1e-3 at the 100 x 100 cavity."""
-    return min(1e-3, safety * min(0.5 * h / lid, 0.1 * h * h / nu) * 2.0)
+    """A step inside the explicit limits of the AB2 projection step on these clouds:
+    safety * min(0.5 h / u, 0.02 h^2 / nu).  The diffusion bound is the AB2 limit
+    1 / (nu |lambda_L|) with |lambda_L| ~ 46 / h^2, the spectral radius of the
+    PHS-RBF-FD Laplacian on the jittered cavity (power iteration at h = 1e-3);
+    calc_dt computes the same bound from the actual eigenvalues."""
+    return safety * min(0.5 * h / lid, 0.02 * h * h / nu)

@@ -1,0 +1,105 @@
+"""GPU: the tensor-core network (tcgen05) against the numpy oracle, training,
+and what the learned initial guess gains in the pressure solve."""
+import numpy as np
+import pytest
+
+from oracle import mlp as omlp
+from memphys_b200 import capi, clouds, meshless
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def net(mp_lib):
+    return meshless.MLP(seed=3)
+
+
+def test_forward_matches_oracle(net):
+    rng = np.random.default_rng(1)
+    X = rng.normal(size=(300, 64)).astype(np.float32)  # not a multiple of the 128-row tile
+    y = net.forward(X)
+    yo, _ = omlp.forward(net.params(), X)
+    assert np.abs(y - yo).max() <= 1e-3 * max(1.0, np.abs(yo).max())
+
+
+def test_gradient_matches_oracle(net):
+    rng = np.random.default_rng(2)
+    X = rng.normal(size=(256, 64)).astype(np.float32)
+    t = rng.normal(size=256).astype(np.float32)
+    loss, g = net.gradient(X, t)
+    lo, go = omlp.loss_grad(net.params(), X, t)
+    assert loss == pytest.approx(lo, rel=1e-4)
+    o = 0
+    for name, shape in omlp.SIZES:
+        n = int(np.prod(shape))
+        a, b = g[o:o + n], go[o:o + n]
+        assert np.linalg.norm(a - b) <= 1e-3 * np.linalg.norm(b) + 1e-7, name
+        o += n
+
+
+def test_training_reduces_loss(mp_lib):
+    rng = np.random.default_rng(4)
+    X = rng.normal(size=(8192, 64)).astype(np.float32)
+    t = (np.tanh(X[:, :8].sum(1) / 3) + 0.1 * X[:, 9]).astype(np.float32)
+    m = meshless.MLP(seed=5)
+    l0, _ = m.gradient(X[:1024], t[:1024])
+    loss = m.train(X, t, epochs=20, batch=1024, lr=2e-3)
+    assert loss < 0.2 * l0
+    y = m.forward(X[:512])
+    assert np.mean((y - t[:512]) ** 2) < 0.25 * l0
+
+
+def test_collected_samples_match_fields(mp_lib):
+    """Each step records, for fixed nodes, the pressure-increment features of its
+    first 20 stencil members and the solved increment, scaled by 1/RMS(p^n - p^{n-1});
+    recompute them from the states before and after each step."""
+    cl, prm, pts, cld, fs = meshless.cavity_setup(48, solver_type="cuda_bicgstab_amg", tol=1e-10)
+    meshless.attach_mlp(fs, meshless.MLP(seed=1), sample_nodes=300, capacity_steps=8)
+    nv = fs.nv
+    P = [fs.get_state()[1][:nv].copy()]
+    for _ in range(6):
+        fs.step(1)
+        P.append(fs.get_state()[1][:nv].copy())
+    X, t, nodes = meshless.samples(fs)
+    assert X.shape == (4 * 300, 64) and np.isfinite(X).all() and np.isfinite(t).all()
+    nb = cld.fetch().nb_points_col
+    bfl = np.asarray(pts.boundary_flag, bool)
+    for q in range(4):                      # ring slot q holds step s = q + 2
+        s = q + 2
+        sp = 1.0 / np.sqrt(np.mean((P[s] - P[s - 1]) ** 2))
+        rows = slice(q * 300, (q + 1) * 300)
+        Xi, ti, ni = X[rows], t[rows], nodes[rows]
+        j = nb[ni, :20]
+        exp1 = (P[s] - P[s - 1])[j] * sp
+        exp2 = (P[s - 1] - P[s - 2])[j] * sp
+        # features are BF16 (8 significant bits), targets FP32
+        for got, exp, rel in ((Xi[:, 1:60:3], exp1, 2.0 ** -8), (Xi[:, 2:60:3], exp2, 2.0 ** -8),
+                              (ti, (P[s + 1] - P[s])[ni] * sp, 1e-5)):
+            tol = rel * np.abs(exp) + 1e-6 * np.abs(exp).max()
+            assert np.all(np.abs(got - exp) <= tol)
+        assert np.array_equal(Xi[:, 61], bfl[ni].astype(np.float32))
+        assert np.all(Xi[:, 62] == 1.0) and np.all(Xi[:, 63] == 0.0)
+        assert np.all(Xi[:, 60] > 0) and np.all(np.isfinite(Xi[:, 60]))
+
+
+def test_learned_guess_saves_iterations(mp_lib):
+    """Plain solves generate the training data; the trained network's guess must
+    need fewer BiCGSTAB iterations than the zero guess, at the same tolerance."""
+    cl, prm, pts, cld, fs = meshless.cavity_setup(96, solver_type="cuda_bicgstab_amg", tol=1e-8)
+    net = meshless.MLP(seed=7)
+    meshless.attach_mlp(fs, net, sample_nodes=4096, capacity_steps=64)
+    fs.step(40)
+    loss = meshless.train_mlp(fs, epochs=30, batch=1024, lr=1e-3)
+    assert np.isfinite(loss)
+    vel, p = fs.get_state()
+    res = {}
+    for guess in (capi.MP_GUESS_ZERO, capi.MP_GUESS_PREVIOUS, capi.MP_GUESS_LEARNED):
+        meshless.set_guess(fs, guess)
+        fs.set_state(vel, p, 40)
+        fs.step(6)
+        log = fs.log(40, 6)
+        assert np.all(log[:, 1] <= 1e-8)
+        res[guess] = (log[2:, 0].mean(), log[2:, 4].mean())
+    # iterations and initial residuals: learned < zero guess
+    assert res[capi.MP_GUESS_LEARNED][0] < res[capi.MP_GUESS_ZERO][0]
+    assert res[capi.MP_GUESS_LEARNED][1] < res[capi.MP_GUESS_ZERO][1]

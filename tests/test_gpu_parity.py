@@ -237,7 +237,7 @@ def ppe_direct(cl, cld):
 
 
 @pytest.mark.parametrize("solver_type", ["cuda_bicgstab_amg", "cuda_bicgstab_jacobi",
-                                         "cuda_bicgstab_amg_mixed"])
+                                         "cuda_bicgstab_amg_mixed", "cuda_bicgstab_amg_mg32"])
 def test_pressure_solve(cav, solver_type):
     cl, prm, pts, cld = cav
     A = ppe_direct(cl, cld)
@@ -297,6 +297,19 @@ def test_fs1_mixed_precision_matches_fp64(mp_lib):
     for d in range(2):
         assert np.abs(gv[d] - rv[d]).max() <= 1e-7 * np.abs(rv[d]).max()
     assert np.all(log[:, 1] <= 1e-10)
+
+
+def test_fs1_mg32_matches_fp64(mp_lib):
+    """FP32 multigrid storage (difference form) under an FP64 Krylov solve: same
+    residual, fields within the FP64 solve's own error, iterations within one."""
+    cl = clouds.cavity_2d(32, seed=3)
+    gv, gp, rv, rp_, log = run_fs1_pair(cl, 2e-4, 6, solver_type="cuda_bicgstab_amg_mg32",
+                                        tol=1e-10)
+    for d in range(2):
+        assert np.abs(gv[d] - rv[d]).max() <= 1e-7 * np.abs(rv[d]).max()
+    assert np.all(log[:, 1] <= 1e-10)
+    *_, log64 = run_fs1_pair(cl, 2e-4, 6, solver_type="cuda_bicgstab_amg", tol=1e-10)
+    assert np.all(log[:, 0] <= log64[:, 0] + 1)
 
 
 def test_fs1_channel_with_outlet_and_neumann_velocity(mp_lib):
