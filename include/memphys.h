@@ -83,6 +83,21 @@ int mp_poly_exponents(int dim, int poly_deg, int *exps);
  */
 int mp_knn_stencils(const double *xyz, const uint8_t *boundary, int nv, int dim, int n,
                     int *nb_col, mp_stream s);
+/*
+ * The same stencils without allocating device memory (no counterpart in the
+ * reference, whose kNN runs on the host).  For callers that cannot allocate
+ * mid-run: cudaMalloc/cudaFree synchronise the whole device (stalling solves
+ * running on other streams) and fail once a run has sized its buffers to fill
+ * the GPU.  Device pointers only.  Work arrays live in a fixed 4 MiB scratch
+ * array per device, enough for about 140,000 nodes in 2D; larger clouds
+ * return MP_BAD_ARG.  The first call on a device looks the scratch up
+ * (cudaGetSymbolAddress), so make it before any stream capture.  Calls share
+ * the scratch: calls that overlap in time on one device race, so order them
+ * on one stream (or with events).  The scratch needs no initial contents;
+ * every call clears what it counts in.
+ */
+int mp_knn_stencils_noalloc(const double *xyz, const uint8_t *boundary, int nv, int dim, int n,
+                            int *nb_col, mp_stream s);
 
 /*
  * PHS-RBF-FD weights of every stencil of a cloud, replacing the loop of

@@ -33,7 +33,8 @@ EXPORTS = [
     "mp_last_error", "mp_version", "mp_device_info", "mp_set_device", "mp_malloc", "mp_free", "mp_malloc_host",
     "mp_free_host", "mp_memcpy", "mp_memset", "mp_stream_create", "mp_stream_destroy",
     "mp_stream_sync", "mp_timer_start", "mp_timer_stop", "mp_profiler", "mp_launch_count", "mp_num_poly_terms",
-    "mp_cloud_size", "mp_poly_exponents", "mp_knn_stencils", "mp_stencil_weights",
+    "mp_cloud_size", "mp_poly_exponents", "mp_knn_stencils", "mp_knn_stencils_noalloc",
+    "mp_stencil_weights",
     "mp_stencil_weights_batched", "mp_cloud_create", "mp_cloud_create_stencils", "mp_cloud_info",
     "mp_cloud_get", "mp_cloud_destroy", "mp_op_create_ell", "mp_op_from_cloud", "mp_op_apply",
     "mp_op_apply_multi", "mp_op_info", "mp_op_destroy", "mp_solver_cfg_default", "mp_ppe_create",
@@ -87,6 +88,7 @@ def lib() -> C.CDLL:
             "mp_profiler": [i], "mp_launch_count": [C.POINTER(C.c_int64), i],
             "mp_num_poly_terms": [i, i], "mp_cloud_size": [i, i, d], "mp_poly_exponents": [i, i, vp],
             "mp_knn_stencils": [vp, vp, i, i, i, vp, vp],
+            "mp_knn_stencils_noalloc": [vp, vp, i, i, i, vp, vp],
             "mp_stencil_weights": [vp, i, i, vp, i, i, i, vp, vp, vp, vp, vp, vp],
             "mp_stencil_weights_batched": [i, vp, vp, vp, i, i, i, vp, vp, vp],
             "mp_cloud_create": [vp, vp, i, i, i, i, d, i, vp, C.POINTER(vp)],

@@ -13,7 +13,9 @@
 // once the k-th distance is within the radius already covered.  This is an
 // exact search, so it selects the same stencils as the KD-tree.
 #include <cub/cub.cuh>
+#include <climits>
 #include <cmath>
+#include <mutex>
 #include "mp_common.cuh"
 
 namespace mp {
@@ -231,5 +233,179 @@ extern "C" int mp_knn_stencils(const double *xyz, const uint8_t *boundary, int n
         MP_CUDA(cudaMemcpyAsync(nb_col, dn, sizeof(int) * nv * n, cudaMemcpyDeviceToHost, st));
         MP_CUDA(cudaStreamSynchronize(st));
     }
+    return MP_OK;
+}
+
+// ------------------------------------------------ no-allocation variant
+// mp_knn_stencils_noalloc runs the same grid + radix sort + query kernels with
+// every work array carved from one fixed scratch array per device, so a call
+// allocates and frees no device memory.
+namespace mp {
+
+constexpr size_t KNN_SCRATCH_BYTES = (size_t)4 << 20;  // 4 MiB: ~140,000 nodes in 2D
+static __device__ __align__(256) unsigned char g_knn_scratch[KNN_SCRATCH_BYTES];
+
+constexpr int KNN_SCRATCH_DEVICES = 64;
+static std::mutex g_knn_scratch_mu;
+static unsigned char *g_knn_scratch_ptr[KNN_SCRATCH_DEVICES];
+
+// device address of the current device's scratch, looked up once per device
+static int knn_scratch(unsigned char **out) {
+    int dev = 0;
+    MP_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= KNN_SCRATCH_DEVICES)
+        return fail(MP_BAD_ARG, "device %d beyond the %d supported", dev, KNN_SCRATCH_DEVICES);
+    std::lock_guard<std::mutex> lock(g_knn_scratch_mu);
+    if (!g_knn_scratch_ptr[dev]) {
+        unsigned char *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void **)&p, g_knn_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(MP_CUDA_ERROR, "cudaGetSymbolAddress(kNN scratch): %s",
+                        cudaGetErrorString(e));
+        g_knn_scratch_ptr[dev] = p;
+    }
+    *out = g_knn_scratch_ptr[dev];
+    return MP_OK;
+}
+
+// bounding box lo[0..2], hi[0..2]; flags[0] = 0 (the query's failure count),
+// flags[1] = lowest index of a node with a non-finite coordinate or INT_MAX; one block
+__global__ void __launch_bounds__(256)
+    knn_bbox(const double *xyz, int nv, int dim, double *box, int *flags) {
+    __shared__ double slo[3][256], shi[3][256];
+    __shared__ int sbad[256];
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    int first_bad = INT_MAX;
+    for (int i = threadIdx.x; i < nv; i += blockDim.x)
+        for (int d = 0; d < dim; d++) {
+            const double v = xyz[(size_t)i * dim + d];
+            if (!isfinite(v)) {
+                first_bad = min(first_bad, i);
+                continue;
+            }
+            lo[d] = fmin(lo[d], v);
+            hi[d] = fmax(hi[d], v);
+        }
+    for (int d = 0; d < 3; d++) {
+        slo[d][threadIdx.x] = lo[d];
+        shi[d][threadIdx.x] = hi[d];
+    }
+    sbad[threadIdx.x] = first_bad;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            for (int d = 0; d < 3; d++) {
+                slo[d][threadIdx.x] = fmin(slo[d][threadIdx.x], slo[d][threadIdx.x + w]);
+                shi[d][threadIdx.x] = fmax(shi[d][threadIdx.x], shi[d][threadIdx.x + w]);
+            }
+            sbad[threadIdx.x] = min(sbad[threadIdx.x], sbad[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int d = 0; d < 3; d++) {
+            box[d] = slo[d][0];
+            box[3 + d] = shi[d][0];
+        }
+        flags[0] = 0;
+        flags[1] = sbad[0];
+    }
+}
+
+// offsets of the work arrays inside the scratch (each 256-byte aligned)
+struct KnnCarve {
+    size_t off = 0;
+    size_t take(size_t bytes) {
+        const size_t o = off;
+        off = (off + bytes + 255) / 256 * 256;
+        return o;
+    }
+};
+
+}  // namespace mp
+
+extern "C" int mp_knn_stencils_noalloc(const double *xyz, const uint8_t *boundary, int nv, int dim,
+                                       int n, int *nb_col, mp_stream s) {
+    if (!xyz || !boundary || !nb_col)
+        return fail(MP_BAD_ARG, "mp_knn_stencils_noalloc: null argument");
+    if (nv <= 0 || (dim != 2 && dim != 3) || n < 2 || n > KNN_MAX)
+        return fail(MP_BAD_ARG, "mp_knn_stencils_noalloc: nv=%d dim=%d n=%d (n must be 2..%d)", nv,
+                    dim, n, KNN_MAX);
+    if (!is_device_ptr(xyz) || !is_device_ptr(boundary) || !is_device_ptr(nb_col))
+        return fail(MP_BAD_ARG, "mp_knn_stencils_noalloc takes device pointers only (staging host "
+                                "arrays would allocate); use mp_knn_stencils for host arrays");
+    // the four per-node arrays alone must fit before anything runs
+    if ((size_t)nv * 16 + 4096 > KNN_SCRATCH_BYTES)
+        return fail(MP_BAD_ARG, "mp_knn_stencils_noalloc: %d nodes exceed its %zu-byte scratch "
+                                "(at most about 140000 nodes in 2D); use mp_knn_stencils", nv,
+                    KNN_SCRATCH_BYTES);
+    unsigned char *base = nullptr;
+    MP_TRY(knn_scratch(&base));
+    cudaStream_t st = S(s);
+    KnnCarve cv;
+    double *box = (double *)(base + cv.take(6 * sizeof(double)));
+    int *flags = (int *)(base + cv.take(2 * sizeof(int)));  // [0] failed queries, [1] first non-finite
+    // bounding box on the device (it also clears the flags); six numbers come back to the host
+    knn_bbox<<<1, 256, 0, st>>>(xyz, nv, dim, box, flags);
+    MP_CHECK_LAUNCH();
+    double hb[6];
+    int hf[2];
+    MP_CUDA(cudaMemcpyAsync(hb, box, sizeof(hb), cudaMemcpyDeviceToHost, st));
+    MP_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
+    MP_CUDA(cudaStreamSynchronize(st));
+    if (hf[1] != INT_MAX)
+        return fail(MP_BAD_ARG, "node %d has a non-finite coordinate", hf[1]);
+    Grid G;
+    double hi[3] = {0, 0, 0};
+    for (int d = 0; d < 3; d++)
+        G.lo[d] = 0.0, G.g[d] = 1;
+    for (int d = 0; d < dim; d++) {
+        G.lo[d] = hb[d];
+        hi[d] = hb[3 + d];
+    }
+    double vol = 1.0;
+    for (int d = 0; d < dim; d++)
+        vol *= (hi[d] - G.lo[d]) > 0 ? (hi[d] - G.lo[d]) : 1.0;
+    G.cell = std::pow(vol * 2.0 / nv, 1.0 / dim);
+    long long ncell = 1;
+    for (int d = 0; d < dim; d++) {
+        G.g[d] = (int)((hi[d] - G.lo[d]) / G.cell) + 1;
+        ncell *= G.g[d];
+    }
+    if (ncell > (1ll << 31))
+        return fail(MP_BAD_ARG, "kNN grid too large (%lld cells)", ncell);
+    int bits = 1;
+    while ((1ll << bits) < ncell)
+        bits++;
+    const size_t o_cid = cv.take(sizeof(unsigned) * nv), o_cid2 = cv.take(sizeof(unsigned) * nv);
+    const size_t o_idx = cv.take(sizeof(int) * nv), o_idx2 = cv.take(sizeof(int) * nv);
+    const size_t o_st = cv.take(sizeof(int) * ncell), o_en = cv.take(sizeof(int) * ncell);
+    unsigned *cid = (unsigned *)(base + o_cid), *cid2 = (unsigned *)(base + o_cid2);
+    int *idx = (int *)(base + o_idx), *idx2 = (int *)(base + o_idx2);
+    int *cst = (int *)(base + o_st), *cen = (int *)(base + o_en);
+    size_t tmp_bytes = 0;  // a size query: no temporary storage is allocated
+    MP_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, cid, cid2, idx, idx2, nv, 0, bits,
+                                            st));
+    const size_t o_tmp = cv.take(tmp_bytes);
+    if (cv.off > KNN_SCRATCH_BYTES)
+        return fail(MP_BAD_ARG, "mp_knn_stencils_noalloc: %d nodes need %zu bytes of scratch, it "
+                                "holds %zu; use mp_knn_stencils", nv, cv.off, KNN_SCRATCH_BYTES);
+    MP_CUDA(cudaMemsetAsync(cst, 0, sizeof(int) * ncell, st));
+    MP_CUDA(cudaMemsetAsync(cen, 0, sizeof(int) * ncell, st));
+    const int tb = 256, nb = (nv + tb - 1) / tb;
+    knn_cell_ids<<<nb, tb, 0, st>>>(xyz, nv, dim, G, cid, idx);
+    MP_CHECK_LAUNCH();
+    MP_CUDA(cub::DeviceRadixSort::SortPairs(base + o_tmp, tmp_bytes, cid, cid2, idx, idx2, nv, 0,
+                                            bits, st));
+    count_launch();
+    knn_cell_ranges<<<nb, tb, 0, st>>>(cid2, nv, cst, cen);
+    MP_CHECK_LAUNCH();
+    knn_query<<<(nv + 127) / 128, 128, 0, st>>>(xyz, boundary, nv, dim, n, G, idx2, cst, cen,
+                                                 nb_col, flags);
+    MP_CHECK_LAUNCH();
+    MP_CUDA(cudaMemcpyAsync(hf, flags, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MP_CUDA(cudaStreamSynchronize(st));
+    if (hf[0])
+        return fail(MP_KNN_FAILED, "%d nodes found fewer than %d stencil candidates", hf[0], n);
     return MP_OK;
 }
