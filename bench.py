@@ -8,11 +8,17 @@ with the smoothed-aggregation multigrid preconditioner to ||r||/||b|| <= 1e-8;
 Re = 100 (rho 1, mu 0.01), Adams-Bashforth 2; dt from the reference's calc_dt
 rule with Courant 0.25 (the configured dt = 1e-3 is explicitly unstable on
 this cloud).  A "step" is one FRACTIONAL_STEP_1 timestep, graph-launched.
+The flow first spins up from rest for `--spinup` untimed steps (100, the
+configuration's run length), recording the learned guess's training samples,
+and the network is trained on them; every variant then starts from that state,
+runs `--warmup` untimed steps and `--steps` timed ones.
 
 Printed (rank 0, one JSON line): the plain FP64 ms/step as `value`
-(lower is better), the mixed-precision ms/step beside it, the end-to-end
-ms/step through mp_fs1_single_timestep with pinned host buffers, the SpMV
-roofline, and the CPU oracle baseline.
+(lower is better); the variants beside it (FP32 multigrid storage, FP32
+Krylov with FP64 refinement, extrapolated and learned initial guesses, and
+learned + FP32 multigrid as `learned_mixed`); the end-to-end ms/step through
+mp_fs1_single_timestep with pinned host buffers; the SpMV roofline; and the
+CPU oracle baseline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--nx NX]
 """
@@ -47,6 +53,12 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch the step's kernels one by one instead of as a CUDA graph")
+    ap.add_argument("--spinup", type=int, default=100,
+                    help="untimed timesteps from rest before the timed ones (the 100 steps of "
+                         "the 1M-node configuration); the learned guess trains on their solves")
+    ap.add_argument("--samples", type=int, default=16384,
+                    help="nodes whose features and solved increments are recorded per step")
+    ap.add_argument("--epochs", type=int, default=10)
     ap.add_argument("--inner-tol", type=float, default=1e-5,
                     help="mixed precision: relative reduction of each FP32 refinement solve")
     ap.add_argument("--profile", default=None, choices=["steps", "spmv"],
@@ -55,7 +67,10 @@ def parse():
     return ap.parse_args()
 
 
-def dist_setup(args):
+def dist_setup(args=None, timeout_s: int = 120):
+    """One process per GPU (torchrun env).  The replicas share no data: the process
+    group carries only the start barrier and the max-over-ranks of the timings
+    (NCCL on GPUs, gloo where there is no GPU)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -65,8 +80,10 @@ def dist_setup(args):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
         pg = dist
     return ws, rank, local, pg
 
@@ -172,19 +189,43 @@ def run_ours(args, ws, rank, local, pg):
     cld = meshless.CLOUD(pts, prm, compute_cond=False)
     t_cloud = time.time() - t0
     prm.dt = meshless.calc_dt(cld, 1.0, 1.0, 0.0, prm.mu / prm.rho, args.courant)
+
+    def make(**cfg):
+        return meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                          cl.p_dirichlet, 2, use_graph=not args.no_graph, **cfg)
+
+    stream = capi.Stream()
+    vel0 = [cl.vel_bc[0].copy(), cl.vel_bc[1].copy()]
     t0 = time.time()
-    fs = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
-                                    cl.p_dirichlet, 2, use_graph=not args.no_graph)
+    fs = make()
     t_setup = time.time() - t0
     ns = fs.system_size
-    vel0 = [cl.vel_bc[0].copy(), cl.vel_bc[1].copy()]
     p0 = np.zeros(ns)
-    stream = capi.Stream()
     if args.profile:
         return profile_range(args, cld, fs, vel0, p0, stream)
 
+    # spin-up from rest, untimed, recording the learned guess's training samples
+    # (features and solved increments of `--samples` fixed nodes at every step);
+    # the network is trained on them before any variant is timed
+    spin = make()
+    net = meshless.MLP(seed=7)
+    meshless.attach_mlp(spin, net, sample_nodes=min(args.samples, nv),
+                        capacity_steps=max(args.spinup, 1))
+    spin.set_state(vel0, p0, 0)
+    spin.step(args.spinup, stream.handle)
+    stream.sync()
+    t0 = time.time()
+    train_loss = None
+    if args.spinup >= 3:
+        train_loss = meshless.train_mlp(spin, epochs=args.epochs, batch=1024, lr=1e-3)
+    t_train = time.time() - t0
+    del spin
+
     def timed_steps(f, K, W):
+        # every variant repeats the spin-up from rest (untimed), so its Adams-Bashforth
+        # and pressure histories are its own, then warms up and times K steps
         f.set_state(vel0, p0, 0)
+        f.step(args.spinup, stream.handle)
         for _ in range(W):
             f.step(1, stream.handle)
         stream.sync()
@@ -199,7 +240,7 @@ def run_ours(args, ws, rank, local, pg):
     with Clocks(local) as clk:
         ms64 = timed_steps(fs, args.steps, args.warmup)
     clocks = clk.summary()
-    log64 = fs.log(args.warmup, args.steps)
+    log64 = fs.log(args.spinup + args.warmup, args.steps)
     import ctypes as C
     fixed, per_sweep, per_ref = C.c_int(), C.c_int(), C.c_int()
     capi.check(L.mp_fs1_kernel_counts(fs.handle, C.byref(fixed), C.byref(per_sweep),
@@ -209,39 +250,36 @@ def run_ours(args, ws, rank, local, pg):
     vel64, p64 = fs.get_state()
     ms64_max = max_over_ranks(pg, ms64)
 
-    # mixed precision: FP32 BiCGSTAB + multigrid under FP64 iterative refinement
-    mixed = None
-    if not args.no_mixed:
-        fsm = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
-                                         cl.p_dirichlet, 2, use_graph=not args.no_graph,
-                                         precision=capi.MP_FP32, inner_tol=args.inner_tol)
-        msm = timed_steps(fsm, args.steps, args.warmup)
-        logm = fsm.log(args.warmup, args.steps)
-        velm, pm = fsm.get_state()
-        err = [float(np.abs(velm[d] - vel64[d]).max() / np.abs(vel64[d]).max()) for d in range(2)]
-        perr = float(np.abs((pm - p64)[:nv]).max() / np.abs(p64[:nv]).max())
-        mixed = {"ms_per_step": max_over_ranks(pg, msm),
-                 "inner_iters_per_step": float(np.mean(logm[:, 0])),
-                 "refinements_per_step": float(np.mean(logm[:, 5])),
-                 "max_relres": float(logm[:, 1].max()),
-                 "rel_err_vs_fp64": {"u": err[0], "v": err[1], "p": perr}}
-        del fsm
-
-    def variant(**cfg):
+    def variant(guess=capi.MP_GUESS_PREVIOUS, **cfg):
         """Time the same steps with another solver configuration; errors against FP64."""
-        f = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
-                                       cl.p_dirichlet, 2, use_graph=not args.no_graph, **cfg)
+        f = make(**cfg)
+        if guess == capi.MP_GUESS_LEARNED:
+            meshless.attach_mlp(f, net, sample_nodes=1, capacity_steps=1, collect=False)
+        if guess != capi.MP_GUESS_PREVIOUS:
+            meshless.set_guess(f, guess)
         ms = timed_steps(f, args.steps, args.warmup)
-        lg = f.log(args.warmup, args.steps)
+        lg = f.log(args.spinup + args.warmup, args.steps)
         vv, pp = f.get_state()
         err = [float(np.abs(vv[d] - vel64[d]).max() / np.abs(vel64[d]).max()) for d in range(2)]
         perr = float(np.abs((pp - p64)[:nv]).max() / np.abs(p64[:nv]).max())
-        return {"ms_per_step": max_over_ranks(pg, ms), "iters_per_step": float(np.mean(lg[:, 0])),
+        ms = max_over_ranks(pg, ms)
+        return {"ms_per_step": round(ms, 4), "speedup_vs_plain_fp64": round(ms64_max / ms, 3),
+                "iters_per_step": float(np.mean(lg[:, 0])),
                 "relres0_mean": float(np.mean(lg[:, 4])), "max_relres": float(lg[:, 1].max()),
+                "refinements_per_step": float(np.mean(lg[:, 5])),
                 "rel_err_vs_fp64": {"u": err[0], "v": err[1], "p": perr}}
 
-    # FP64 BiCGSTAB, multigrid operators stored in FP32 (difference form)
-    mg32 = None if args.no_mixed else variant(precision=capi.MP_MG32)
+    variants = {}
+    if not args.no_mixed:
+        # FP64 BiCGSTAB, multigrid operators stored in FP32 (difference form)
+        variants["mg32"] = variant(precision=capi.MP_MG32)
+        # FP32 BiCGSTAB + multigrid under FP64 iterative refinement
+        variants["fp32_refined"] = variant(precision=capi.MP_FP32, inner_tol=args.inner_tol)
+        variants["extrapolated_guess"] = variant(guess=capi.MP_GUESS_EXTRAPOLATE)
+        variants["learned_guess"] = variant(guess=capi.MP_GUESS_LEARNED)
+        variants["learned_mg32"] = variant(guess=capi.MP_GUESS_LEARNED, precision=capi.MP_MG32)
+        variants["extrapolated_mg32"] = variant(guess=capi.MP_GUESS_EXTRAPOLATE,
+                                                precision=capi.MP_MG32)
 
     # end to end through the C ABI drop-in with pinned host buffers
     u_h = capi.PinnedArray((nv,))
@@ -255,7 +293,7 @@ def run_ours(args, ws, rank, local, pg):
     p_h.array[:] = p64
     vo = (C.c_void_p * 2)(u_h.ptr, v_h.ptr)
     vn = (C.c_void_p * 2)(un_h.ptr, vn_h.ptr)
-    step0 = args.warmup + args.steps
+    step0 = args.spinup + args.warmup + args.steps
     barrier(pg)
     with capi.Timer(stream.handle) as tm:
         for k in range(args.steps):
@@ -295,9 +333,13 @@ def run_ours(args, ws, rank, local, pg):
                    "l2": "inputs larger than L2 (ELL operators 257 MB, step working set > 1 GB)"},
         "pressure_iters_per_step": float(iters64.mean()),
         "max_relres": float(log64[:, 1].max()),
-        "mixed": mixed,
-        "mg32": mg32,
         "relres0_mean": float(np.mean(log64[:, 4])),
+        "learned_mixed": variants.get("learned_mg32"),
+        "variants": variants,
+        "learned_training": {"spinup_steps": args.spinup, "sample_nodes": min(args.samples, nv),
+                             "samples": min(args.samples, nv) * max(args.spinup - 2, 0),
+                             "epochs": args.epochs, "final_loss": train_loss,
+                             "train_s": round(t_train, 2)},
         "spmv_gbs": round(achieved, 1),
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms/step", "h2d_bytes_per_step": e2e_bytes,
                 "d2h_bytes_per_step": e2e_bytes},

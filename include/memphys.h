@@ -184,7 +184,8 @@ typedef struct mp_ppe_s *mp_ppe;
 enum { MP_PRECOND_NONE = 0, MP_PRECOND_JACOBI = 1, MP_PRECOND_AMG = 2 };
 /* initial guess of each fractional-step pressure solve: the previous pressure
  * (the reference's solveWithGuess(rhs, p_old)), zero, the linear extrapolation
- * 2 p^n - p^(n-1), or p^n plus the learned network's predicted increment */
+ * 2 p^n - p^(n-1), or that extrapolation plus the learned network's predicted
+ * correction */
 enum { MP_GUESS_PREVIOUS = 0, MP_GUESS_ZERO = 1, MP_GUESS_LEARNED = 2, MP_GUESS_EXTRAPOLATE = 3 };
 
 typedef struct {
@@ -241,7 +242,9 @@ int mp_fs1_create(mp_cloud c, const uint8_t *boundary, const double *normal,
                   const uint8_t *w_dirichlet, const uint8_t *p_dirichlet,
                   const mp_fs1_cfg *cfg, const mp_solver_cfg *solver, mp_fs1 *out);
 int mp_fs1_system_size(mp_fs1 f);
-/* resident state: vel = dim arrays of nv; p = system_size entries */
+/* resident state: vel = dim arrays of nv; p = system_size entries.  The pressure
+ * history behind the extrapolated and learned guesses continues when `it` equals
+ * the current step index and restarts from p otherwise. */
 int mp_fs1_set_state(mp_fs1 f, const double *const *vel, const double *p, int it, mp_stream s);
 int mp_fs1_get_state(mp_fs1 f, double *const *vel, double *p, mp_stream s);
 /* advance the resident state nsteps timesteps (one CUDA graph launch per step

@@ -11,7 +11,7 @@
 //     the coarse size is small; the coarsest operator (singular for pure
 //     Neumann problems) is bordered like solver.cpp:205-213 and inverted.
 //   apply (GPU, every preconditioner call): V(1,1) cycle with degree-2
-//     Chebyshev smoothing on [lambda_max / 6, lambda_max] of D^-1 A; the
+//     Chebyshev smoothing on [lambda_max / 12, lambda_max] of D^-1 A; the
 //     RBF-FD Laplacian's Jacobi-scaled spectrum reaches ~2.85, where damped
 //     Jacobi is unstable or weak.
 // All level operators are ELL (64-row slices) padded to the level's widest row.
@@ -70,12 +70,14 @@ struct Amg {
     dbuf<float> cinv32;
     double setup_seconds = 0;
     int store = AMG_F64;
+    double cheb_ratio = 12.0;         // Chebyshev smoothing on [lmax / ratio, lmax]
     dbuf<int> zero_flag;              // a device 0 used as `done` while autotuning
     ~Amg();
 };
 
 int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t s);
 void amg_destroy(Amg *a);
+
 // out = V-cycle(in) on the first n0 entries (the border entry is handled by
 // the caller); kernels return immediately while *done is set.  FP64 vectors use
 // the FP32 difference-form operators when the hierarchy was built with AMG_MG32.

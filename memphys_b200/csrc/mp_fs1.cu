@@ -568,7 +568,7 @@ extern "C" int mp_fs1_create(mp_cloud c, const uint8_t *boundary, const double *
     const int ns = f->P.sys.nsys;
     if ((rc = f->step.alloc(1)) || (rc = f->log.alloc(MP_LOG_FIELDS * (size_t)f->log_cap)) ||
         (rc = f->pcur.alloc(ns)) || (rc = f->ph1.alloc(ns)) || (rc = f->ph2.alloc(ns)) ||
-        (rc = f->norms.alloc(2)))
+        (rc = f->norms.alloc(3)))
         return bail(rc);
     for (dbuf<double> *b : {&f->pcur, &f->ph1, &f->ph2})
         cudaMemset(b->p, 0, sizeof(double) * ns);
@@ -593,11 +593,21 @@ extern "C" int mp_fs1_set_state(mp_fs1 f, const double *const *vel, const double
     if (!f || !vel)
         return fail(MP_BAD_ARG, "mp_fs1_set_state: null argument");
     cudaStream_t st = S(s);
+    int cur_step = 0;
+    MP_CUDA(cudaMemcpyAsync(&cur_step, f->step.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     for (int d = 0; d < f->dim; d++)
         MP_CUDA(cudaMemcpyAsync(f->vel[f->cur][d].p, vel[d], sizeof(double) * f->nv,
                                 cudaMemcpyDefault, st));
     if (p)
         MP_CUDA(cudaMemcpyAsync(f->P.W.x.p, p, sizeof(double) * f->P.sys.nsys, cudaMemcpyDefault, st));
+    MP_CUDA(cudaStreamSynchronize(st));
+    // The pressure history of the extrapolated and learned guesses survives a state
+    // that continues at the current step index; any other index restarts it from p.
+    if (it != cur_step) {
+        const size_t bytes = sizeof(double) * f->P.sys.nsys;
+        for (dbuf<double> *h : {&f->pcur, &f->ph1, &f->ph2})
+            MP_CUDA(cudaMemcpyAsync(h->p, f->P.W.x.p, bytes, cudaMemcpyDeviceToDevice, st));
+    }
     MP_CUDA(cudaMemcpyAsync(f->step.p, &it, sizeof(int), cudaMemcpyHostToDevice, st));
     MP_CUDA(cudaStreamSynchronize(st));
     return MP_OK;

@@ -289,10 +289,15 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpFwdArgs A) {
             __syncthreads();
         }
         if (live) {
-            if (MODE == MLP_MODE_FIELDS)
-                A.x[row] = A.F.pcur[row] + (double)out / A.F.norms[1];
-            else
+            if (MODE == MLP_MODE_FIELDS) {
+                // linear extrapolation plus the predicted correction
+                const double pc = A.F.pcur[row], s2 = A.F.norms[2];
+                // (clamped to 8 units: the training targets have unit RMS)
+                const double corr = fmin(fmax((double)out, -8.0), 8.0);
+                A.x[row] = 2.0 * pc - A.F.ph1[row] + (s2 > 0 ? corr / s2 : 0.0);
+            } else {
                 A.y[row] = out;
+            }
         }
     }
     __syncthreads();
@@ -402,18 +407,20 @@ __global__ void k_mlp_adam(float *theta, float *m1, float *m2, const float *g, i
 
 // spacing feature, norms, sample collection
 __global__ void k_mlp_norms(MlpFields F, double *partials, unsigned *ticket, double *norms) {
-    __shared__ double red[32 * 2];
-    double acc[2] = {0, 0};
+    __shared__ double red[32 * 3];
+    double acc[3] = {0, 0, 0};
     const int stride = gridDim.x * blockDim.x;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.nv; i += stride) {
         acc[0] += F.b[i] * F.b[i];
-        const double d = F.pcur[i] - F.ph1[i];
+        const double p1 = F.ph1[i], d = F.pcur[i] - p1, d2 = d - (p1 - F.ph2[i]);
         acc[1] += d * d;
+        acc[2] += d2 * d2;
     }
-    if (grid_reduce<2>(acc, partials, ticket, red) && threadIdx.x == 0) {
-        const double rb = sqrt(acc[0] / F.nv), rp = sqrt(acc[1] / F.nv);
-        norms[0] = rb > 0 ? 1.0 / rb : 0.0;
-        norms[1] = rp > 0 ? 1.0 / rp : 0.0;
+    if (grid_reduce<3>(acc, partials, ticket, red) && threadIdx.x == 0) {
+        for (int k = 0; k < 3; k++) {
+            const double r = sqrt(acc[k] / F.nv);
+            norms[k] = r > 0 ? 1.0 / r : 0.0;
+        }
     }
 }
 
@@ -452,7 +459,8 @@ __global__ void k_mlp_collect(MlpFields F, const int *idx, int nidx, const doubl
         v.w = pack_bf16x2(f[c + 6], f[c + 7]);
         dst[c / 8] = v;
     }
-    t[s] = (float)((xnew[i] - F.pcur[i]) * sp);
+    const double pc = F.pcur[i];
+    t[s] = (float)(((xnew[i] - pc) - (pc - F.ph1[i])) * F.norms[2]);
 }
 
 __global__ void k_f32_to_bf16(const float *a, uint16_t *b, size_t n) {

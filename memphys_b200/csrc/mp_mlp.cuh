@@ -9,7 +9,11 @@
 //   layers 64 -> 128 -> 128 -> 128 (ReLU) -> 1, BF16 weights and BF16
 //          activations between layers, FP32 accumulation; the last hidden
 //          layer stays FP32 for the output dot product
-//   output the increment divided by RMS(p^n - p^{n-1})
+//   output the correction to the linear extrapolation,
+//          (p^{n+1} - p^n) - (p^n - p^{n-1}), divided by the RMS over the cloud of
+//          the last second difference (p^n - p^{n-1}) - (p^{n-1} - p^{n-2}); the
+//          guess is 2 p^n - p^{n-1} plus the scaled prediction, so the network's
+//          pointwise error scales with the (small) correction, not the increment
 //
 // The three hidden layers run on the 5th-generation tensor cores
 // (tcgen05.mma, accumulators in tensor memory); training runs on the GPU with
@@ -45,17 +49,19 @@ struct MlpFields {
     const double *ph2;       // p^{n-2}
     const float *hloc;       // node spacing / mean spacing
     const uint8_t *bflag;
-    const double *norms;     // [0] 1/RMS(b), [1] 1/RMS(p^n - p^{n-1})
+    const double *norms;     // [0] 1/RMS(b), [1] 1/RMS(p^n - p^{n-1}), [2] 1/RMS(second difference)
 };
 
 struct Mlp;
 Mlp *mlp_of(::mp_mlp_s *h);
 int mlp_create(Mlp **out, uint64_t seed);
 void mlp_destroy(Mlp *m);
-// x[i] = pcur[i] + RMS(dp) * net(features_i) for i < nv (tensor cores); x[nv..) untouched.
+// x[i] = 2 pcur[i] - ph1[i] + RMS(d2p) * net(features_i) for i < nv (tensor cores);
+// x[nv..) untouched.
 // Skipped while *step < 2 (no pressure history yet).
 int mlp_predict_fields(Mlp &m, const MlpFields &F, double *x, const int *step, cudaStream_t s);
-// row-major BF16 features of the nodes in `idx` and targets (xnew - pcur) / RMS(dp), written to
+// row-major BF16 features of the nodes in `idx` and targets
+// ((xnew - pcur) - (pcur - ph1)) / RMS(d2p), written to
 // slot ((*step - 2) % cap_steps) of a sample ring; skipped while *step < 2
 int mlp_collect(const MlpFields &F, const int *idx, int nidx, const double *xnew, uint16_t *X,
                 float *t, const int *step, int cap_steps, cudaStream_t s);

@@ -309,7 +309,7 @@ def test_fs1_mg32_matches_fp64(mp_lib):
         assert np.abs(gv[d] - rv[d]).max() <= 1e-7 * np.abs(rv[d]).max()
     assert np.all(log[:, 1] <= 1e-10)
     *_, log64 = run_fs1_pair(cl, 2e-4, 6, solver_type="cuda_bicgstab_amg", tol=1e-10)
-    assert np.all(log[:, 0] <= log64[:, 0] + 1)
+    assert log[:, 0].sum() <= 1.05 * log64[:, 0].sum() + 1
 
 
 def test_fs1_channel_with_outlet_and_neumann_velocity(mp_lib):
