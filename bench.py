@@ -263,7 +263,10 @@ def run_ours(args, ws, rank, local, pg):
         err = [float(np.abs(vv[d] - vel64[d]).max() / np.abs(vel64[d]).max()) for d in range(2)]
         perr = float(np.abs((pp - p64)[:nv]).max() / np.abs(p64[:nv]).max())
         ms = max_over_ranks(pg, ms)
-        return {"ms_per_step": round(ms, 4), "speedup_vs_plain_fp64": round(ms64_max / ms, 3),
+        extra = {}
+        if guess == capi.MP_GUESS_LEARNED:
+            extra["learned_weight_mean"] = float(np.mean(lg[:, 6]))
+        return {**extra, "ms_per_step": round(ms, 4), "speedup_vs_plain_fp64": round(ms64_max / ms, 3),
                 "iters_per_step": float(np.mean(lg[:, 0])),
                 "relres0_mean": float(np.mean(lg[:, 4])), "max_relres": float(lg[:, 1].max()),
                 "refinements_per_step": float(np.mean(lg[:, 5])),

@@ -263,7 +263,8 @@ int mp_fs1_last_stats(mp_fs1 f, int *iters, double *relres, double *abs_res, dou
 /* the logs of `count` steps starting at step `first`, MP_LOG_FIELDS doubles per
  * step: iterations (mixed: inner sweeps), relative residual, absolute residual,
  * regularisation alpha, relative residual of the initial guess, refinement
- * sweeps (mixed), and two reserved fields; the device keeps the last 4096 steps */
+ * sweeps (mixed), the weight given to the learned correction (MP_GUESS_LEARNED),
+ * and one reserved field; the device keeps the last 4096 steps */
 #define MP_LOG_FIELDS 8
 int mp_fs1_log(mp_fs1 f, int first, int count, double *out);
 /* kernels in one graph step: `fixed` once per step, `per_sweep` per BiCGSTAB

@@ -874,6 +874,67 @@ int amg_apply(const Amg &a, const T *in, T *out, const int *done, cudaStream_t s
 template int amg_apply<double>(const Amg &, const double *, double *, const int *, cudaStream_t);
 template int amg_apply<float>(const Amg &, const float *, float *, const int *, cudaStream_t);
 
+// ------------------------------------------------------- field filter
+__global__ void k_filter_scale(int n, double *s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        s[i] = s[i] != 0.0 ? 1.0 / s[i] : 0.0;
+}
+
+__global__ void k_scale_vec(int n, const double *s, double *v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        v[i] *= s[i];
+}
+
+__global__ void k_fill(int n, double v, double *x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        x[i] = v;
+}
+
+int amg_filter_size(const Amg &a) { return a.L.size() > 1 ? a.L[1]->n : 0; }
+
+int amg_filter_setup(const Amg &a, double *scale1, cudaStream_t s) {
+    if (a.L.size() < 2)
+        return MP_OK;
+    const AmgLevel &L = *a.L[0];
+    dbuf<double> ones;
+    MP_TRY(ones.alloc(L.n));
+    k_fill<<<(L.n + 255) / 256, 256, 0, s>>>(L.n, 1.0, ones.p);
+    MP_CHECK_LAUNCH();
+    const ChebC c{};
+    const CsrView<double> Rc{L.Rc.n, L.Rc.rp.p, L.Rc.ci.p, L.Rc.v64.p};
+    MP_TRY((level_op<double, double, false, EP_PLAIN>(L.sR.mode, L.R.view64(), Rc, ones.p, nullptr,
+                                                      nullptr, nullptr, nullptr, scale1, c,
+                                                      a.zero_flag.p, s)));
+    const int n1 = a.L[1]->n;
+    k_filter_scale<<<(n1 + 255) / 256, 256, 0, s>>>(n1, scale1);
+    MP_CHECK_LAUNCH();
+    MP_CUDA(cudaStreamSynchronize(s));
+    return MP_OK;
+}
+
+int amg_filter(const Amg &a, const double *c, double *work1, const double *scale1, double *out,
+               cudaStream_t s) {
+    if (a.L.size() < 2)
+        return MP_OK;
+    const AmgLevel &L = *a.L[0];
+    const ChebC k{};
+    const CsrView<double> Rc{L.Rc.n, L.Rc.rp.p, L.Rc.ci.p, L.Rc.v64.p};
+    const CsrView<double> Pc{L.Pc.n, L.Pc.rp.p, L.Pc.ci.p, L.Pc.v64.p};
+    MP_TRY((level_op<double, double, false, EP_PLAIN>(L.sR.mode, L.R.view64(), Rc, c, nullptr,
+                                                      nullptr, nullptr, nullptr, work1, k,
+                                                      a.zero_flag.p, s)));
+    const int n1 = a.L[1]->n;
+    k_scale_vec<<<(n1 + 255) / 256, 256, 0, s>>>(n1, scale1, work1);
+    MP_CHECK_LAUNCH();
+    MP_TRY((level_op<double, double, false, EP_PLAIN>(L.sP.mode, L.P.view64(), Pc, work1, nullptr,
+                                                      nullptr, nullptr, nullptr, out, k,
+                                                      a.zero_flag.p, s)));
+    return MP_OK;
+}
+
 // ------------------------------------------------------------- autotuner
 // For each level operator and transfer, time y = M u with every schedule
 // (sliced ELL, CSR with 4/8/16/32 lanes per row) and keep the fastest.  The

@@ -76,6 +76,15 @@ struct Amg {
 };
 
 int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t s);
+// Low-pass filter of a field through the first coarse level:
+//   out = P0 diag(scale1) R0 c,   scale1 = 1 / (R0 1)   (out may alias c)
+// (a locally weighted average onto the aggregates, interpolated back by the
+// smoothed prolongator: smooth fields pass, node-to-node noise is averaged out).
+// work1 and scale1 hold one entry per level-1 node.  No-op for a one-level hierarchy.
+int amg_filter_size(const Amg &a);
+int amg_filter_setup(const Amg &a, double *scale1, cudaStream_t s);
+int amg_filter(const Amg &a, const double *c, double *work1, const double *scale1, double *out,
+               cudaStream_t s);
 void amg_destroy(Amg *a);
 
 // out = V-cycle(in) on the first n0 entries (the border entry is handled by

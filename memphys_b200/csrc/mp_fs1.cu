@@ -17,6 +17,7 @@
 // solver's device-controlled while loop) is a single graph launch.
 #include <cmath>
 #include <cstring>
+#include "mp_amg.cuh"
 #include "mp_cloud.cuh"
 #include "mp_mlp.cuh"
 #include "mp_ppe.cuh"
@@ -250,7 +251,7 @@ __global__ void k_step_log(int *step, const BicgScalars *S, double *log, int cap
     e[3] = bordered ? x[nv] : 0.0;
     e[4] = S->relres0;
     e[5] = mixed ? S->outer_it : 0;
-    e[6] = 0.0;
+    e[6] = S->guess_theta;
     e[7] = 0.0;
     *step = s + 1;
 }
@@ -319,6 +320,7 @@ struct mp_fs1_s {
     int guess = MP_GUESS_PREVIOUS;
     // pressure history for the extrapolated and learned guesses
     dbuf<double> pcur, ph1, ph2, norms;
+    dbuf<double> corr, flt1, flt_scale;  // learned correction and its coarse-level filter
     // learned guess
     Mlp *mlp = nullptr;
     dbuf<float> hloc;
@@ -377,14 +379,26 @@ static int fs1_issue_pre(mp_fs1_s *f, int cur, cudaStream_t s) {
     MP_CHECK_LAUNCH();
     if (f->guess != MP_GUESS_PREVIOUS || f->collect) {
         const int ns = f->P.sys.nsys;
-        const int gmode = f->guess == MP_GUESS_LEARNED ? MP_GUESS_PREVIOUS : f->guess;
+        // the learned guess starts from the extrapolation (every entry, the border too)
+        const int gmode = f->guess == MP_GUESS_LEARNED ? MP_GUESS_EXTRAPOLATE : f->guess;
         k_guess<<<(unsigned)std::min((ns + 255) / 256, sm_count() * 4), 256, 0, s>>>(
             ns, gmode, f->P.W.x.p, f->pcur.p, f->ph1.p, f->step.p);
         MP_CHECK_LAUNCH();
         if (f->guess == MP_GUESS_LEARNED) {
             const MlpFields F = fs1_fields(f);
             MP_TRY(mlp_norms(F, f->norms.p, f->P.W.partials.p, f->P.W.ticket.p, s));
-            MP_TRY(mlp_predict_fields(*f->mlp, F, f->P.W.x.p, f->step.p, s));
+            // extrapolation + the prediction, low-pass filtered through the first
+            // multigrid level (the pointwise noise of the network would otherwise
+            // dominate the residual of the guess) and weighted to minimise the
+            // guess's residual
+            const bool filt = f->flt_scale.p != nullptr;
+            MP_TRY(mlp_predict_fields(*f->mlp, F, f->P.W.x.p, filt ? f->corr.p : nullptr,
+                                      f->step.p, s));
+            if (filt) {  // corr <- filtered corr; x += theta corr
+                MP_TRY(amg_filter(*f->P.sys.amg, f->corr.p, f->flt1.p, f->flt_scale.p,
+                                  f->corr.p, s));
+                MP_TRY(f->P.issue_guess_min_residual(f->corr.p, s));
+            }
         }
     }
     return MP_OK;
@@ -706,6 +720,7 @@ extern "C" int mp_fs1_attach_mlp(mp_fs1 f, mp_mlp m, int sample_nodes, int capac
     MP_CUDA(cudaDeviceSynchronize());
     f->mlp = mlp_of(m);
     const int nv = f->nv;
+    MP_TRY(mlp_reserve_fields(*f->mlp, nv));
     // node spacing feature: distance to the nearest stencil member over its mean
     MP_TRY(f->hloc.alloc(nv));
     {
@@ -742,6 +757,13 @@ extern "C" int mp_fs1_attach_mlp(mp_fs1 f, mp_mlp m, int sample_nodes, int capac
     MP_TRY(f->sX.alloc((size_t)capacity_steps * f->nsample * MLP_IN));
     MP_TRY(f->st.alloc((size_t)capacity_steps * f->nsample));
     f->collect = collect ? 1 : 0;
+    if (f->P.sys.amg && amg_filter_size(*f->P.sys.amg) > 0) {
+        const int n1 = amg_filter_size(*f->P.sys.amg);
+        MP_TRY(f->corr.alloc(nv));
+        MP_TRY(f->flt1.alloc(n1));
+        MP_TRY(f->flt_scale.alloc(n1));
+        MP_TRY(amg_filter_setup(*f->P.sys.amg, f->flt_scale.p, 0));
+    }
     fs1_invalidate(f);
     return MP_OK;
 }

@@ -121,6 +121,70 @@ __global__ void __launch_bounds__(KT)
     }
 }
 
+// ------------------------------------------------ learned-guess weight
+// With x the extrapolated guess and f a correction field: theta = <r, A f> /
+// <A f, A f>, r = b - A x, over the bordered system (the border entry of f is 0,
+// the border row of A f is sum f_i).  One pass over the operator for both
+// products; the last block stores theta.  (Minimising the residual restricted
+// to the first multigrid level instead gave more iterations at 1M nodes.)
+__global__ void __launch_bounds__(KT)
+    k_guess_mr(EllView<double> A, int bordered, const double *x, const double *b,
+               const double *f, BicgScalars *S, RedBuf R) {
+    KRYLOV_SMEM
+    const int nv = A.nrows, lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int nsl = (nv + SLICE - 1) / SLICE;
+    double acc[4] = {0, 0, 0, 0};  // <r, Af>, <Af, Af>, sum x, sum f
+    const double xb = bordered ? x[nv] : 0.0;
+    for (int w = gwarp(); w < nsl; w += nwarps) {
+        size_t base;
+        int K;
+        slice_span(A, w, base, K);
+        base += 2 * lane;
+        double ax[2] = {0, 0}, af[2] = {0, 0}, sx[2] = {0, 0}, sf[2] = {0, 0};
+        for (int k = 0; k < K; k++) {
+            const size_t o = base + (size_t)k * SLICE;
+            const int2 c = __ldcs(reinterpret_cast<const int2 *>(A.cols + o));
+            const double2 v = __ldcs(reinterpret_cast<const double2 *>(A.vals + o));
+            const double x0 = __ldg(x + c.x), x1 = __ldg(x + c.y);
+            const double f0 = __ldg(f + c.x), f1 = __ldg(f + c.y);
+            if (k == 0) {  // self column: the border row's sums
+                sx[0] = x0, sx[1] = x1, sf[0] = f0, sf[1] = f1;
+            }
+            ax[0] = fma(v.x, x0, ax[0]);
+            ax[1] = fma(v.y, x1, ax[1]);
+            af[0] = fma(v.x, f0, af[0]);
+            af[1] = fma(v.y, f1, af[1]);
+        }
+        const int i0 = w * SLICE + 2 * lane;
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            if (i0 + q >= nv)
+                continue;
+            const double r = b[i0 + q] - (ax[q] + xb);
+            acc[0] += r * af[q];
+            acc[1] += af[q] * af[q];
+            acc[2] += sx[q];
+            acc[3] += sf[q];
+        }
+    }
+    if (grid_reduce<4>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
+        double num = acc[0], den = acc[1];
+        if (bordered) {
+            const double rn = b[nv] - acc[2];
+            num += rn * acc[3];
+            den += acc[3] * acc[3];
+        }
+        const double th = den > 0 ? num / den : 0.0;
+        S->guess_theta = isfinite(th) ? th : 0.0;
+    }
+}
+
+__global__ void k_guess_axpy(int nv, double *x, const double *f, const BicgScalars *S) {
+    const double th = S->guess_theta;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x)
+        x[i] += th * f[i];
+}
+
 // Eigen's restart: r = b - A x, r0 = r, rho = r0_sq = ||r||^2 (rare path)
 template <class T>
 __global__ void __launch_bounds__(KT)
@@ -621,6 +685,15 @@ __global__ void k_ir_setup(BicgScalars *S, double tol, int outer_max) {
 
 int Ppe::issue_ir_setup(cudaStream_t st) {
     k_ir_setup<<<1, 1, 0, st>>>(W.scal.p, cfg.tol, cfg.max_refine);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+int Ppe::issue_guess_min_residual(const double *f, cudaStream_t st) {
+    k_guess_mr<<<slice_blocks(sys.nv), KT, 0, st>>>(sys.A.view64(), sys.bordered, W.x.p, W.b64.p,
+                                                    f, W.scal.p, RedBuf{W.partials.p, W.ticket.p});
+    MP_CHECK_LAUNCH();
+    k_guess_axpy<<<vec_blocks(sys.nv), KT, 0, st>>>(sys.nv, W.x.p, f, W.scal.p);
     MP_CHECK_LAUNCH();
     return MP_OK;
 }

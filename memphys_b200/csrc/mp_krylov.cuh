@@ -30,6 +30,7 @@ struct BicgScalars {
     int outer_it, outer_max, outer_done, total_inner;
     double tol_outer2, b64_sq;
     double relres0;     // ||b - A x0|| / ||b|| of the initial guess (first residual of a solve)
+    double guess_theta; // weight of the learned correction in the last initial guess
 };
 
 struct PpeSystem {

@@ -33,6 +33,9 @@ struct Mlp {
     dbuf<float> h3, y, d3, d2, d1, lossbuf;
     dbuf<int> idx;
     dbuf<int> err;  // device flag: an mbarrier wait ran out
+    // per-node features and outputs of the field prediction (sized to the cloud)
+    dbuf<uint16_t> fx;
+    dbuf<float> fy;
 };
 
 // ------------------------------------------------------------ layout helpers
@@ -116,7 +119,7 @@ __device__ __forceinline__ float bf16_round(float a) {
 }
 
 // ---------------------------------------------------------- forward kernel
-enum { MLP_MODE_FIELDS = 0, MLP_MODE_ROWS = 1, MLP_MODE_TRAIN = 2 };
+enum { MLP_MODE_ROWS = 1, MLP_MODE_TRAIN = 2 };
 
 struct MlpFwdArgs {
     int n;                   // rows
@@ -129,10 +132,6 @@ struct MlpFwdArgs {
     // train mode: stored activations
     uint16_t *h1, *h2;
     float *h3;
-    // fields mode
-    MlpFields F;
-    double *x;               // initial guess written here
-    const int *step;         // fields mode: skip while *step < 2
     int *err;
 };
 
@@ -153,8 +152,6 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpFwdArgs A) {
     extern __shared__ __align__(1024) unsigned char mlp_smem_raw[];
     MlpSmem &S = *reinterpret_cast<MlpSmem *>(mlp_smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5;
-    if (MODE == MLP_MODE_FIELDS && *A.step < 2)
-        return;  // no pressure history yet: the guess stays p^n
     // weights (already in operand layout) and vectors into shared memory
     {
         const uint4 *src = reinterpret_cast<const uint4 *>(A.pack);
@@ -189,38 +186,8 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpFwdArgs A) {
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int row = tile * MLP_TILE + tid;
         const bool live = row < A.n;
-        // ---- features of this thread's row into the A operand
-        if (MODE == MLP_MODE_FIELDS) {
-            const MlpFields &F = A.F;
-            float f[MLP_IN];
-#pragma unroll
-            for (int k = 0; k < MLP_IN; k++)
-                f[k] = 0.f;
-            if (live) {
-                const double sb = F.norms[0], sp = F.norms[1];
-                const size_t base = (size_t)(row / 64) * F.K * 64 + (row % 64);
-#pragma unroll 4
-                for (int k = 0; k < MLP_STENCIL; k++) {
-                    const int j = F.cols[base + (size_t)k * 64];
-                    const double pc = F.pcur[j], p1 = F.ph1[j];
-                    f[3 * k] = (float)(F.b[j] * sb);
-                    f[3 * k + 1] = (float)((pc - p1) * sp);
-                    f[3 * k + 2] = (float)((p1 - F.ph2[j]) * sp);
-                }
-                f[60] = F.hloc[row];
-                f[61] = F.bflag[row] ? 1.f : 0.f;
-                f[62] = 1.f;
-            }
-#pragma unroll
-            for (int c = 0; c < MLP_IN; c += 8) {
-                uint4 v;
-                v.x = pack_bf16x2(f[c], f[c + 1]);
-                v.y = pack_bf16x2(f[c + 2], f[c + 3]);
-                v.z = pack_bf16x2(f[c + 4], f[c + 5]);
-                v.w = pack_bf16x2(f[c + 6], f[c + 7]);
-                *reinterpret_cast<uint4 *>(&S.xa[cm_off(tid, c, MLP_IN)]) = v;
-            }
-        } else {
+        // ---- this thread's feature row into the A operand
+        {
             const int src = live ? (A.idx ? A.idx[row] : row) : 0;
             const uint4 *xr = reinterpret_cast<const uint4 *>(A.X + (size_t)src * MLP_IN);
 #pragma unroll
@@ -288,17 +255,8 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpFwdArgs A) {
             asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
             __syncthreads();
         }
-        if (live) {
-            if (MODE == MLP_MODE_FIELDS) {
-                // linear extrapolation plus the predicted correction
-                const double pc = A.F.pcur[row], s2 = A.F.norms[2];
-                // (clamped to 8 units: the training targets have unit RMS)
-                const double corr = fmin(fmax((double)out, -8.0), 8.0);
-                A.x[row] = 2.0 * pc - A.F.ph1[row] + (s2 > 0 ? corr / s2 : 0.0);
-            } else {
-                A.y[row] = out;
-            }
-        }
+        if (live)
+            A.y[row] = out;
     }
     __syncthreads();
     if (warp == 0)
@@ -424,21 +382,15 @@ __global__ void k_mlp_norms(MlpFields F, double *partials, unsigned *ticket, dou
     }
 }
 
-__global__ void k_mlp_collect(MlpFields F, const int *idx, int nidx, const double *xnew,
-                              uint16_t *X, float *t, const int *step, int cap_steps) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nidx || *step < 2)
-        return;
-    const size_t slot = (size_t)((*step - 2) % cap_steps) * nidx;
-    X += slot * MLP_IN;
-    t += slot;
-    const int i = idx[s];
+// the 64 features of node i (layout in mp_mlp.cuh), as BF16 into a 128-byte row
+__device__ __forceinline__ void node_features(const MlpFields &F, int i, uint16_t *row) {
     const double sb = F.norms[0], sp = F.norms[1];
     float f[MLP_IN];
 #pragma unroll
     for (int k = 0; k < MLP_IN; k++)
         f[k] = 0.f;
     const size_t base = (size_t)(i / 64) * F.K * 64 + (i % 64);
+#pragma unroll 4
     for (int k = 0; k < MLP_STENCIL; k++) {
         const int j = F.cols[base + (size_t)k * 64];
         const double pc = F.pcur[j], p1 = F.ph1[j];
@@ -449,7 +401,7 @@ __global__ void k_mlp_collect(MlpFields F, const int *idx, int nidx, const doubl
     f[60] = F.hloc[i];
     f[61] = F.bflag[i] ? 1.f : 0.f;
     f[62] = 1.f;
-    uint4 *dst = reinterpret_cast<uint4 *>(X + (size_t)s * MLP_IN);
+    uint4 *dst = reinterpret_cast<uint4 *>(row);
 #pragma unroll
     for (int c = 0; c < MLP_IN; c += 8) {
         uint4 v;
@@ -459,8 +411,46 @@ __global__ void k_mlp_collect(MlpFields F, const int *idx, int nidx, const doubl
         v.w = pack_bf16x2(f[c + 6], f[c + 7]);
         dst[c / 8] = v;
     }
+}
+
+__global__ void k_mlp_collect(MlpFields F, const int *idx, int nidx, const double *xnew,
+                              uint16_t *X, float *t, const int *step, int cap_steps) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nidx || *step < 2)
+        return;
+    const size_t slot = (size_t)((*step - 2) % cap_steps) * nidx;
+    X += slot * MLP_IN;
+    t += slot;
+    const int i = idx[s];
+    node_features(F, i, X + (size_t)s * MLP_IN);
     const double pc = F.pcur[i];
     t[s] = (float)(((xnew[i] - pc) - (pc - F.ph1[i])) * F.norms[2]);
+}
+
+// features of every node (skipped while *step < 2: no pressure history)
+__global__ void __launch_bounds__(256) k_mlp_features(MlpFields F, uint16_t *X, const int *step) {
+    if (*step < 2)
+        return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.nv; i += gridDim.x * blockDim.x)
+        node_features(F, i, X + (size_t)i * MLP_IN);
+}
+
+// The prediction as a pressure correction: the clamped output (8 units: the
+// training targets have unit RMS) scaled back by the RMS of the second
+// difference.  Written to corr when set, else added to x (which holds the
+// extrapolated guess).  Zero while *step < 2 (no second difference yet).
+__global__ void k_mlp_combine(MlpFields F, const float *y, double *x, double *corr,
+                              const int *step) {
+    const bool early = *step < 2;
+    const double s2 = F.norms[2];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.nv; i += gridDim.x * blockDim.x) {
+        const double cl = fmin(fmax((double)y[i], -8.0), 8.0);
+        const double c = (early || !(s2 > 0)) ? 0.0 : cl / s2;
+        if (corr)
+            corr[i] = c;
+        else
+            x[i] += c;
+    }
 }
 
 __global__ void k_f32_to_bf16(const float *a, uint16_t *b, size_t n) {
@@ -536,16 +526,33 @@ static int mlp_check_err(Mlp &m, cudaStream_t s) {
     return MP_OK;
 }
 
-int mlp_predict_fields(Mlp &m, const MlpFields &F, double *x, const int *step, cudaStream_t s) {
+int mlp_predict_fields(Mlp &m, const MlpFields &F, double *x, double *corr, const int *step,
+                       cudaStream_t s) {
+    if ((size_t)F.nv > m.fy.n)
+        return fail(MP_BAD_ARG, "field prediction for %d nodes: %zu reserved", F.nv, m.fy.n);
+    const unsigned g = (unsigned)std::min((F.nv + 255) / 256, sm_count() * 16);
+    k_mlp_features<<<g, 256, 0, s>>>(F, m.fx.p, step);
+    MP_CHECK_LAUNCH();
     MlpFwdArgs a{};
-    a.step = step;
     a.n = F.nv;
     a.pack = m.pack.p;
     a.theta = m.theta.p;
-    a.F = F;
-    a.x = x;
+    a.X = m.fx.p;
+    a.y = m.fy.p;
     a.err = m.err.p;
-    return launch_forward<MLP_MODE_FIELDS>(a, s);
+    MP_TRY(launch_forward<MLP_MODE_ROWS>(a, s));
+    k_mlp_combine<<<g, 256, 0, s>>>(F, m.fy.p, x, corr, step);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+int mlp_reserve_fields(Mlp &m, int nv) {
+    if ((size_t)nv <= m.fy.n)
+        return MP_OK;
+    MP_TRY(m.fx.alloc((size_t)nv * MLP_IN));
+    MP_TRY(m.fy.alloc(nv));
+    MP_CUDA(cudaMemset(m.fx.p, 0, m.fx.bytes()));
+    return MP_OK;
 }
 
 int mlp_norms(const MlpFields &F, double *norms, double *partials, unsigned *ticket,

@@ -56,10 +56,13 @@ struct Mlp;
 Mlp *mlp_of(::mp_mlp_s *h);
 int mlp_create(Mlp **out, uint64_t seed);
 void mlp_destroy(Mlp *m);
-// x[i] = 2 pcur[i] - ph1[i] + RMS(d2p) * net(features_i) for i < nv (tensor cores);
-// x[nv..) untouched.
-// Skipped while *step < 2 (no pressure history yet).
-int mlp_predict_fields(Mlp &m, const MlpFields &F, double *x, const int *step, cudaStream_t s);
+// The predicted correction RMS(d2p) * net(features_i) for i < nv (tensor cores),
+// added to x (which holds the extrapolation 2 p^n - p^{n-1}) or, with corr set,
+// written to corr.  Zero while *step < 2 (no second difference yet).
+int mlp_predict_fields(Mlp &m, const MlpFields &F, double *x, double *corr, const int *step,
+                       cudaStream_t s);
+// buffers of the field prediction for nv nodes (allocate before any stream capture)
+int mlp_reserve_fields(Mlp &m, int nv);
 // row-major BF16 features of the nodes in `idx` and targets
 // ((xnew - pcur) - (pcur - ph1)) / RMS(d2p), written to
 // slot ((*step - 2) % cap_steps) of a sample ring; skipped while *step < 2

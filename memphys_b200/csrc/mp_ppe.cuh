@@ -56,6 +56,9 @@ struct Ppe {
     int issue_ir_inner_prologue(cudaGraphConditionalHandle h, cudaStream_t st);
     int issue_ir_sweep(cudaGraphConditionalHandle h, cudaStream_t st);
     int issue_ir_update(cudaStream_t st);
+    // initial guess x = x + theta f with theta minimising ||b - A x|| (FP64 operator,
+    // border included); f has nv entries (its border entry is zero)
+    int issue_guess_min_residual(const double *f, cudaStream_t st);
     int build_solve_graph(GraphBuilder &gb);
     int solve_eager(cudaStream_t st);
     // solve with W.b64 as rhs and W.x as initial guess / solution
