@@ -61,9 +61,13 @@ def parse():
     ap.add_argument("--epochs", type=int, default=10)
     ap.add_argument("--inner-tol", type=float, default=1e-5,
                     help="mixed precision: relative reduction of each FP32 refinement solve")
-    ap.add_argument("--profile", default=None, choices=["steps", "spmv"],
-                    help="set up, warm up, then run `--steps` steps (or SpMV launches) inside a "
-                         "profiler capture range and exit (for ncu --profile-from-start off)")
+    ap.add_argument("--profile", default=None, choices=["steps", "spmv", "stencil"],
+                    help="set up, warm up, then run `--steps` steps (SpMV launches, stencil-weight "
+                         "computations) inside a profiler capture range and exit (for ncu "
+                         "--profile-from-start off)")
+    ap.add_argument("--variant", default="plain",
+                    choices=["plain", "mg32", "extrapolated_mg32", "learned_mg32"],
+                    help="solver configuration of --profile steps")
     return ap.parse_args()
 
 
@@ -202,7 +206,7 @@ def run_ours(args, ws, rank, local, pg):
     ns = fs.system_size
     p0 = np.zeros(ns)
     if args.profile:
-        return profile_range(args, cld, fs, vel0, p0, stream)
+        return profile_range(args, cl, cld, make, fs, vel0, p0, stream)
 
     # spin-up from rest, untimed, recording the learned guess's training samples
     # (features and solved increments of `--samples` fixed nodes at every step);
@@ -360,22 +364,61 @@ def run_ours(args, ws, rank, local, pg):
     return out
 
 
-def profile_range(args, cld, fs, vel0, p0, stream):
-    """Warm-up outside, `--steps` steps (or SpMV launches) inside the capture range."""
-    from memphys_b200 import capi
+def profile_range(args, cl, cld, make, fs, vel0, p0, stream):
+    """Warm-up outside, `--steps` steps (SpMV launches, weight computations) inside the
+    capture range."""
+    from memphys_b200 import capi, meshless
     L = capi.lib()
+    nv = cld.nv
     if args.profile == "steps":
+        if args.variant != "plain":
+            fs = make(precision=capi.MP_MG32)
+            if args.variant == "learned_mg32":
+                # train on a short spin-up first (outside the capture range)
+                net = meshless.MLP(seed=7)
+                meshless.attach_mlp(fs, net, sample_nodes=min(args.samples, nv),
+                                    capacity_steps=max(args.spinup, 3))
+                fs.set_state(vel0, p0, 0)
+                fs.step(max(args.spinup, 3), stream.handle)
+                stream.sync()
+                meshless.train_mlp(fs, epochs=args.epochs, batch=1024, lr=1e-3)
+                meshless.attach_mlp(fs, net, sample_nodes=1, capacity_steps=1, collect=False)
+                meshless.set_guess(fs, capi.MP_GUESS_LEARNED)
+            elif args.variant == "extrapolated_mg32":
+                meshless.set_guess(fs, capi.MP_GUESS_EXTRAPOLATE)
         fs.set_state(vel0, p0, 0)
-        fs.step(args.warmup, stream.handle)
+        fs.step(args.spinup + args.warmup, stream.handle)
         stream.sync()
         capi.check(L.mp_profiler(1))
         fs.step(args.steps, stream.handle)
         stream.sync()
         capi.check(L.mp_profiler(0))
-        log = fs.log(args.warmup, args.steps)
-        return {"profile": "steps", "iters": log[:, 0].tolist()}
+        log = fs.log(args.spinup + args.warmup, args.steps)
+        return {"profile": "steps", "variant": args.variant, "iters": log[:, 0].tolist()}
+    if args.profile == "stencil":
+        # the cloud's PHS-RBF-FD weights from its own stencils, device in and out
+        cld.fetch()
+        nb = cld.nb_points_col
+        n = nb.shape[1]
+        dx = capi.DeviceArray.from_host(np.ascontiguousarray(cl.xyz, np.float64))
+        dn = capi.DeviceArray.from_host(np.ascontiguousarray(nb, np.int32))
+        w = [capi.DeviceArray((nv, n)) for _ in range(3)]
+
+        def weights():
+            capi.check(L.mp_stencil_weights(capi.ptr(dx), nv, cl.dim, capi.ptr(dn), n, 3, 3,
+                                            capi.ptr(w[0]), capi.ptr(w[1]), None,
+                                            capi.ptr(w[2]), None, stream.handle),
+                       "mp_stencil_weights")
+        for _ in range(args.warmup):
+            weights()
+        stream.sync()
+        capi.check(L.mp_profiler(1))
+        for _ in range(args.steps):
+            weights()
+        stream.sync()
+        capi.check(L.mp_profiler(0))
+        return {"profile": "stencil", "launches": args.steps, "stencils": nv, "n": n}
     op = cld.operator(capi.MP_LAPLACIAN)
-    nv = cld.nv
     x = capi.DeviceArray.from_host(np.random.default_rng(0).standard_normal(nv))
     y = capi.DeviceArray((nv,))
     for _ in range(args.warmup):

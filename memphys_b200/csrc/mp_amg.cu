@@ -377,6 +377,20 @@ __global__ void k_diff_level0(EllView<double> A, float *out, int *bad) {
         out[base] = i < A.nrows ? (float)sum : 0.f;
 }
 
+__global__ void k_pack_pairs(const int *cols, const float *v, int2 *out, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        out[i] = make_int2(cols[i], __float_as_int(v[i]));
+}
+
+static int pack_pairs(const int *cols, const float *v, size_t n, dbuf<int2> &out,
+                      cudaStream_t s) {
+    MP_TRY(out.alloc(n));
+    k_pack_pairs<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(cols, v, out.p, n);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
 static int diff_level0(const Ell &A0, AmgLevel &L, cudaStream_t s) {
     const EllView<double> A = A0.view64();
     MP_TRY(L.Ad.v32.alloc(A0.v64.n));
@@ -392,7 +406,8 @@ static int diff_level0(const Ell &A0, AmgLevel &L, cudaStream_t s) {
     if (hb)
         return fail(MP_BAD_ARG, "FP32 multigrid storage needs every stencil row to start with its "
                                 "own node (%d rows do not)", hb);
-    L.Ad32 = EllView<float>{A0.nrows, A0.ncols, A0.K, A0.cols.p, L.Ad.v32.p, A0.soff.p};
+    MP_TRY(pack_pairs(A0.cols.p, L.Ad.v32.p, A0.v64.n, L.Adpk, s));
+    L.Ad32 = EllView<float>{A0.nrows, A0.ncols, A0.K, A0.cols.p, L.Ad.v32.p, A0.soff.p, L.Adpk.p};
     return MP_OK;
 }
 
@@ -406,7 +421,10 @@ static int diff_level(const Csr &A, AmgLevel &L, cudaStream_t s) {
     MP_CUDA(cudaStreamSynchronize(s));
     L.Ad.v64.release();
     L.Acd.v64.release();
+    MP_TRY(pack_pairs(L.Ad.cols.p, L.Ad.v32.p, L.Ad.v32.n, L.Adpk, s));
+    MP_TRY(pack_pairs(L.Acd.ci.p, L.Acd.v32.p, L.Acd.v32.n, L.Acd.pk, s));
     L.Ad32 = L.Ad.view32();
+    L.Ad32.pk = L.Adpk.p;
     return MP_OK;
 }
 
@@ -618,6 +636,28 @@ __device__ __forceinline__ void spmv_pair(const EllView<V> &A, int w, int lane,
     a1 = 0;
     T s0 = 0, s1 = 0;
     int k0 = 0;
+    if constexpr (sizeof(V) == 4) {
+        if (A.pk) {  // {col, value} of both rows in one 16-byte load
+            const int4 *P = reinterpret_cast<const int4 *>(A.pk + base);
+            if (DIFF && K > 0) {
+                const int i0 = w * SLICE + 2 * lane;
+                s0 = i0 < A.nrows ? __ldg(x + i0) : T(0);
+                s1 = i0 + 1 < A.nrows ? __ldg(x + i0 + 1) : T(0);
+                const int4 e = __ldcs(P);
+                a0 = (T)__int_as_float(e.y) * s0;
+                a1 = (T)__int_as_float(e.w) * s1;
+                k0 = 1;
+            }
+#pragma unroll 4
+            for (int k = k0; k < K; k++) {
+                const int4 e = __ldcs(P + (size_t)k * (SLICE / 2));
+                const T g0 = __ldg(x + e.x), g1 = __ldg(x + e.z);
+                a0 = fma((T)__int_as_float(e.y), DIFF ? g0 - s0 : g0, a0);
+                a1 = fma((T)__int_as_float(e.w), DIFF ? g1 - s1 : g1, a1);
+            }
+            return;
+        }
+    }
     if (DIFF && K > 0) {
         const int i0 = w * SLICE + 2 * lane;
         s0 = i0 < A.nrows ? __ldg(x + i0) : T(0);
@@ -651,6 +691,7 @@ template <class V> struct CsrView {
     int nrows;
     const int *rp, *ci;
     const V *v;
+    const int2 *pk = nullptr;  // (column, FP32 value bits) pairs, when packed
 };
 
 // Row i of one fused SpMV (a = (M u)_i) followed by its epilogue:
@@ -713,9 +754,17 @@ __global__ void __launch_bounds__(256)
     if (row < M.nrows) {
         const int b0 = M.rp[row], e = M.rp[row + 1];
         const T ui = DIFF ? __ldg(u + row) : T(0);
-        for (int t = b0 + li; t < e; t += G) {
-            const T ut = __ldg(u + __ldcs(M.ci + t));
-            acc = fma((T)__ldcs(M.v + t), (DIFF && t != b0) ? ut - ui : ut, acc);
+        if (M.pk) {  // (column, FP32 value) pairs: one 8-byte load per entry
+            for (int t = b0 + li; t < e; t += G) {
+                const int2 q = __ldcs(M.pk + t);
+                const T ut = __ldg(u + q.x);
+                acc = fma((T)__int_as_float(q.y), (DIFF && t != b0) ? ut - ui : ut, acc);
+            }
+        } else {
+            for (int t = b0 + li; t < e; t += G) {
+                const T ut = __ldg(u + __ldcs(M.ci + t));
+                acc = fma((T)__ldcs(M.v + t), (DIFF && t != b0) ? ut - ui : ut, acc);
+            }
         }
     }
 #pragma unroll
@@ -806,7 +855,9 @@ template <> struct LvlOps<float, false> {
 };
 template <> struct LvlOps<float, true> : LvlOps<float, false> {
     static EllView<float> A(const AmgLevel &L) { return L.Ad32; }
-    static CsrView<float> Ac(const AmgLevel &L) { return {L.Acd.n, L.Acd.rp.p, L.Acd.ci.p, L.Acd.v32.p}; }
+    static CsrView<float> Ac(const AmgLevel &L) {
+        return {L.Acd.n, L.Acd.rp.p, L.Acd.ci.p, L.Acd.v32.p, L.Acd.pk.p};
+    }
 };
 
 static unsigned sblocks(int n) { return (unsigned)(((n + SLICE - 1) / SLICE + 7) / 8); }

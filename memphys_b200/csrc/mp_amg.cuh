@@ -28,6 +28,7 @@ struct DCsr {
     dbuf<int> rp, ci;
     dbuf<double> v64;
     dbuf<float> v32;
+    dbuf<int2> pk;  // (column, FP32 value bits) pairs, when packed
 };
 
 // kernel schedule of one operator, chosen by the setup-time autotuner:
@@ -57,6 +58,7 @@ struct AmgLevel {
     // Level 0 shares the PPE operator's columns and stores only values.
     Ell Ad;
     EllView<float> Ad32{};
+    dbuf<int2> Adpk;         // Ad as (column, value bits) pairs
     DCsr Acd;
 };
 

@@ -31,6 +31,9 @@ template <class T> struct EllView {
     const int *cols;
     const T *vals;
     const int *soff;
+    // FP32 operators may also carry (column, value bits) pairs in the same sliced
+    // order: one 16-byte load then fetches both entries of a lane's two rows
+    const int2 *pk = nullptr;
 };
 
 // start offset and width of slice w
