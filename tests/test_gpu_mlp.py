@@ -109,3 +109,36 @@ def test_learned_guess_saves_iterations(mp_lib):
     print("mean iterations / initial relres by guess:", res)
     assert res[capi.MP_GUESS_LEARNED][0] < res[capi.MP_GUESS_ZERO][0]
     assert res[capi.MP_GUESS_LEARNED][1] < res[capi.MP_GUESS_ZERO][1]
+
+
+def test_learned_guess_channel_with_obstacle(mp_lib):
+    """The learned-guess configuration at reduced size: channel [0,8]x[0,1] with a
+    cylinder of radius 0.1 at (1, 0.5), Re = 200; the network trains on the plain
+    solver's own steps, then its guess is compared with the zero initial guess."""
+    cl = clouds.channel_2d(0.025, seed=6)
+    prm = meshless.PARAMETERS(solver_type="cuda_bicgstab_amg", solver_tolerance=1e-8, n_iter=4000)
+    prm.rho, prm.mu = 1.0, 0.2 / 200.0  # Re = u D / nu with u = 1, D = 0.2
+    pts = meshless.POINTS(cl)
+    cld = meshless.CLOUD(pts, prm, compute_cond=False)
+    # a tenth of the calc_dt step: explicit PHS-RBF-FD advection on this coarse cloud
+    # (h = 0.025) grows spurious modes within ~60 steps at the full step
+    prm.dt = 0.1 * meshless.calc_dt(cld, 1.5, 1.0, 0.0, prm.mu / prm.rho, 0.25)
+    fs = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                    cl.p_dirichlet, 2, w_dirichlet_flag=cl.w_dirichlet)
+    fs.set_state([cl.vel_bc[0], cl.vel_bc[1]], np.zeros(fs.system_size), 0)
+    net = meshless.MLP(seed=11)
+    meshless.attach_mlp(fs, net, sample_nodes=4096, capacity_steps=60)
+    fs.step(60)
+    loss = meshless.train_mlp(fs, epochs=10, batch=1024, lr=1e-3)
+    assert np.isfinite(loss)
+    vel, p = fs.get_state()
+    res = {}
+    for guess in (capi.MP_GUESS_ZERO, capi.MP_GUESS_LEARNED):
+        meshless.set_guess(fs, guess)
+        fs.set_state(vel, p, 60 if guess == capi.MP_GUESS_LEARNED else 0)
+        fs.step(8)
+        log = fs.log(60 if guess == capi.MP_GUESS_LEARNED else 0, 8)
+        assert np.all(log[:, 1] <= 1e-8)
+        res[guess] = log[2:, 0].mean()
+    print("channel: mean iterations zero / learned guess:", res)
+    assert res[capi.MP_GUESS_LEARNED] < 0.8 * res[capi.MP_GUESS_ZERO]

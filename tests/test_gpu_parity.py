@@ -328,6 +328,20 @@ def test_fs1_3d_matches_oracle(mp_lib):
         assert np.abs(gv[d] - rv[d]).max() <= 1e-7 * max(np.abs(rv[d]).max(), 1e-12)
 
 
+@pytest.mark.parametrize("solver_type", ["cuda_bicgstab_amg_mixed", "cuda_bicgstab_amg_mg32"])
+def test_fs1_3d_mixed_precision_per_field_error(mp_lib, solver_type):
+    """The 3D mixed-precision configuration at reduced size (cube, PHS r^3 + degree 3,
+    20 monomials, 40-node stencils): FP32 inner solves under FP64 refinement, or FP32
+    multigrid under FP64 BiCGSTAB, against the FP64 oracle, error stated per field."""
+    cl = clouds.cube_3d(12, seed=4)
+    gv, gp, rv, rp_, log = run_fs1_pair(cl, 2e-4, 4, solver_type=solver_type, tol=1e-8)
+    err = [np.abs(gv[d] - rv[d]).max() / max(np.abs(rv[d]).max(), 1e-12) for d in range(3)]
+    perr = np.abs(gp[:cl.nv] - rp_[:cl.nv]).max() / np.abs(rp_[:cl.nv]).max()
+    print(f"{solver_type}: relative error u {err[0]:.2e} v {err[1]:.2e} w {err[2]:.2e} p {perr:.2e}")
+    assert max(err) <= 1e-6 and perr <= 1e-5
+    assert np.all(log[:, 1] <= 1e-8)
+
+
 def test_single_timestep_drop_in(mp_lib):
     """FRACTIONAL_STEP_1::single_timestep_2d with the reference's argument order."""
     cl = clouds.cavity_2d(24, seed=8)
