@@ -15,6 +15,11 @@ template <> struct V2t<float> { using type = float2; };
 
 constexpr double EPS2 = 2.220446049250313e-16 * 2.220446049250313e-16;
 constexpr int KT = 256;  // threads per block in all Krylov kernels (8 slices)
+// resident blocks per SM the kernels are compiled for (32 registers): the fused
+// SpMV + reduction kernels wait on memory; at 48 registers and 4 blocks per SM
+// they ran at 42 % warps active and 40 % of DRAM bandwidth (k_spmv_omega 62 us at
+// 1M rows; 6 blocks: 50 us; 8 blocks: 46 us)
+constexpr int KT_BLOCKS = 8;
 
 __device__ __forceinline__ int gwarp() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
 
@@ -54,7 +59,7 @@ struct RedBuf {
 // ---------------------------------------------------------------- init
 // r = b - A x, r0 = r, p = v = 0, scalars of Eigen's BiCGSTAB prologue.
 template <class T, bool ZERO_X>
-__global__ void __launch_bounds__(KT)
+__global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_init(EllView<T> A, int bordered, const T *x, const T *b, T *r, T *r0, T *p, T *v,
            BicgScalars *S, RedBuf R, double tol, int maxit, cudaGraphConditionalHandle h) {
     KRYLOV_SMEM
@@ -127,7 +132,7 @@ __global__ void __launch_bounds__(KT)
 // the border row of A f is sum f_i).  One pass over the operator for both
 // products; the last block stores theta.  (Minimising the residual restricted
 // to the first multigrid level instead gave more iterations at 1M nodes.)
-__global__ void __launch_bounds__(KT)
+__global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_guess_mr(EllView<double> A, int bordered, const double *x, const double *b,
                const double *f, BicgScalars *S, RedBuf R) {
     KRYLOV_SMEM
@@ -187,7 +192,7 @@ __global__ void k_guess_axpy(int nv, double *x, const double *f, const BicgScala
 
 // Eigen's restart: r = b - A x, r0 = r, rho = r0_sq = ||r||^2 (rare path)
 template <class T>
-__global__ void __launch_bounds__(KT)
+__global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_restart(EllView<T> A, int bordered, const T *x, const T *b, T *r, T *r0, BicgScalars *S,
               RedBuf R) {
     KRYLOV_SMEM
@@ -232,7 +237,7 @@ __global__ void __launch_bounds__(KT)
 
 // p = r + beta (p - omega v); y = M^-1 p for the fused preconditioners
 template <class T, int PK>
-__global__ void __launch_bounds__(KT)
+__global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_update_p(int nv, int bordered, const T *r, T *p, const T *v, T *y, const T *dinv,
                const BicgScalars *S) {
     if (S->done)
@@ -256,7 +261,7 @@ __global__ void __launch_bounds__(KT)
 
 // v = A y, alpha = rho / (r0 . v)
 template <class T>
-__global__ void __launch_bounds__(KT)
+__global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_spmv_alpha(EllView<T> A, int bordered, const T *y, T *v, const T *r0, BicgScalars *S,
                  RedBuf R) {
     KRYLOV_SMEM
@@ -296,7 +301,7 @@ __global__ void __launch_bounds__(KT)
 
 // s = r - alpha v; z = M^-1 s for the fused preconditioners
 template <class T, int PK>
-__global__ void __launch_bounds__(KT)
+__global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_update_s(int nv, int bordered, const T *r, const T *v, T *s, T *z, const T *dinv,
                const BicgScalars *S) {
     if (S->done)
@@ -319,7 +324,7 @@ __global__ void __launch_bounds__(KT)
 
 // t = A z, omega = (t . s) / (t . t)
 template <class T>
-__global__ void __launch_bounds__(KT)
+__global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_spmv_omega(EllView<T> A, int bordered, const T *z, T *t, const T *s, BicgScalars *S,
                  RedBuf R) {
     KRYLOV_SMEM
@@ -362,7 +367,7 @@ __global__ void __launch_bounds__(KT)
 
 // x += alpha y + omega z; r = s - omega t; convergence test for the next sweep
 template <class T>
-__global__ void __launch_bounds__(KT)
+__global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_update_xr(int nsys, T *x, const T *y, const T *z, const T *s, const T *t, T *r, const T *r0,
                 BicgScalars *S, RedBuf R, cudaGraphConditionalHandle h) {
     KRYLOV_SMEM
@@ -398,7 +403,7 @@ __global__ void __launch_bounds__(KT)
 
 // ||b - A x||^2 in FP64 (the residual solver.cpp:342-343 logs); zero x when
 // ||b|| = 0 as Eigen's BiCGSTAB does.  Optionally stores r64 = b - A x.
-__global__ void __launch_bounds__(KT)
+__global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_true_residual(EllView<double> A, int bordered, double *x, const double *b, double *r64,
                     BicgScalars *S, RedBuf R, int refine, cudaGraphConditionalHandle h) {
     KRYLOV_SMEM
@@ -545,14 +550,14 @@ __global__ void k_assemble_ppe(int nv, int K, int dim, const int *cols, const do
 // ------------------------------------------------------------ host side
 static unsigned vec_blocks(int n) {
     int b = (n + KT - 1) / KT;
-    int cap = sm_count() * 4;
+    int cap = sm_count() * KT_BLOCKS;
     return (unsigned)(b < cap ? (b < 1 ? 1 : b) : cap);
 }
-// reduction kernels walk the slices with a grid of a few blocks per SM, so the
-// last-block ticket sees few atomics
+// reduction kernels walk the slices with a grid of KT_BLOCKS blocks per SM (all
+// resident at once), so the last-block ticket sees a bounded number of atomics
 static unsigned slice_blocks(int nv) {
     int ns = (nv + SLICE - 1) / SLICE;
-    int b = (ns + 7) / 8, cap = sm_count() * 4;
+    int b = (ns + 7) / 8, cap = sm_count() * KT_BLOCKS;
     return (unsigned)(b < cap ? b : cap);
 }
 
