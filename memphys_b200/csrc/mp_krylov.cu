@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
 // the border row of A f is sum f_i).  One pass over the operator for both
 // products; the last block stores theta.  (Minimising the residual restricted
 // to the first multigrid level instead gave more iterations at 1M nodes.)
-__global__ void __launch_bounds__(KT, KT_BLOCKS)
+__global__ void __launch_bounds__(KT, 4)  // two operator streams + 4 sums: 64 registers
     k_guess_mr(EllView<double> A, int bordered, const double *x, const double *b,
                const double *f, BicgScalars *S, RedBuf R) {
     KRYLOV_SMEM

@@ -36,6 +36,7 @@ struct Mlp {
     // per-node features and outputs of the field prediction (sized to the cloud)
     dbuf<uint16_t> fx;
     dbuf<float> fy;
+    dbuf<float4> fq;  // per node: the three scaled fields the features gather
 };
 
 // ------------------------------------------------------------ layout helpers
@@ -94,18 +95,23 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
     return false;
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-    uint32_t r[16];
+// 32 consecutive accumulator columns of this thread's row; one wait per 32
+// columns keeps the tensor-memory latency off the epilogue's critical path
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-        "%11, %12, %13, %14, %15}, [%16];\n"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+        "%28, %29, %30, %31}, [%32];\n"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-          "=r"(r[14]), "=r"(r[15])
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 16; i++)
+    for (int i = 0; i < 32; i++)
         v[i] = __uint_as_float(r[i]);
 }
 
@@ -135,74 +141,99 @@ struct MlpFwdArgs {
     int *err;
 };
 
+// Four warpgroups per CTA work on four tiles at once, each with its own operand
+// staging buffer, mbarrier and 128 accumulator columns of tensor memory (all
+// 512 columns): while some groups run their epilogues (TMEM -> registers ->
+// BF16 in shared memory) the tensor core runs the others' MMAs.  The weights
+// are shared.  A group's buffer holds its feature tile (K = 64) for layer 1,
+// then each hidden activation (K = 128) once the MMA that read it completed.
+constexpr int MLP_WG = 4;
+
 struct MlpSmem {
     uint16_t w1[MLP_H * MLP_IN];
     uint16_t w2[MLP_H * MLP_H];
     uint16_t w3[MLP_H * MLP_H];
-    uint16_t xa[MLP_TILE * MLP_IN];
-    uint16_t ha[MLP_TILE * MLP_H];
+    uint16_t buf[MLP_WG][MLP_TILE * MLP_H];
     float bias[3][MLP_H];
     float w4[MLP_H];
-    uint64_t mbar;
+    uint64_t mbar[MLP_WG];
     uint32_t tmem;
 };
 
+// barrier of one warpgroup (named barrier 1 + wg; 0 is __syncthreads)
+__device__ __forceinline__ void wg_sync(int wg) {
+    asm volatile("bar.sync %0, 128;\n" ::"r"(1 + wg) : "memory");
+}
+
 template <int MODE>
-__global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpFwdArgs A) {
+__global__ void __launch_bounds__(128 * MLP_WG, 1) k_mlp_forward(MlpFwdArgs A) {
     extern __shared__ __align__(1024) unsigned char mlp_smem_raw[];
     MlpSmem &S = *reinterpret_cast<MlpSmem *>(mlp_smem_raw);
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int warp = threadIdx.x >> 5, wg = threadIdx.x >> 7, tid = threadIdx.x & 127;
     // weights (already in operand layout) and vectors into shared memory
     {
         const uint4 *src = reinterpret_cast<const uint4 *>(A.pack);
         uint4 *dst = reinterpret_cast<uint4 *>(S.w1);  // w1, w2, w3 are contiguous
-        for (int i = tid; i < MLP_PACK / 8; i += blockDim.x)
+        for (int i = threadIdx.x; i < MLP_PACK / 8; i += blockDim.x)
             dst[i] = src[i];
-        for (int i = tid; i < MLP_H; i += blockDim.x) {
+        for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
             S.bias[0][i] = A.theta[MLP_OFF_B1 + i];
             S.bias[1][i] = A.theta[MLP_OFF_B2 + i];
             S.bias[2][i] = A.theta[MLP_OFF_B3 + i];
             S.w4[i] = A.theta[MLP_OFF_W4 + i];
         }
     }
-    if (tid == 0)
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&S.mbar)));
+    if (threadIdx.x == 0)
+        for (int g = 0; g < MLP_WG; g++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&S.mbar[g])));
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                          smem_u32(&S.tmem)),
-                     "r"(MLP_H));
+                     "r"(MLP_H * MLP_WG));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    const uint32_t tmem = S.tmem;
-    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    // this group's accumulator columns; warp w reads TMEM lanes 32 (w % 4) ..
+    const uint32_t tmem = S.tmem + (uint32_t)(wg * MLP_H);
+    const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    uint16_t *xa = S.buf[wg], *ha = S.buf[wg];
+    uint64_t *mbar = &S.mbar[wg];
     const float b4 = A.theta[MLP_OFF_B4];
     uint32_t phase = 0;
     bool ok = true;
     const int ntiles = (A.n + MLP_TILE - 1) / MLP_TILE;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int stride = gridDim.x * MLP_WG;
+    // this thread's 128-byte feature row of tile t (zeros past the end)
+    auto load_row = [&](int t, uint4 (&f)[MLP_IN / 8]) {
+        const int r = t * MLP_TILE + tid;
+        const bool lv = t < ntiles && r < A.n;
+        const int src = lv ? (A.idx ? A.idx[r] : r) : 0;
+        const uint4 *xr = reinterpret_cast<const uint4 *>(A.X + (size_t)src * MLP_IN);
+#pragma unroll
+        for (int c = 0; c < MLP_IN / 8; c++)
+            f[c] = lv ? xr[c] : make_uint4(0, 0, 0, 0);
+    };
+    uint4 feat[MLP_IN / 8];
+    load_row(blockIdx.x * MLP_WG + wg, feat);
+    for (int tile = blockIdx.x * MLP_WG + wg; tile < ntiles; tile += stride) {
         const int row = tile * MLP_TILE + tid;
         const bool live = row < A.n;
-        // ---- this thread's feature row into the A operand
-        {
-            const int src = live ? (A.idx ? A.idx[row] : row) : 0;
-            const uint4 *xr = reinterpret_cast<const uint4 *>(A.X + (size_t)src * MLP_IN);
+        // ---- this thread's feature row into the A operand; the next tile's row is
+        // loaded while this tile's MMAs and epilogues run
 #pragma unroll
-            for (int c = 0; c < MLP_IN; c += 8) {
-                uint4 v = live ? xr[c / 8] : make_uint4(0, 0, 0, 0);
-                *reinterpret_cast<uint4 *>(&S.xa[cm_off(tid, c, MLP_IN)]) = v;
-            }
-        }
+        for (int c = 0; c < MLP_IN / 8; c++)
+            *reinterpret_cast<uint4 *>(&xa[cm_off(tid, 8 * c, MLP_IN)]) = feat[c];
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-        __syncthreads();
+        wg_sync(wg);
+        load_row(tile + stride, feat);
         float out = b4;
         for (int layer = 0; layer < 3; layer++) {
             const int K = layer == 0 ? MLP_IN : MLP_H;
-            const uint16_t *Ab = layer == 0 ? S.xa : S.ha;
+            const uint16_t *Ab = layer == 0 ? xa : ha;
             const uint16_t *Bw = layer == 0 ? S.w1 : (layer == 1 ? S.w2 : S.w3);
             if (tid == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
@@ -211,29 +242,29 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpFwdArgs A) {
                     const uint32_t koff = (uint32_t)(k0 / 8) * 128u;
                     umma_bf16(tmem, umma_desc(a0 + koff, K), umma_desc(b0 + koff, K), k0 > 0);
                 }
-                umma_commit(&S.mbar);
+                umma_commit(mbar);
             }
-            if (!mbar_wait(&S.mbar, phase))
+            if (!mbar_wait(mbar, phase))
                 ok = false;
             phase ^= 1u;
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             // ---- epilogue: this thread's row of the accumulator
 #pragma unroll 1
-            for (int c0 = 0; c0 < MLP_H; c0 += 16) {
-                float v[16];
-                tmem_ld16(lane_addr + (uint32_t)c0, v);
+            for (int c0 = 0; c0 < MLP_H; c0 += 32) {
+                float v[32];
+                tmem_ld32(lane_addr + (uint32_t)c0, v);
 #pragma unroll
-                for (int i = 0; i < 16; i++)
+                for (int i = 0; i < 32; i++)
                     v[i] = fmaxf(v[i] + S.bias[layer][c0 + i], 0.f);
                 if (layer < 2) {
 #pragma unroll
-                    for (int h = 0; h < 16; h += 8) {
+                    for (int h = 0; h < 32; h += 8) {
                         uint4 q;
                         q.x = pack_bf16x2(v[h], v[h + 1]);
                         q.y = pack_bf16x2(v[h + 2], v[h + 3]);
                         q.z = pack_bf16x2(v[h + 4], v[h + 5]);
                         q.w = pack_bf16x2(v[h + 6], v[h + 7]);
-                        *reinterpret_cast<uint4 *>(&S.ha[cm_off(tid, c0 + h, MLP_H)]) = q;
+                        *reinterpret_cast<uint4 *>(&ha[cm_off(tid, c0 + h, MLP_H)]) = q;
                         if (MODE == MLP_MODE_TRAIN && live) {
                             uint16_t *hg = (layer == 0 ? A.h1 : A.h2) + (size_t)row * MLP_H + c0 + h;
                             *reinterpret_cast<uint4 *>(hg) = q;
@@ -241,26 +272,28 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpFwdArgs A) {
                     }
                 } else {
 #pragma unroll
-                    for (int i = 0; i < 16; i++)
+                    for (int i = 0; i < 32; i++)
                         out = fmaf(v[i], S.w4[c0 + i], out);
                     if (MODE == MLP_MODE_TRAIN && live) {
                         float4 *hg = reinterpret_cast<float4 *>(A.h3 + (size_t)row * MLP_H + c0);
 #pragma unroll
-                        for (int i = 0; i < 4; i++)
+                        for (int i = 0; i < 8; i++)
                             hg[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
                     }
                 }
             }
             asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-            __syncthreads();
+            wg_sync(wg);
         }
         if (live)
             A.y[row] = out;
     }
     __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(MLP_H));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(S.tmem),
+                     "r"(MLP_H * MLP_WG));
     if (!ok && tid == 0 && A.err)
         atomicExch(A.err, 1);
 }
@@ -428,11 +461,51 @@ __global__ void k_mlp_collect(MlpFields F, const int *idx, int nidx, const doubl
 }
 
 // features of every node (skipped while *step < 2: no pressure history)
-__global__ void __launch_bounds__(256) k_mlp_features(MlpFields F, uint16_t *X, const int *step) {
+// the three gathered fields of every node, scaled and rounded to FP32 once
+// (the same values node_features forms per gather), so that the feature kernel
+// fetches one 16-byte record per stencil member instead of four doubles
+__global__ void k_mlp_prep(MlpFields F, float4 *q, const int *step) {
     if (*step < 2)
         return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.nv; i += gridDim.x * blockDim.x)
-        node_features(F, i, X + (size_t)i * MLP_IN);
+    const double sb = F.norms[0], sp = F.norms[1];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < F.nv; j += gridDim.x * blockDim.x) {
+        const double pc = F.pcur[j], p1 = F.ph1[j];
+        q[j] = make_float4((float)(F.b[j] * sb), (float)((pc - p1) * sp),
+                           (float)((p1 - F.ph2[j]) * sp), 0.f);
+    }
+}
+
+// features of every node from the prepared records (skipped while *step < 2: no
+// pressure history)
+__global__ void __launch_bounds__(256)
+    k_mlp_features(MlpFields F, const float4 *__restrict__ q, uint16_t *X, const int *step) {
+    if (*step < 2)
+        return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.nv; i += gridDim.x * blockDim.x) {
+        float f[MLP_IN];
+        const size_t base = (size_t)(i / 64) * F.K * 64 + (i % 64);
+#pragma unroll
+        for (int k = 0; k < MLP_STENCIL; k++) {
+            const float4 v = __ldg(q + F.cols[base + (size_t)k * 64]);
+            f[3 * k] = v.x;
+            f[3 * k + 1] = v.y;
+            f[3 * k + 2] = v.z;
+        }
+        f[60] = F.hloc[i];
+        f[61] = F.bflag[i] ? 1.f : 0.f;
+        f[62] = 1.f;
+        f[63] = 0.f;
+        uint4 *dst = reinterpret_cast<uint4 *>(X + (size_t)i * MLP_IN);
+#pragma unroll
+        for (int c = 0; c < MLP_IN; c += 8) {
+            uint4 v;
+            v.x = pack_bf16x2(f[c], f[c + 1]);
+            v.y = pack_bf16x2(f[c + 2], f[c + 3]);
+            v.z = pack_bf16x2(f[c + 4], f[c + 5]);
+            v.w = pack_bf16x2(f[c + 6], f[c + 7]);
+            dst[c / 8] = v;
+        }
+    }
 }
 
 // The prediction as a pressure correction: the clamped output (8 units: the
@@ -468,8 +541,8 @@ template <int MODE> static int launch_forward(MlpFwdArgs &a, cudaStream_t s) {
     const int sm = fwd_smem();
     MP_CUDA(cudaFuncSetAttribute(k_mlp_forward<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     const int tiles = (a.n + MLP_TILE - 1) / MLP_TILE;
-    const int grid = std::max(1, std::min(tiles, sm_count()));
-    k_mlp_forward<MODE><<<grid, 128, sm, s>>>(a);
+    const int grid = std::max(1, std::min((tiles + MLP_WG - 1) / MLP_WG, sm_count()));
+    k_mlp_forward<MODE><<<grid, 128 * MLP_WG, sm, s>>>(a);
     MP_CHECK_LAUNCH();
     return MP_OK;
 }
@@ -531,7 +604,9 @@ int mlp_predict_fields(Mlp &m, const MlpFields &F, double *x, double *corr, cons
     if ((size_t)F.nv > m.fy.n)
         return fail(MP_BAD_ARG, "field prediction for %d nodes: %zu reserved", F.nv, m.fy.n);
     const unsigned g = (unsigned)std::min((F.nv + 255) / 256, sm_count() * 16);
-    k_mlp_features<<<g, 256, 0, s>>>(F, m.fx.p, step);
+    k_mlp_prep<<<g, 256, 0, s>>>(F, m.fq.p, step);
+    MP_CHECK_LAUNCH();
+    k_mlp_features<<<g, 256, 0, s>>>(F, m.fq.p, m.fx.p, step);
     MP_CHECK_LAUNCH();
     MlpFwdArgs a{};
     a.n = F.nv;
@@ -551,6 +626,7 @@ int mlp_reserve_fields(Mlp &m, int nv) {
         return MP_OK;
     MP_TRY(m.fx.alloc((size_t)nv * MLP_IN));
     MP_TRY(m.fy.alloc(nv));
+    MP_TRY(m.fq.alloc(nv));
     MP_CUDA(cudaMemset(m.fx.p, 0, m.fx.bytes()));
     return MP_OK;
 }
