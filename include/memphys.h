@@ -196,9 +196,9 @@ typedef struct {
     int guess;         /* MP_GUESS_* */
     double inner_tol;  /* mixed precision: relative reduction per refinement sweep */
     int amg_max_levels;
-    int amg_coarse_size;
-    int smoother_sweeps;
-    double smoother_omega;
+    int amg_coarse_size;  /* levels stop at or below this size; the coarsest is inverted densely */
+    int smoother_sweeps;  /* degree-2 Chebyshev applications before and after each coarse correction */
+    double cheb_lower;    /* Chebyshev interval [cheb_lower * lambda_max, 1.1 lambda_max] of D^-1 A */
 } mp_solver_cfg;
 
 /* sensible defaults for the fields above */

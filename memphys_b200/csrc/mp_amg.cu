@@ -446,7 +446,8 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
     const bool mixed = store == AMG_F32;
     Amg *a = new Amg;
     a->store = store;
-    a->cheb_ratio = 12.0;
+    a->cheb_ratio = 1.0 / cfg.cheb_lower;
+    a->sweeps = std::max(1, cfg.smoother_sweeps);
     Csr A;
     int rc = csr_from_ell(A0, A);
     if (rc != MP_OK) {
@@ -729,6 +730,8 @@ template <class T, class V, bool DIFF, int EP>
 __global__ void __launch_bounds__(256, 8)
     k_level(EllView<V> M, const T *__restrict__ u, const T *__restrict__ b,
             const T *__restrict__ dinv, T *d, T *x, T *y, ChebC c, const int *done) {
+    pdl_wait();
+    pdl_trigger();
     if (*done)
         return;
     const int w = gwarp_a(), lane = threadIdx.x & 31;
@@ -749,6 +752,8 @@ template <class T, class V, int G, bool DIFF, int EP>
 __global__ void __launch_bounds__(256)
     k_level_csr(CsrView<V> M, const T *__restrict__ u, const T *__restrict__ b,
                 const T *__restrict__ dinv, T *d, T *x, T *y, ChebC c, const int *done) {
+    pdl_wait();
+    pdl_trigger();
     if (*done)
         return;
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -780,6 +785,8 @@ __global__ void __launch_bounds__(256)
 // d = dinv b / theta (start of the pre-smoother from a zero guess)
 template <class T>
 __global__ void k_cheb_start(int n, const T *b, const T *dinv, T *d, T inv_theta, const int *done) {
+    pdl_wait();
+    pdl_trigger();
     if (*done)
         return;
     const int stride = gridDim.x * blockDim.x;
@@ -791,6 +798,8 @@ __global__ void k_cheb_start(int n, const T *b, const T *dinv, T *d, T inv_theta
 template <class T>
 __global__ void k_coarse(int nc, const T *__restrict__ cinv, const T *__restrict__ b, T *x,
                          const int *done) {
+    pdl_wait();
+    pdl_trigger();
     if (*done)
         return;
     const int row = gwarp_a(), lane = threadIdx.x & 31;
@@ -871,13 +880,17 @@ static int level_op(int mode, const EllView<V> &E, const CsrView<V> &Cv, const T
                     const T *dinv, T *d, T *x, T *y, const ChebC &c, const int *done,
                     cudaStream_t s) {
     const int n = E.nrows;
+    const dim3 blk(256);
+    cudaError_t e;
     switch (mode) {
-    case 0: k_level<T, V, DIFF, EP><<<sblocks(n), 256, 0, s>>>(E, u, b, dinv, d, x, y, c, done); break;
-    case 1: k_level_csr<T, V, 4, DIFF, EP><<<(unsigned)((n * 4 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
-    case 2: k_level_csr<T, V, 8, DIFF, EP><<<(unsigned)((n * 8 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
-    case 3: k_level_csr<T, V, 16, DIFF, EP><<<(unsigned)((n * 16 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
-    default: k_level_csr<T, V, 32, DIFF, EP><<<(unsigned)(((size_t)n * 32 + 255) / 256), 256, 0, s>>>(Cv, u, b, dinv, d, x, y, c, done); break;
+    case 0: e = launch_pdl(k_level<T, V, DIFF, EP>, dim3(sblocks(n)), blk, s, E, u, b, dinv, d, x, y, c, done); break;
+    case 1: e = launch_pdl(k_level_csr<T, V, 4, DIFF, EP>, dim3((unsigned)((n * 4 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
+    case 2: e = launch_pdl(k_level_csr<T, V, 8, DIFF, EP>, dim3((unsigned)((n * 8 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
+    case 3: e = launch_pdl(k_level_csr<T, V, 16, DIFF, EP>, dim3((unsigned)((n * 16 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
+    default: e = launch_pdl(k_level_csr<T, V, 32, DIFF, EP>, dim3((unsigned)(((size_t)n * 32 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
     }
+    if (e != cudaSuccess)
+        return fail(MP_CUDA_ERROR, "multigrid launch: %s", cudaGetErrorString(e));
     MP_CHECK_LAUNCH();
     return MP_OK;
 }
@@ -889,7 +902,10 @@ static int vcycle(const Amg &a, size_t l, const T *b, T *x, const int *done, cud
     using LO = LvlOps<V, DIFF>;
     AmgLevel &L = *a.L[l];
     if (l + 1 == a.L.size()) {
-        k_coarse<T><<<(unsigned)((a.nc + 7) / 8), 256, 0, s>>>(a.nc, LV::cinv(a), b, x, done);
+        const cudaError_t e = launch_pdl(k_coarse<T>, dim3((unsigned)((a.nc + 7) / 8)), dim3(256), s,
+                                         a.nc, LV::cinv(a), b, x, done);
+        if (e != cudaSuccess)
+            return fail(MP_CUDA_ERROR, "multigrid launch: %s", cudaGetErrorString(e));
         MP_CHECK_LAUNCH();
         return MP_OK;
     }
@@ -901,17 +917,26 @@ static int vcycle(const Amg &a, size_t l, const T *b, T *x, const int *done, cud
     T *d = LV::d(L), *r = LV::r(L);
     const unsigned vb = (unsigned)std::min((L.n + 255) / 256, sm_count() * 8);
     const int mA = l == 0 ? 0 : L.sA.mode;
-    k_cheb_start<T><<<vb, 256, 0, s>>>(L.n, b, dinv, d, (T)c.inv_theta, done);
+    const cudaError_t e = launch_pdl(k_cheb_start<T>, dim3(vb), dim3(256), s, L.n, b, dinv, d,
+                                     (T)c.inv_theta, done);
+    if (e != cudaSuccess)
+        return fail(MP_CUDA_ERROR, "multigrid launch: %s", cudaGetErrorString(e));
     MP_CHECK_LAUNCH();
     MP_TRY((level_op<T, V, DIFF, EP_CHEB_PRE>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
+    for (int k = 1; k < a.sweeps; k++) {  // further pre-smoothing from the current x
+        MP_TRY((level_op<T, V, DIFF, EP_CHEB_POST1>(mA, A, Ac, x, b, dinv, d, x, nullptr, c, done, s)));
+        MP_TRY((level_op<T, V, DIFF, EP_CHEB_POST2>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
+    }
     MP_TRY((level_op<T, V, DIFF, EP_RESID>(mA, A, Ac, x, b, dinv, d, x, r, c, done, s)));
     MP_TRY((level_op<T, V, false, EP_PLAIN>(L.sR.mode, LO::R(L), Rc, r, nullptr, nullptr, nullptr,
                                             nullptr, LV::b(N), c, done, s)));
     MP_TRY((vcycle<T, V, DIFF>(a, l + 1, LV::b(N), LV::x(N), done, s)));
     MP_TRY((level_op<T, V, false, EP_PROLONG>(L.sP.mode, LO::P(L), Pc, LV::x(N), nullptr, nullptr,
                                               nullptr, x, nullptr, c, done, s)));
-    MP_TRY((level_op<T, V, DIFF, EP_CHEB_POST1>(mA, A, Ac, x, b, dinv, d, x, nullptr, c, done, s)));
-    MP_TRY((level_op<T, V, DIFF, EP_CHEB_POST2>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
+    for (int k = 0; k < a.sweeps; k++) {
+        MP_TRY((level_op<T, V, DIFF, EP_CHEB_POST1>(mA, A, Ac, x, b, dinv, d, x, nullptr, c, done, s)));
+        MP_TRY((level_op<T, V, DIFF, EP_CHEB_POST2>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
+    }
     return MP_OK;
 }
 

@@ -73,6 +73,7 @@ struct Amg {
     double setup_seconds = 0;
     int store = AMG_F64;
     double cheb_ratio = 12.0;         // Chebyshev smoothing on [lmax / ratio, lmax]
+    int sweeps = 1;                   // degree-2 Chebyshev applications per side
     dbuf<int> zero_flag;              // a device 0 used as `done` while autotuning
     ~Amg();
 };

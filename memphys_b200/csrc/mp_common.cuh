@@ -27,6 +27,33 @@ void count_launch(int n = 1);
                               cudaGetErrorString(e_), __FILE__, __LINE__);                   \
     } while (0)
 
+// Programmatic dependent launch (sm_90+): a kernel launched by launch_pdl may be
+// scheduled while its predecessor in the stream is still draining, so its launch
+// latency overlaps the predecessor's tail.  Such a kernel calls pdl_wait() before
+// touching anything the predecessor wrote (it returns once that grid has
+// completed and its writes are visible), and pdl_trigger() to let its own
+// successor launch once all of its blocks are resident.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
+template <class... KArgs, class... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
+                              Args... args) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 #define MP_CHECK_LAUNCH()                                                                    \
     do {                                                                                     \
         cudaError_t e_ = cudaGetLastError();                                                 \

@@ -917,7 +917,7 @@ Cfg Cfg::from(const mp_solver_cfg &c) {
     o.amg_max_levels = c.amg_max_levels > 0 ? c.amg_max_levels : 12;
     o.amg_coarse_size = c.amg_coarse_size > 0 ? c.amg_coarse_size : 512;
     o.smoother_sweeps = c.smoother_sweeps > 0 ? c.smoother_sweeps : 1;
-    o.smoother_omega = c.smoother_omega > 0 ? c.smoother_omega : 0.7;
+    o.cheb_lower = c.cheb_lower > 0 && c.cheb_lower < 1 ? c.cheb_lower : 1.0 / 12.0;
     return o;
 }
 
@@ -937,7 +937,7 @@ extern "C" int mp_solver_cfg_default(mp_solver_cfg *c) {
     c->amg_max_levels = 12;
     c->amg_coarse_size = 512;
     c->smoother_sweeps = 1;
-    c->smoother_omega = 0.7;
+    c->cheb_lower = 1.0 / 12.0;
     return MP_OK;
 }
 

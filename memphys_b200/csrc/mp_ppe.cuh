@@ -8,7 +8,7 @@ struct mp_cloud_s;
 namespace mp {
 
 struct Cfg {
-    double tol, inner_tol, smoother_omega;
+    double tol, inner_tol, cheb_lower;
     int maxit, precond, precision, guess, max_refine, amg_max_levels, amg_coarse_size,
         smoother_sweeps;
     static Cfg from(const mp_solver_cfg &c);
