@@ -125,7 +125,7 @@ __device__ __forceinline__ float bf16_round(float a) {
 }
 
 // ---------------------------------------------------------- forward kernel
-enum { MLP_MODE_ROWS = 1, MLP_MODE_TRAIN = 2 };
+enum { MLP_MODE_ROWS = 1, MLP_MODE_TRAIN = 2 };  // (template argument: k_mlp_forward<1> is the row forward)
 
 struct MlpFwdArgs {
     int n;                   // rows

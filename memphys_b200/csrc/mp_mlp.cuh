@@ -1,5 +1,6 @@
-// mp_mlp.cuh -- the per-node network that predicts the pressure increment of a
-// fractional step from its stencil neighbourhood (the learned initial guess).
+// mp_mlp.cuh -- the per-node network that predicts, from a node's stencil
+// neighbourhood, how a fractional step's pressure increment departs from linear
+// extrapolation (the learned initial guess).
 //
 //   input  64 features: for the node's first 20 stencil members, the new
 //          pressure right-hand side b^{n+1} and the last two pressure
@@ -11,9 +12,11 @@
 //          layer stays FP32 for the output dot product
 //   output the correction to the linear extrapolation,
 //          (p^{n+1} - p^n) - (p^n - p^{n-1}), divided by the RMS over the cloud of
-//          the last second difference (p^n - p^{n-1}) - (p^{n-1} - p^{n-2}); the
-//          guess is 2 p^n - p^{n-1} plus the scaled prediction, so the network's
-//          pointwise error scales with the (small) correction, not the increment
+//          the last second difference (p^n - p^{n-1}) - (p^{n-1} - p^{n-2}), so
+//          the network's pointwise error scales with the (small) correction,
+//          not the increment; the fractional step adds the scaled prediction to
+//          2 p^n - p^{n-1} after a coarse-level low-pass filter and with the
+//          weight that minimises the guess's residual (mp_fs1.cu)
 //
 // The three hidden layers run on the 5th-generation tensor cores
 // (tcgen05.mma, accumulators in tensor memory); training runs on the GPU with
