@@ -763,12 +763,14 @@ __global__ void __launch_bounds__(256)
         const int b0 = M.rp[row], e = M.rp[row + 1];
         const T ui = DIFF ? __ldg(u + row) : T(0);
         if (M.pk) {  // (column, FP32 value) pairs: one 8-byte load per entry
+#pragma unroll 4
             for (int t = b0 + li; t < e; t += G) {
                 const int2 q = __ldcs(M.pk + t);
                 const T ut = __ldg(u + q.x);
                 acc = fma((T)__int_as_float(q.y), (DIFF && t != b0) ? ut - ui : ut, acc);
             }
         } else {
+#pragma unroll 4
             for (int t = b0 + li; t < e; t += G) {
                 const T ut = __ldg(u + __ldcs(M.ci + t));
                 acc = fma((T)__ldcs(M.v + t), (DIFF && t != b0) ? ut - ui : ut, acc);
@@ -1018,11 +1020,13 @@ int amg_filter(const Amg &a, const double *c, double *work1, const double *scale
 // For each level operator and transfer, time y = M u with every schedule
 // (sliced ELL, CSR with 4/8/16/32 lanes per row) in the precision and form the
 // cycle will run (FP64; FP32; FP32 difference form for the MG32 level
-// operators), as bursts of launches so that launch jitter does not decide, and
-// keep the fastest.
+// operators) and keep the fastest.  Each timed launch starts with L2 flushed
+// (a write larger than L2), as inside the cycle, where the finer levels'
+// traffic evicts a coarse operator between its uses; an operator timed warm
+// from L2 ranks the schedules differently.  The median of five launches decides.
 template <class T, class V, bool DIFF>
 static int tune_one(const EllView<V> &E, const CsrView<V> &Cv, int ncols, bool allow_sell,
-                    OpSched &out, const int *zero, cudaStream_t s) {
+                    OpSched &out, const int *zero, dbuf<char> &flush, cudaStream_t s) {
     const int n = Cv.nrows;
     if (!n) {
         out.mode = 0;
@@ -1037,27 +1041,26 @@ static int tune_one(const EllView<V> &E, const CsrView<V> &Cv, int ncols, bool a
     MP_CUDA(cudaEventCreate(&e1));
     const ChebC c{};
     const bool sell = allow_sell && (E.vals || E.pk);
-    constexpr int BURST = 20;
+    constexpr int REPS = 5;
     float best = 1e30f;
     int rc = MP_OK;
     for (int mode = sell ? 0 : 1; mode <= 4 && rc == MP_OK; mode++) {
-        float ms_best = 1e30f;
-        for (int rep = 0; rep < 4 && rc == MP_OK; rep++) {
+        float t[REPS];
+        for (int rep = 0; rep < REPS && rc == MP_OK; rep++) {
+            cudaMemsetAsync(flush.p, rep & 0xff, flush.n, s);
             cudaEventRecord(e0, s);
-            for (int q = 0; q < BURST && rc == MP_OK; q++)
-                rc = level_op<T, V, DIFF, EP_PLAIN>(mode, E, Cv, u.p, nullptr, nullptr, nullptr,
-                                                    nullptr, y.p, c, zero, s);
+            rc = level_op<T, V, DIFF, EP_PLAIN>(mode, E, Cv, u.p, nullptr, nullptr, nullptr,
+                                                nullptr, y.p, c, zero, s);
             cudaEventRecord(e1, s);
             cudaEventSynchronize(e1);
-            float ms = 0;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (rep > 0 && ms < ms_best)  // the first burst warms up
-                ms_best = ms;
+            t[rep] = 0;
+            cudaEventElapsedTime(&t[rep], e0, e1);
         }
-        ms_best /= BURST;
-        out.us[mode] = ms_best * 1e3f;
-        if (ms_best < best) {
-            best = ms_best;
+        std::sort(t, t + REPS);
+        const float ms = t[REPS / 2];
+        out.us[mode] = ms * 1e3f;
+        if (ms < best) {
+            best = ms;
             out.mode = mode;
         }
     }
@@ -1070,12 +1073,14 @@ template <class T, class V, bool DIFF> static int tune_levels(Amg &a, cudaStream
     using LO = LvlOps<V, DIFF>;
     using LT = LvlOps<V, false>;
     const int *z = a.zero_flag.p;
+    dbuf<char> flush;  // larger than the 126 MB L2
+    MP_TRY(flush.alloc((size_t)192 << 20));
     for (size_t l = 0; l + 1 < a.L.size(); l++) {
         AmgLevel &L = *a.L[l];
         if (l > 0)
-            MP_TRY((tune_one<T, V, DIFF>(LO::A(L), LO::Ac(L), L.n, true, L.sA, z, s)));
-        MP_TRY((tune_one<T, V, false>(LT::P(L), LT::Pc(L), a.L[l + 1]->n, true, L.sP, z, s)));
-        MP_TRY((tune_one<T, V, false>(LT::R(L), LT::Rc(L), L.n, true, L.sR, z, s)));
+            MP_TRY((tune_one<T, V, DIFF>(LO::A(L), LO::Ac(L), L.n, true, L.sA, z, flush, s)));
+        MP_TRY((tune_one<T, V, false>(LT::P(L), LT::Pc(L), a.L[l + 1]->n, true, L.sP, z, flush, s)));
+        MP_TRY((tune_one<T, V, false>(LT::R(L), LT::Rc(L), L.n, true, L.sR, z, flush, s)));
     }
     return MP_OK;
 }
