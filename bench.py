@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--samples", type=int, default=16384,
                     help="nodes whose features and solved increments are recorded per step")
     ap.add_argument("--epochs", type=int, default=10)
+    ap.add_argument("--batched", type=int, default=4_000_000,
+                    help="independent uneven stencil systems per dimension in the batched "
+                         "weights measurement (0 skips it)")
     ap.add_argument("--inner-tol", type=float, default=1e-5,
                     help="mixed precision: relative reduction of each FP32 refinement solve")
     ap.add_argument("--profile", default=None, choices=["steps", "spmv", "stencil"],
@@ -361,7 +364,55 @@ def run_ours(args, ws, rank, local, pg):
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(cl, cld)
+    if args.batched > 0:
+        out["batched_stencils"] = batched_stencils(args.batched)
     return out
+
+
+def batched_stencils(nsys: int):
+    """The batched uneven stencil workload: nsys independent augmented PHS r^3 +
+    degree-3 systems per dimension, n from {20, 30, 40} for interior stencils and 60
+    for the 10 % marked boundary, offsets uniform in the unit ball scaled by h in
+    [1e-3, 1e-2]; one mp_stencil_weights_batched call on device arrays, timed by
+    wall clock around the (synchronous) call.  (The weights of this workload are
+    checked against per-stencil LAPACK in tests/test_gpu_parity.py.)
+    FLOPs count the useful FMAs of Gauss-Jordan on the s x (s + dim + 1) system."""
+    from memphys_b200 import capi
+    L = capi.lib()
+    res = {}
+    for dim, m in ((2, 10), (3, 20)):
+        rng = np.random.default_rng(20261203 + dim)
+        bnd = rng.random(nsys) < 0.1
+        sizes = np.where(bnd, 60, rng.choice([20, 30, 40], size=nsys)).astype(np.int32)
+        off = np.zeros(nsys, np.int64)
+        off[1:] = np.cumsum(sizes[:-1], dtype=np.int64)
+        total = int(sizes.sum(dtype=np.int64))
+        pts = rng.normal(size=(total, dim))
+        pts /= np.linalg.norm(pts, axis=1, keepdims=True)
+        pts *= rng.random((total, 1)) ** (1.0 / dim)
+        pts *= np.repeat(rng.uniform(1e-3, 1e-2, nsys), sizes)[:, None]
+        pts[off] = 0.0  # the centre node first
+        d_sizes = capi.DeviceArray.from_host(sizes)
+        d_off = capi.DeviceArray.from_host(off)
+        d_pts = capi.DeviceArray.from_host(np.ascontiguousarray(pts))
+        d_w = capi.DeviceArray(((dim + 1) * total,))
+        del pts
+
+        def call():
+            capi.check(L.mp_stencil_weights_batched(nsys, capi.ptr(d_sizes), capi.ptr(d_off),
+                                                    capi.ptr(d_pts), dim, 3, 3, capi.ptr(d_w),
+                                                    None, None), "mp_stencil_weights_batched")
+        call()  # warm-up (first-use set-up of the kernels)
+        t0 = time.time()
+        call()
+        secs = time.time() - t0
+        s_ = sizes.astype(np.float64) + m
+        fmas = float(np.sum(s_ * (s_ + dim + 1) * (s_ - 1)))
+        res[f"{dim}d"] = {"systems": nsys, "monomials": m, "seconds": round(secs, 4),
+                          "systems_per_s": round(nsys / secs),
+                          "gflops_fp64": round(2 * fmas / secs / 1e9, 1)}
+        del d_w, d_pts
+    return res
 
 
 def profile_range(args, cl, cld, make, fs, vel0, p0, stream):
