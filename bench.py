@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--batched", type=int, default=4_000_000,
                     help="independent uneven stencil systems per dimension in the batched "
                          "weights measurement (0 skips it)")
-    ap.add_argument("--inner-tol", type=float, default=1e-5,
+    ap.add_argument("--inner-tol", type=float, default=1e-3,
                     help="mixed precision: relative reduction of each FP32 refinement solve")
     ap.add_argument("--profile", default=None, choices=["steps", "spmv", "stencil"],
                     help="set up, warm up, then run `--steps` steps (SpMV launches, stencil-weight "
@@ -374,7 +374,7 @@ def batched_stencils(nsys: int):
     degree-3 systems per dimension, n from {20, 30, 40} for interior stencils and 60
     for the 10 % marked boundary, offsets uniform in the unit ball scaled by h in
     [1e-3, 1e-2]; one mp_stencil_weights_batched call on device arrays, timed by
-    wall clock around the (synchronous) call.  (The weights of this workload are
+    wall clock around the (synchronous) call, best of two.  (The weights of this workload are
     checked against per-stencil LAPACK in tests/test_gpu_parity.py.)
     FLOPs count the useful FMAs of Gauss-Jordan on the s x (s + dim + 1) system."""
     from memphys_b200 import capi
@@ -403,9 +403,11 @@ def batched_stencils(nsys: int):
                                                     capi.ptr(d_pts), dim, 3, 3, capi.ptr(d_w),
                                                     None, None), "mp_stencil_weights_batched")
         call()  # warm-up (first-use set-up of the kernels)
-        t0 = time.time()
-        call()
-        secs = time.time() - t0
+        secs = 1e30
+        for _ in range(2):  # the call includes host-side work: best of two
+            t0 = time.time()
+            call()
+            secs = min(secs, time.time() - t0)
         s_ = sizes.astype(np.float64) + m
         fmas = float(np.sum(s_ * (s_ + dim + 1) * (s_ - 1)))
         res[f"{dim}d"] = {"systems": nsys, "monomials": m, "seconds": round(secs, 4),

@@ -391,6 +391,23 @@ static int pack_pairs(const int *cols, const float *v, size_t n, dbuf<int2> &out
     return MP_OK;
 }
 
+int ell_diff32(const Ell &A0, dbuf<float> &v32, dbuf<int2> &pk, cudaStream_t s) {
+    MP_TRY(v32.alloc(A0.v64.n));
+    dbuf<int> bad;
+    MP_TRY(bad.alloc(1));
+    MP_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+    const int np = ell_padded_rows(A0.nrows);
+    k_diff_level0<<<(np + 255) / 256, 256, 0, s>>>(A0.view64(), v32.p, bad.p);
+    MP_CHECK_LAUNCH();
+    int hb = 0;
+    MP_CUDA(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    if (hb)
+        return fail(MP_BAD_ARG, "FP32 difference form needs every stencil row to start with its "
+                                "own node (%d rows do not)", hb);
+    return pack_pairs(A0.cols.p, v32.p, A0.v64.n, pk, s);
+}
+
 static int diff_level0(const Ell &A0, AmgLevel &L, cudaStream_t s) {
     const EllView<double> A = A0.view64();
     MP_TRY(L.Ad.v32.alloc(A0.v64.n));
@@ -470,13 +487,13 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
             L->borrowed = true;
             L->A64 = A0.view64();
             L->A32 = A0.view32();
-            if (store == AMG_MG32 && (rc = diff_level0(A0, *L, s)) != MP_OK)
+            if (store != AMG_F64 && (rc = diff_level0(A0, *L, s)) != MP_OK)
                 return bail(rc);
         } else {
             if ((rc = upload_ell(A, L->A, true, s)) != MP_OK || (rc = upload_csr(A, L->Ac, s)) != MP_OK)
                 return bail(rc);
             L->A64 = L->A.view64();
-            if (store == AMG_MG32 && (rc = diff_level(A, *L, s)) != MP_OK)
+            if (store != AMG_F64 && (rc = diff_level(A, *L, s)) != MP_OK)
                 return bail(rc);
         }
         if ((rc = L->dinv.alloc(A.n)) != MP_OK)
@@ -949,7 +966,7 @@ int amg_apply(const Amg &a, const T *in, T *out, const int *done, cudaStream_t s
             return vcycle<double, float, true>(a, 0, in, out, done, s);
         return vcycle<double, double, false>(a, 0, in, out, done, s);
     } else {
-        return vcycle<float, float, false>(a, 0, in, out, done, s);
+        return vcycle<float, float, true>(a, 0, in, out, done, s);
     }
 }
 template int amg_apply<double>(const Amg &, const double *, double *, const int *, cudaStream_t);
@@ -1091,7 +1108,7 @@ static int amg_autotune(Amg &a, cudaStream_t s) {
     if (a.store == AMG_MG32)
         return tune_levels<double, float, true>(a, s);
     if (a.store == AMG_F32)
-        return tune_levels<float, float, false>(a, s);
+        return tune_levels<float, float, true>(a, s);
     return tune_levels<double, double, false>(a, s);
 }
 

@@ -79,6 +79,9 @@ struct Amg {
 };
 
 int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t s);
+// FP32 difference-form copy of a stencil operator whose rows start with their own
+// node: the self slot holds the row sum, as (column, value bits) pairs in pk
+int ell_diff32(const Ell &A0, dbuf<float> &v32, dbuf<int2> &pk, cudaStream_t s);
 // Low-pass filter of a field through the first coarse level:
 //   out = P0 diag(scale1) R0 c,   scale1 = 1 / (R0 1)   (out may alias c)
 // (a locally weighted average onto the aggregates, interpolated back by the

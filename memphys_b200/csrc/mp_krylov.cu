@@ -33,6 +33,23 @@ __device__ __forceinline__ void ell_pair(const EllView<T> &A, int w, int lane,
     int K;
     slice_span(A, w, base, K);
     base += 2 * lane;
+    if constexpr (sizeof(T) == 4) {
+        if (A.pk) {  // FP32 difference form as (column, value) pairs; self entry = row sum
+            const int4 *P = reinterpret_cast<const int4 *>(A.pk + base);
+            int4 e = __ldcs(P);
+            xs0 = __ldg(x + e.x);
+            xs1 = __ldg(x + e.z);
+            a0 = __int_as_float(e.y) * xs0;
+            a1 = __int_as_float(e.w) * xs1;
+#pragma unroll 4
+            for (int k = 1; k < K; k++) {
+                e = __ldcs(P + (size_t)k * (SLICE / 2));
+                a0 = fma(__int_as_float(e.y), __ldg(x + e.x) - xs0, a0);
+                a1 = fma(__int_as_float(e.w), __ldg(x + e.z) - xs1, a1);
+            }
+            return;
+        }
+    }
     int2 c = __ldcs(reinterpret_cast<const int2 *>(A.cols + base));
     V2 v = __ldcs(reinterpret_cast<const V2 *>(A.vals + base));
     xs0 = __ldg(x + c.x);
@@ -132,13 +149,13 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
 // the border row of A f is sum f_i).  One pass over the operator for both
 // products; the last block stores theta.  (Minimising the residual restricted
 // to the first multigrid level instead gave more iterations at 1M nodes.)
-__global__ void __launch_bounds__(KT, 4)  // two operator streams + 4 sums: 64 registers
+__global__ void __launch_bounds__(KT, 4)  // two operator streams + 5 sums: 64 registers
     k_guess_mr(EllView<double> A, int bordered, const double *x, const double *b,
                const double *f, BicgScalars *S, RedBuf R) {
-    KRYLOV_SMEM
+    __shared__ double red_smem[32 * 5];
     const int nv = A.nrows, lane = threadIdx.x & 31, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int nsl = (nv + SLICE - 1) / SLICE;
-    double acc[4] = {0, 0, 0, 0};  // <r, Af>, <Af, Af>, sum x, sum f
+    double acc[5] = {0, 0, 0, 0, 0};  // <r, Af>, <Af, Af>, sum x, sum f, <r, r>
     const double xb = bordered ? x[nv] : 0.0;
     for (int w = gwarp(); w < nsl; w += nwarps) {
         size_t base;
@@ -170,17 +187,24 @@ __global__ void __launch_bounds__(KT, 4)  // two operator streams + 4 sums: 64 r
             acc[1] += af[q] * af[q];
             acc[2] += sx[q];
             acc[3] += sf[q];
+            acc[4] += r * r;
         }
     }
-    if (grid_reduce<4>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
-        double num = acc[0], den = acc[1];
+    if (grid_reduce<5>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
+        double num = acc[0], den = acc[1], rr = acc[4];
         if (bordered) {
             const double rn = b[nv] - acc[2];
             num += rn * acc[3];
             den += acc[3] * acc[3];
+            rr += rn * rn;
         }
-        const double th = den > 0 ? num / den : 0.0;
-        S->guess_theta = isfinite(th) ? th : 0.0;
+        // ||r - th A f||^2 = rr - num^2 / den: a correction that removes under 10 % of
+        // the squared residual is dropped (a small weight on a rough field helps the
+        // residual norm a little and the iteration count not at all)
+        double th = den > 0 ? num / den : 0.0;
+        if (!(den > 0 && num * num >= 0.1 * rr * den) || !isfinite(th))
+            th = 0.0;
+        S->guess_theta = th;
     }
 }
 
@@ -579,7 +603,7 @@ int Krylov::alloc(int nv_, int bordered_, bool mixed, bool external_pc) {
     size_t maxb = slice_blocks(nv);
     if (vec_blocks(nsys) > maxb)
         maxb = vec_blocks(nsys);
-    MP_TRY(partials.alloc(4 * maxb + 64));
+    MP_TRY(partials.alloc(5 * maxb + 64));  // up to 5 sums per block (learned-guess weight)
     MP_TRY(ticket.alloc(4));
     MP_TRY(scal.alloc(1));
     MP_CUDA(cudaMemset(ticket.p, 0, 4 * sizeof(unsigned int)));
@@ -661,14 +685,14 @@ int Ppe::issue_ir_inner_prologue(cudaGraphConditionalHandle h, cudaStream_t st) 
     MP_CHECK_LAUNCH();
     // inner solve of A e = b32 from e = 0; BiCGSTAB's prologue skips the SpMV
     k_init<float, true><<<slice_blocks(sys.nv), KT, 0, st>>>(
-        sys.A.view32(), sys.bordered, W.e32.p, W.b32.p, W.r32.p, W.r032.p, W.p32.p, W.v32.p,
+        sys.diff32(), sys.bordered, W.e32.p, W.b32.p, W.r32.p, W.r032.p, W.p32.p, W.v32.p,
         W.scal.p, RedBuf{W.partials.p, W.ticket.p}, cfg.inner_tol, cfg.maxit, h);
     MP_CHECK_LAUNCH();
     return MP_OK;
 }
 
 int Ppe::issue_ir_sweep(cudaGraphConditionalHandle h, cudaStream_t st) {
-    return issue_iteration<float>(sys, sys.A.view32(), sys.dinv32.p, W.e32.p, W.b32.p, W.r32.p,
+    return issue_iteration<float>(sys, sys.diff32(), sys.dinv32.p, W.e32.p, W.b32.p, W.r32.p,
                                   W.r032.p, W.p32.p, W.v32.p, W.s32.p, W.t32.p, W.y32.p, W.z32.p,
                                   W.scal.p, RedBuf{W.partials.p, W.ticket.p}, pk(), h, st);
 }
@@ -867,8 +891,10 @@ int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet
     if (hbad)
         return fail(MP_BAD_ARG, "%d stencils do not start with their own node", hbad);
     const bool mixed = cfg.precision == MP_FP32;  // FP32 Krylov + FP64 refinement
-    if (mixed)
+    if (mixed) {
         MP_TRY(ell_make_fp32(sys.A, st));
+        MP_TRY(ell_diff32(sys.A, sys.d32, sys.dpk, st));
+    }
     MP_TRY(sys.dinv.alloc(nv));
     if (mixed)
         MP_TRY(sys.dinv32.alloc(nv));
@@ -912,7 +938,7 @@ Cfg Cfg::from(const mp_solver_cfg &c) {
     o.precond = c.precond;
     o.precision = c.precision;
     o.guess = c.guess;
-    o.inner_tol = c.inner_tol > 0 ? c.inner_tol : 1e-5;
+    o.inner_tol = c.inner_tol > 0 ? c.inner_tol : 1e-3;
     o.max_refine = 12;
     o.amg_max_levels = c.amg_max_levels > 0 ? c.amg_max_levels : 12;
     o.amg_coarse_size = c.amg_coarse_size > 0 ? c.amg_coarse_size : 512;
@@ -933,7 +959,7 @@ extern "C" int mp_solver_cfg_default(mp_solver_cfg *c) {
     c->precond = MP_PRECOND_AMG;
     c->precision = MP_FP64;
     c->guess = MP_GUESS_PREVIOUS;
-    c->inner_tol = 1e-5;
+    c->inner_tol = 1e-3;
     c->amg_max_levels = 12;
     c->amg_coarse_size = 512;
     c->smoother_sweeps = 1;

@@ -38,6 +38,12 @@ struct PpeSystem {
     Ell A;                 // stencil rows, FP64 (+FP32 copy for mixed precision)
     dbuf<double> dinv;     // Jacobi: 1 / self coefficient
     dbuf<float> dinv32;
+    // FP32 Krylov: the operator in FP32 difference form, (column, value) pairs
+    dbuf<float> d32;
+    dbuf<int2> dpk;
+    EllView<float> diff32() const {
+        return EllView<float>{A.nrows, A.ncols, A.K, A.cols.p, d32.p, A.soff.p, dpk.p};
+    }
     Amg *amg = nullptr;
 };
 
