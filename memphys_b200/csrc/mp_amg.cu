@@ -1,6 +1,9 @@
 // mp_amg.cu -- smoothed-aggregation multigrid: host setup, GPU V-cycle.
 #include <algorithm>
 #include <chrono>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <type_traits>
 #include <cmath>
 #include <unordered_map>
@@ -1086,18 +1089,50 @@ static int tune_one(const EllView<V> &E, const CsrView<V> &Cv, int ncols, bool a
     return rc;
 }
 
+// Schedules already tuned in this process, keyed by the hierarchy's shape (device,
+// store, level, rows and entries of each operator): a second solver on the same
+// operator (another precision's twin, a restarted run) reuses them, so that both
+// sum in the same order and reproduce each other's iteration counts.
+struct TuneKey {
+    int dev, store, level, n, next;
+    size_t nnzA, nnzP, nnzR;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(dev, store, level, n, next, nnzA, nnzP, nnzR) <
+               std::tie(o.dev, o.store, o.level, o.n, o.next, o.nnzA, o.nnzP, o.nnzR);
+    }
+};
+struct TuneVal {
+    OpSched A, P, R;
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, TuneVal> g_tuned;
+
 template <class T, class V, bool DIFF> static int tune_levels(Amg &a, cudaStream_t s) {
     using LO = LvlOps<V, DIFF>;
     using LT = LvlOps<V, false>;
     const int *z = a.zero_flag.p;
-    dbuf<char> flush;  // larger than the 126 MB L2
-    MP_TRY(flush.alloc((size_t)192 << 20));
+    int dev = 0;
+    MP_CUDA(cudaGetDevice(&dev));
+    dbuf<char> flush;  // larger than the 126 MB L2; allocated on the first miss
+    std::lock_guard<std::mutex> lock(g_tune_mu);
     for (size_t l = 0; l + 1 < a.L.size(); l++) {
         AmgLevel &L = *a.L[l];
+        const TuneKey key{dev,          a.store,       (int)l,        L.n,          a.L[l + 1]->n,
+                          L.Ac.ci.n,    L.Pc.ci.n,     L.Rc.ci.n};
+        const auto hit = g_tuned.find(key);
+        if (hit != g_tuned.end()) {
+            L.sA = hit->second.A;
+            L.sP = hit->second.P;
+            L.sR = hit->second.R;
+            continue;
+        }
+        if (!flush.p)
+            MP_TRY(flush.alloc((size_t)192 << 20));
         if (l > 0)
             MP_TRY((tune_one<T, V, DIFF>(LO::A(L), LO::Ac(L), L.n, true, L.sA, z, flush, s)));
         MP_TRY((tune_one<T, V, false>(LT::P(L), LT::Pc(L), a.L[l + 1]->n, true, L.sP, z, flush, s)));
         MP_TRY((tune_one<T, V, false>(LT::R(L), LT::Rc(L), L.n, true, L.sR, z, flush, s)));
+        g_tuned[key] = TuneVal{L.sA, L.sP, L.sR};
     }
     return MP_OK;
 }
