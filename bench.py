@@ -15,8 +15,8 @@ runs `--warmup` untimed steps and `--steps` timed ones.
 
 Printed (rank 0, one JSON line): the plain FP64 ms/step as `value`
 (lower is better); the variants beside it (FP32 multigrid storage, FP32
-Krylov with FP64 refinement, extrapolated and learned initial guesses, and
-learned + FP32 multigrid as `learned_mixed`); the end-to-end ms/step through
+Krylov with FP64 refinement, extrapolated, projected and learned initial
+guesses, and learned + FP32 multigrid as `learned_mixed`); the end-to-end ms/step through
 mp_fs1_single_timestep with pinned host buffers; the SpMV roofline; and the
 CPU oracle baseline.
 
@@ -69,7 +69,8 @@ def parse():
                          "computations) inside a profiler capture range and exit (for ncu "
                          "--profile-from-start off)")
     ap.add_argument("--variant", default="plain",
-                    choices=["plain", "mg32", "extrapolated_mg32", "learned_mg32"],
+                    choices=["plain", "mg32", "extrapolated_mg32", "projected_mg32",
+                             "learned_mg32"],
                     help="solver configuration of --profile steps")
     return ap.parse_args()
 
@@ -290,6 +291,8 @@ def run_ours(args, ws, rank, local, pg):
         variants["learned_mg32"] = variant(guess=capi.MP_GUESS_LEARNED, precision=capi.MP_MG32)
         variants["extrapolated_mg32"] = variant(guess=capi.MP_GUESS_EXTRAPOLATE,
                                                 precision=capi.MP_MG32)
+        variants["projected_guess"] = variant(guess=capi.MP_GUESS_PROJECT)
+        variants["projected_mg32"] = variant(guess=capi.MP_GUESS_PROJECT, precision=capi.MP_MG32)
 
     # end to end through the C ABI drop-in with pinned host buffers
     u_h = capi.PinnedArray((nv,))
@@ -439,6 +442,8 @@ def profile_range(args, cl, cld, make, fs, vel0, p0, stream):
                 meshless.set_guess(fs, capi.MP_GUESS_LEARNED)
             elif args.variant == "extrapolated_mg32":
                 meshless.set_guess(fs, capi.MP_GUESS_EXTRAPOLATE)
+            elif args.variant == "projected_mg32":
+                meshless.set_guess(fs, capi.MP_GUESS_PROJECT)
         fs.set_state(vel0, p0, 0)
         fs.step(args.spinup + args.warmup, stream.handle)
         stream.sync()

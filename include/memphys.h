@@ -184,9 +184,14 @@ typedef struct mp_ppe_s *mp_ppe;
 enum { MP_PRECOND_NONE = 0, MP_PRECOND_JACOBI = 1, MP_PRECOND_AMG = 2 };
 /* initial guess of each fractional-step pressure solve: the previous pressure
  * (the reference's solveWithGuess(rhs, p_old)), zero, the linear extrapolation
- * 2 p^n - p^(n-1), or that extrapolation plus the learned network's predicted
- * correction */
-enum { MP_GUESS_PREVIOUS = 0, MP_GUESS_ZERO = 1, MP_GUESS_LEARNED = 2, MP_GUESS_EXTRAPOLATE = 3 };
+ * 2 p^n - p^(n-1), the projection p^n + sum_j c_j (p^(j+1) - p^j) over the last
+ * four increments with c minimising the guess's residual (Fischer's projection
+ * of successive right-hand sides; the increments' images are the differences of
+ * successive right-hand sides, so it costs no extra matrix product), or that
+ * projection plus the learned network's predicted correction, weighted to
+ * minimise the residual */
+enum { MP_GUESS_PREVIOUS = 0, MP_GUESS_ZERO = 1, MP_GUESS_LEARNED = 2, MP_GUESS_EXTRAPOLATE = 3,
+       MP_GUESS_PROJECT = 4 };
 
 typedef struct {
     double tol;        /* relative residual ||b - A x|| / ||b||, solver.cpp:154 */

@@ -21,7 +21,7 @@ MP_FP64, MP_FP32, MP_MG32 = 0, 1, 2
 MP_GRAD_X, MP_GRAD_Y, MP_GRAD_Z, MP_LAPLACIAN = range(4)
 MP_ROWS_ALL, MP_ROWS_INTERNAL, MP_ROWS_BOUNDARY = range(3)
 MP_PRECOND_NONE, MP_PRECOND_JACOBI, MP_PRECOND_AMG = range(3)
-MP_GUESS_PREVIOUS, MP_GUESS_ZERO, MP_GUESS_LEARNED, MP_GUESS_EXTRAPOLATE = range(4)
+MP_GUESS_PREVIOUS, MP_GUESS_ZERO, MP_GUESS_LEARNED, MP_GUESS_EXTRAPOLATE, MP_GUESS_PROJECT = range(5)
 MP_LOG_FIELDS = 8
 
 STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "NAN_DETECTED",

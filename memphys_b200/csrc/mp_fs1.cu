@@ -280,6 +280,145 @@ __global__ void k_hist_rotate(int nsys, const double *pcur, double *ph1, double 
     }
 }
 
+// ------------------------------------------------------------ projection guess
+// Fischer's projection of successive right-hand sides: with D_j the last pressure
+// increments and W_j = A D_j (= b_j - b_{j-1}: each p^{j+1} solved A p = b_j to the
+// tolerance), the guess p^n + sum_j c_j D_j minimises ||(b_n - b_{n-1}) - sum_j
+// c_j W_j|| = ||b_n - A(p^n + sum c_j D_j)|| up to the tolerance.  One pass forms
+// the right-hand side and the Gram matrix of the W_j (normalised, with a small
+// ridge: successive increments are nearly parallel), the last block solves it.
+constexpr int PROJ_MAX = 4;
+constexpr int PROJ_SUMS = PROJ_MAX + PROJ_MAX * (PROJ_MAX + 1) / 2;
+
+__global__ void __launch_bounds__(256)
+    k_proj_solve(int nsys, const double *b, const double *bprev, const double *W, int *state,
+                 double *coef, double *partials, unsigned *ticket) {
+    __shared__ double red[32 * PROJ_SUMS];
+    const int cnt = state[0];
+    double acc[PROJ_SUMS];
+#pragma unroll
+    for (int q = 0; q < PROJ_SUMS; q++)
+        acc[q] = 0.0;
+    if (cnt > 0) {
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += gridDim.x * blockDim.x) {
+            const double r = b[i] - bprev[i];
+            double w[PROJ_MAX];
+#pragma unroll
+            for (int j = 0; j < PROJ_MAX; j++)
+                w[j] = j < cnt ? W[(size_t)j * nsys + i] : 0.0;
+            int q = PROJ_MAX;
+#pragma unroll
+            for (int j = 0; j < PROJ_MAX; j++) {
+                acc[j] += w[j] * r;
+#pragma unroll
+                for (int l = j; l < PROJ_MAX; l++)
+                    acc[q++] += w[j] * w[l];
+            }
+        }
+    }
+    if (grid_reduce<PROJ_SUMS>(acc, partials, ticket, red) && threadIdx.x == 0) {
+        double G[PROJ_MAX][PROJ_MAX], h[PROJ_MAX], c[PROJ_MAX], sc[PROJ_MAX];
+        int q = PROJ_MAX;
+        for (int j = 0; j < PROJ_MAX; j++)
+            for (int l = j; l < PROJ_MAX; l++) {
+                G[j][l] = G[l][j] = acc[q];
+                q++;
+            }
+        const int m = cnt > 0 ? cnt : 0;
+        bool ok = m > 0;
+        for (int j = 0; j < m; j++) {
+            sc[j] = G[j][j] > 0 ? 1.0 / sqrt(G[j][j]) : 0.0;
+            ok = ok && G[j][j] > 0;
+        }
+        if (ok) {  // Cholesky of the normalised Gram matrix + 1e-12 ridge
+            double L[PROJ_MAX][PROJ_MAX];
+            for (int j = 0; j < m; j++) {
+                h[j] = acc[j] * sc[j];
+                for (int l = 0; l <= j; l++) {
+                    double v = G[j][l] * sc[j] * sc[l] + (j == l ? 1e-12 : 0.0);
+                    for (int k = 0; k < l; k++)
+                        v -= L[j][k] * L[l][k];
+                    if (j == l) {
+                        if (!(v > 0)) {
+                            ok = false;
+                            break;
+                        }
+                        L[j][j] = sqrt(v);
+                    } else {
+                        L[j][l] = v / L[l][l];
+                    }
+                }
+                if (!ok)
+                    break;
+            }
+            if (ok) {
+                for (int j = 0; j < m; j++) {  // L y = h
+                    double v = h[j];
+                    for (int k = 0; k < j; k++)
+                        v -= L[j][k] * c[k];
+                    c[j] = v / L[j][j];
+                }
+                for (int j = m - 1; j >= 0; j--) {  // L^T z = y
+                    double v = c[j];
+                    for (int k = j + 1; k < m; k++)
+                        v -= L[k][j] * c[k];
+                    c[j] = v / L[j][j];
+                }
+            }
+        }
+        for (int j = 0; j < PROJ_MAX; j++) {
+            const double v = (ok && j < m) ? c[j] * sc[j] : 0.0;
+            coef[j] = isfinite(v) ? v : 0.0;
+        }
+    }
+}
+
+// x = p^n + sum_j coef_j D_j (x holds p^n on entry)
+__global__ void k_proj_apply(int nsys, double *x, const double *D, const double *coef,
+                             const int *state) {
+    const int cnt = state[0];
+    if (cnt <= 0)
+        return;
+    double c[PROJ_MAX];
+#pragma unroll
+    for (int j = 0; j < PROJ_MAX; j++)
+        c[j] = j < cnt ? coef[j] : 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += gridDim.x * blockDim.x) {
+        double v = x[i];
+#pragma unroll
+        for (int j = 0; j < PROJ_MAX; j++)
+            if (j < cnt)
+                v = fma(c[j], D[(size_t)j * nsys + i], v);
+        x[i] = v;
+    }
+}
+
+// after the solve: the new increment and its image into the ring slot at the head
+// (the first step after a restart only records the right-hand side)
+__global__ void k_proj_push(int nsys, const double *x, const double *pcur, const double *b,
+                            double *bprev, double *D, double *W, const int *state) {
+    const int cnt = state[0], head = state[1];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += gridDim.x * blockDim.x) {
+        const double bi = b[i];
+        if (cnt >= 0) {
+            D[(size_t)head * nsys + i] = x[i] - pcur[i];
+            W[(size_t)head * nsys + i] = bi - bprev[i];
+        }
+        bprev[i] = bi;
+    }
+}
+
+__global__ void k_proj_advance(int *state) {
+    if (state[0] >= 0)
+        state[1] = (state[1] + 1) % PROJ_MAX;
+    state[0] = state[0] < 0 ? 0 : min(state[0] + 1, PROJ_MAX);
+}
+
+// the projected and the learned guesses keep the increment history
+static bool uses_projection(int guess) {
+    return guess == MP_GUESS_PROJECT || guess == MP_GUESS_LEARNED;
+}
+
 // distance from each node to its nearest stencil member
 __global__ void k_spacing(int nv, int dim, int K, const int *cols, const double *xyz, float *h) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -321,6 +460,13 @@ struct mp_fs1_s {
     // pressure history for the extrapolated and learned guesses
     dbuf<double> pcur, ph1, ph2, norms;
     dbuf<double> corr, flt1, flt_scale;  // learned correction and its coarse-level filter
+    // projection guess: the last PROJ_MAX increments D_j = p^{j+1} - p^j, their images
+    // W_j = A D_j = b_j - b_{j-1}, the previous right-hand side, and on the device the
+    // number of valid columns (-1: no previous right-hand side yet), the ring head and
+    // the coefficients of the last guess
+    dbuf<double> pD, pW, pbprev, pcoef, ppart;
+    dbuf<int> pstate;  // [0] valid columns, [1] ring head
+    dbuf<unsigned> pticket;
     // learned guess
     Mlp *mlp = nullptr;
     dbuf<float> hloc;
@@ -379,26 +525,32 @@ static int fs1_issue_pre(mp_fs1_s *f, int cur, cudaStream_t s) {
     MP_CHECK_LAUNCH();
     if (f->guess != MP_GUESS_PREVIOUS || f->collect) {
         const int ns = f->P.sys.nsys;
-        // the learned guess starts from the extrapolation (every entry, the border too)
-        const int gmode = f->guess == MP_GUESS_LEARNED ? MP_GUESS_EXTRAPOLATE : f->guess;
+        // the learned guess starts from the projection (every entry, the border too)
+        const int gmode = f->guess == MP_GUESS_LEARNED ? MP_GUESS_PROJECT : f->guess;
         k_guess<<<(unsigned)std::min((ns + 255) / 256, sm_count() * 4), 256, 0, s>>>(
             ns, gmode, f->P.W.x.p, f->pcur.p, f->ph1.p, f->step.p);
         MP_CHECK_LAUNCH();
+        if (uses_projection(f->guess)) {
+            const unsigned g = (unsigned)std::min((ns + 255) / 256, sm_count() * 4);
+            k_proj_solve<<<g, 256, 0, s>>>(ns, f->P.W.b64.p, f->pbprev.p, f->pW.p, f->pstate.p,
+                                           f->pcoef.p, f->ppart.p, f->pticket.p);
+            MP_CHECK_LAUNCH();
+            k_proj_apply<<<g, 256, 0, s>>>(ns, f->P.W.x.p, f->pD.p, f->pcoef.p, f->pstate.p);
+            MP_CHECK_LAUNCH();
+        }
         if (f->guess == MP_GUESS_LEARNED) {
             const MlpFields F = fs1_fields(f);
             MP_TRY(mlp_norms(F, f->norms.p, f->P.W.partials.p, f->P.W.ticket.p, s));
-            // extrapolation + the prediction, low-pass filtered through the first
-            // multigrid level (the pointwise noise of the network would otherwise
-            // dominate the residual of the guess) and weighted to minimise the
-            // guess's residual
-            const bool filt = f->flt_scale.p != nullptr;
-            MP_TRY(mlp_predict_fields(*f->mlp, F, f->P.W.x.p, filt ? f->corr.p : nullptr,
-                                      f->step.p, s));
-            if (filt) {  // corr <- filtered corr; x += theta corr
+            // projection + the predicted second difference, low-pass filtered through
+            // the first multigrid level where there is one (the pointwise noise of the
+            // network would otherwise dominate the residual of the guess) and weighted
+            // to minimise the guess's residual: x += theta corr, theta = 0 unless the
+            // correction removes a tenth of the squared residual
+            MP_TRY(mlp_predict_fields(*f->mlp, F, f->P.W.x.p, f->corr.p, f->step.p, s));
+            if (f->flt_scale.p)
                 MP_TRY(amg_filter(*f->P.sys.amg, f->corr.p, f->flt1.p, f->flt_scale.p,
                                   f->corr.p, s));
-                MP_TRY(f->P.issue_guess_min_residual(f->corr.p, s));
-            }
+            MP_TRY(f->P.issue_guess_min_residual(f->corr.p, s));
         }
     }
     return MP_OK;
@@ -441,6 +593,15 @@ static int fs1_issue_post(mp_fs1_s *f, int cur, cudaStream_t s) {
             MP_TRY(mlp_norms(F, f->norms.p, f->P.W.partials.p, f->P.W.ticket.p, s));
         MP_TRY(mlp_collect(F, f->sidx.p, f->nsample, f->P.W.x.p, f->sX.p, f->st.p, f->step.p,
                            f->cap_steps, s));
+    }
+    if (uses_projection(f->guess)) {
+        const int ns = f->P.sys.nsys;
+        const unsigned g = (unsigned)std::min((ns + 255) / 256, sm_count() * 4);
+        k_proj_push<<<g, 256, 0, s>>>(ns, f->P.W.x.p, f->pcur.p, f->P.W.b64.p, f->pbprev.p,
+                                      f->pD.p, f->pW.p, f->pstate.p);
+        MP_CHECK_LAUNCH();
+        k_proj_advance<<<1, 1, 0, s>>>(f->pstate.p);
+        MP_CHECK_LAUNCH();
     }
     if (f->guess != MP_GUESS_PREVIOUS || f->collect) {
         const int ns = f->P.sys.nsys;
@@ -488,6 +649,26 @@ static int fs1_step_once(mp_fs1_s *f, bool graph, cudaStream_t s) {
 }
 
 }  // namespace mp
+
+// storage of the projection guess, its history emptied (the first step only
+// records its right-hand side)
+static int proj_reserve(mp_fs1 f) {
+    const size_t ns = (size_t)f->P.sys.nsys;
+    if (!f->pD.p) {
+        MP_TRY(f->pD.alloc(ns * PROJ_MAX));
+        MP_TRY(f->pW.alloc(ns * PROJ_MAX));
+        MP_TRY(f->pbprev.alloc(ns));
+        MP_TRY(f->pcoef.alloc(PROJ_MAX));
+        MP_TRY(f->ppart.alloc((size_t)PROJ_SUMS * sm_count() * 4 + 64));
+        MP_TRY(f->pticket.alloc(1));
+        MP_TRY(f->pstate.alloc(2));
+        MP_CUDA(cudaMemset(f->pticket.p, 0, sizeof(unsigned)));
+        MP_CUDA(cudaMemset(f->pcoef.p, 0, sizeof(double) * PROJ_MAX));
+    }
+    const int st[2] = {-1, 0};
+    MP_CUDA(cudaMemcpy(f->pstate.p, st, sizeof(st), cudaMemcpyHostToDevice));
+    return MP_OK;
+}
 
 extern "C" int mp_fs1_create(mp_cloud c, const uint8_t *boundary, const double *normal,
                              const uint8_t *u_dir, const uint8_t *v_dir, const uint8_t *w_dir,
@@ -587,11 +768,13 @@ extern "C" int mp_fs1_create(mp_cloud c, const uint8_t *boundary, const double *
     for (dbuf<double> *b : {&f->pcur, &f->ph1, &f->ph2})
         cudaMemset(b->p, 0, sizeof(double) * ns);
     f->guess = solver->guess;
-    if (f->guess < MP_GUESS_PREVIOUS || f->guess > MP_GUESS_EXTRAPOLATE)
+    if (f->guess < MP_GUESS_PREVIOUS || f->guess > MP_GUESS_PROJECT)
         return bail(fail(MP_BAD_ARG, "unknown initial-guess mode %d", f->guess));
     if (f->guess == MP_GUESS_LEARNED)
         return bail(fail(MP_BAD_ARG, "the learned guess needs a network: mp_fs1_attach_mlp, then "
                                      "mp_fs1_set_guess"));
+    if (f->guess == MP_GUESS_PROJECT && (rc = proj_reserve(f)) != MP_OK)
+        return bail(rc);
     cudaMemset(f->step.p, 0, sizeof(int));
     cudaMemset(f->P.W.x.p, 0, sizeof(double) * f->P.sys.nsys);
     if (cudaDeviceSynchronize() != cudaSuccess)
@@ -621,6 +804,10 @@ extern "C" int mp_fs1_set_state(mp_fs1 f, const double *const *vel, const double
         const size_t bytes = sizeof(double) * f->P.sys.nsys;
         for (dbuf<double> *h : {&f->pcur, &f->ph1, &f->ph2})
             MP_CUDA(cudaMemcpyAsync(h->p, f->P.W.x.p, bytes, cudaMemcpyDeviceToDevice, st));
+        if (f->pstate.p) {
+            const int ps[2] = {-1, 0};
+            MP_CUDA(cudaMemcpyAsync(f->pstate.p, ps, sizeof(ps), cudaMemcpyHostToDevice, st));
+        }
     }
     MP_CUDA(cudaMemcpyAsync(f->step.p, &it, sizeof(int), cudaMemcpyHostToDevice, st));
     MP_CUDA(cudaStreamSynchronize(st));
@@ -757,9 +944,9 @@ extern "C" int mp_fs1_attach_mlp(mp_fs1 f, mp_mlp m, int sample_nodes, int capac
     MP_TRY(f->sX.alloc((size_t)capacity_steps * f->nsample * MLP_IN));
     MP_TRY(f->st.alloc((size_t)capacity_steps * f->nsample));
     f->collect = collect ? 1 : 0;
+    MP_TRY(f->corr.alloc(nv));
     if (f->P.sys.amg && amg_filter_size(*f->P.sys.amg) > 0) {
         const int n1 = amg_filter_size(*f->P.sys.amg);
-        MP_TRY(f->corr.alloc(nv));
         MP_TRY(f->flt1.alloc(n1));
         MP_TRY(f->flt_scale.alloc(n1));
         MP_TRY(amg_filter_setup(*f->P.sys.amg, f->flt_scale.p, 0));
@@ -769,11 +956,13 @@ extern "C" int mp_fs1_attach_mlp(mp_fs1 f, mp_mlp m, int sample_nodes, int capac
 }
 
 extern "C" int mp_fs1_set_guess(mp_fs1 f, int guess) {
-    if (!f || guess < MP_GUESS_PREVIOUS || guess > MP_GUESS_EXTRAPOLATE)
+    if (!f || guess < MP_GUESS_PREVIOUS || guess > MP_GUESS_PROJECT)
         return fail(MP_BAD_ARG, "mp_fs1_set_guess: unknown mode %d", guess);
     if (guess == MP_GUESS_LEARNED && !f->mlp)
         return fail(MP_BAD_ARG, "the learned guess needs mp_fs1_attach_mlp first");
     if (guess != f->guess) {
+        if (uses_projection(guess))
+            MP_TRY(proj_reserve(f));
         f->guess = guess;
         fs1_invalidate(f);
     }

@@ -97,7 +97,7 @@ def test_learned_guess_saves_iterations(mp_lib):
     vel, p = fs.get_state()
     res = {}
     for guess in (capi.MP_GUESS_ZERO, capi.MP_GUESS_PREVIOUS, capi.MP_GUESS_EXTRAPOLATE,
-                  capi.MP_GUESS_LEARNED):
+                  capi.MP_GUESS_PROJECT, capi.MP_GUESS_LEARNED):
         meshless.set_guess(fs, guess)
         fs.set_state(vel, p, 40)
         fs.step(6)
