@@ -17,8 +17,11 @@ Printed (rank 0, one JSON line): the plain FP64 ms/step as `value`
 (lower is better); the variants beside it (FP32 multigrid storage, FP32
 Krylov with FP64 refinement, extrapolated, projected and learned initial
 guesses, and learned + FP32 multigrid as `learned_mixed`); the end-to-end ms/step through
-mp_fs1_single_timestep with pinned host buffers; the SpMV roofline; and the
-CPU oracle baseline.
+mp_fs1_single_timestep with pinned host buffers; the SpMV roofline; the
+CPU oracle baseline; the batched uneven stencils; the 3D mixed-precision cube
+(2,195,456 nodes, per-field error against FP64); and the learned-guess channel
+(1,004,010 nodes, network trained on 500 plain-solver steps, each initial guess
+timed from the same state).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--nx NX]
 """
@@ -62,6 +65,15 @@ def parse():
     ap.add_argument("--batched", type=int, default=4_000_000,
                     help="independent uneven stencil systems per dimension in the batched "
                          "weights measurement (0 skips it)")
+    ap.add_argument("--no-cube", action="store_true",
+                    help="skip the 3D mixed-precision cube (2,195,456 nodes)")
+    ap.add_argument("--cube-n", type=int, default=128)
+    ap.add_argument("--cube-spinup", type=int, default=10)
+    ap.add_argument("--no-channel", action="store_true",
+                    help="skip the learned-guess channel (1,004,010 nodes)")
+    ap.add_argument("--channel-h", type=float, default=2.828e-3)
+    ap.add_argument("--channel-train-steps", type=int, default=500)
+    ap.add_argument("--channel-samples", type=int, default=4096)
     ap.add_argument("--inner-tol", type=float, default=1e-3,
                     help="mixed precision: relative reduction of each FP32 refinement solve")
     ap.add_argument("--profile", default=None, choices=["steps", "spmv", "stencil"],
@@ -369,7 +381,136 @@ def run_ours(args, ws, rank, local, pg):
         out["cpu_baseline"] = cpu_baseline(cl, cld)
     if args.batched > 0:
         out["batched_stencils"] = batched_stencils(args.batched)
+    if ws == 1 and not args.no_cube:
+        out["cube3d_mixed"] = cube_mixed(args, stream)
+    if ws == 1 and not args.no_channel:
+        out["channel_learned"] = channel_learned(args, stream)
     return out
+
+
+def steps_timed(f, stream, first, warmup, steps):
+    """`warmup` untimed steps, then `steps` steps between CUDA events; returns the
+    ms per step and the solver log of the timed steps (first = the step index the
+    state was set to)."""
+    from memphys_b200 import capi
+    for _ in range(warmup):
+        f.step(1, stream.handle)
+    stream.sync()
+    with capi.Timer(stream.handle) as tm:
+        for _ in range(steps):
+            f.step(1, stream.handle)
+    return tm.ms / steps, f.log(first + warmup, steps)
+
+
+def cube_mixed(args, stream):
+    """The 3D mixed-precision configuration: unit-cube lid-driven cavity, 128^3
+    jittered interior + 6 * 128^2 face nodes, PHS r^3 + degree 3 (20 monomials),
+    40-node stencils, Re = 100.  From rest, `--cube-spinup` untimed steps, then the
+    bench's warm-up and timed steps, for FP64, FP32 Krylov + FP64 refinement
+    (MP_FP32) and FP32 multigrid storage (MP_MG32); the error of each field after
+    the same steps is stated against the FP64 run."""
+    from memphys_b200 import capi, clouds, meshless
+    t0 = time.time()
+    cl = clouds.cube_3d(args.cube_n)
+    prm = meshless.PARAMETERS(solver_type="cuda_bicgstab_amg", solver_tolerance=1e-8, n_iter=2000)
+    prm.rho, prm.mu = 1.0, 0.01
+    pts = meshless.POINTS(cl)
+    cld = meshless.CLOUD(pts, prm, compute_cond=False)
+    t_cloud = time.time() - t0
+    prm.dt = meshless.calc_dt(cld, 1.0, 1.0, 1.0, prm.mu / prm.rho, args.courant)
+    vel0 = [cl.vel_bc[d].copy() for d in range(3)]
+    res, states = {}, {}
+    for name, cfg in (("fp64", {}),
+                      ("fp32_refined", {"precision": capi.MP_FP32, "inner_tol": args.inner_tol}),
+                      ("mg32", {"precision": capi.MP_MG32})):
+        t0 = time.time()
+        f = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                       cl.p_dirichlet, 2, w_dirichlet_flag=cl.w_dirichlet, **cfg)
+        t_setup = time.time() - t0
+        f.set_state(vel0, np.zeros(f.system_size), 0)
+        f.step(args.cube_spinup, stream.handle)
+        ms, lg = steps_timed(f, stream, args.cube_spinup, args.warmup, args.steps)
+        states[name] = f.get_state()
+        res[name] = {"ms_per_step": round(ms, 3), "iters_per_step": float(lg[:, 0].mean()),
+                     "refinements_per_step": float(lg[:, 5].mean()),
+                     "max_relres": float(lg[:, 1].max()), "setup_s": round(t_setup, 2)}
+        del f
+    v64, p64 = states["fp64"]
+    for name in ("fp32_refined", "mg32"):
+        vv, pp = states[name]
+        err = {c: float(np.abs(vv[d] - v64[d]).max() / max(np.abs(v64[d]).max(), 1e-300))
+               for d, c in enumerate("uvw")}
+        err["p"] = float(np.abs((pp - p64)[:cl.nv]).max() / np.abs(p64[:cl.nv]).max())
+        res[name]["rel_err_vs_fp64"] = err
+        res[name]["speedup_vs_fp64"] = round(res["fp64"]["ms_per_step"] / res[name]["ms_per_step"], 3)
+    return {"workload": f"cube_3d {args.cube_n}^3 jittered + faces = {cl.nv} nodes, 40-node "
+                        "stencils, BiCGSTAB + SA multigrid to 1e-8",
+            "nodes": cl.nv, "dt": prm.dt, "spinup_steps": args.cube_spinup,
+            "cloud_s": round(t_cloud, 2), **res}
+
+
+def channel_learned(args, stream):
+    """The learned-guess configuration: channel [0,8] x [0,1] with a cylinder of
+    radius 0.1 at (1, 0.5), Re = 200, h = `--channel-h` (1,004,010 nodes), 20-node
+    stencils, outlet p-Dirichlet.  The plain solver runs `--channel-train-steps`
+    steps from rest while the network records its samples; the network is trained
+    on them; then, from that state, each initial guess times the same steps
+    (iterations and ms/step; the configuration's comparison is learned against
+    zero).  The size of the second temporal difference that the network predicts,
+    relative to the increment and to the pressure, is stated beside it."""
+    from memphys_b200 import capi, clouds, meshless
+    cl = clouds.channel_2d(args.channel_h)
+    prm = meshless.PARAMETERS(solver_type="cuda_bicgstab_amg", solver_tolerance=1e-8, n_iter=4000)
+    prm.rho, prm.mu = 1.0, 0.2 / 200.0
+    pts = meshless.POINTS(cl)
+    cld = meshless.CLOUD(pts, prm, compute_cond=False)
+    prm.dt = meshless.calc_dt(cld, 1.5, 1.0, 0.0, prm.mu / prm.rho, args.courant)
+    f = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet, cl.p_dirichlet,
+                                   2, w_dirichlet_flag=cl.w_dirichlet)
+    T = max(args.channel_train_steps, 4)
+    net = meshless.MLP(seed=11)
+    ns_ = min(args.channel_samples, cl.nv)
+    meshless.attach_mlp(f, net, sample_nodes=ns_, capacity_steps=T)
+    f.set_state([cl.vel_bc[0], cl.vel_bc[1]], np.zeros(f.system_size), 0)
+    t0 = time.time()
+    f.step(T - 2, stream.handle)
+    p1 = f.get_state()[1][:cl.nv]
+    f.step(1, stream.handle)
+    p2 = f.get_state()[1][:cl.nv]
+    f.step(1, stream.handle)
+    vel, p = f.get_state()
+    t_spin = time.time() - t0
+    plain = f.log(T - 100, 100) if T > 100 else f.log(0, T)
+    rms = lambda a: float(np.sqrt(np.mean(a * a)))
+    inc, d2 = p[:cl.nv] - p2, (p[:cl.nv] - p2) - (p2 - p1)
+    t0 = time.time()
+    loss = meshless.train_mlp(f, epochs=args.epochs, batch=1024, lr=1e-3)
+    t_train = time.time() - t0
+    meshless.attach_mlp(f, net, sample_nodes=1, capacity_steps=1, collect=False)
+    res = {}
+    for name, g in (("zero", capi.MP_GUESS_ZERO), ("previous", capi.MP_GUESS_PREVIOUS),
+                    ("extrapolated", capi.MP_GUESS_EXTRAPOLATE),
+                    ("projected", capi.MP_GUESS_PROJECT), ("learned", capi.MP_GUESS_LEARNED)):
+        meshless.set_guess(f, g)
+        f.set_state(vel, p, T + 1)
+        ms, lg = steps_timed(f, stream, T + 1, args.warmup, args.steps)
+        res[name] = {"ms_per_step": round(ms, 3), "iters_per_step": float(lg[:, 0].mean()),
+                     "relres0_median": float(np.median(lg[:, 4])),
+                     "max_relres": float(lg[:, 1].max())}
+        if g == capi.MP_GUESS_LEARNED:
+            res[name]["learned_weight_mean"] = float(np.mean(lg[:, 6]))
+    res["learned"]["speedup_vs_zero_guess"] = round(res["zero"]["ms_per_step"] /
+                                                    res["learned"]["ms_per_step"], 3)
+    return {"workload": f"channel_2d h={args.channel_h} with cylinder, {cl.nv} nodes, Re 200, "
+                        "BiCGSTAB + SA multigrid to 1e-8",
+            "nodes": cl.nv, "dt": prm.dt,
+            "training": {"plain_steps": T, "sample_nodes": ns_, "samples": ns_ * (T - 2),
+                         "epochs": args.epochs, "final_loss": loss,
+                         "spinup_s": round(t_spin, 2), "train_s": round(t_train, 2),
+                         "plain_iters_last_steps": float(plain[:, 0].mean())},
+            "second_difference_over_increment": rms(d2) / rms(inc),
+            "increment_over_pressure": rms(inc) / rms(p[:cl.nv]),
+            "guesses": res}
 
 
 def batched_stencils(nsys: int):

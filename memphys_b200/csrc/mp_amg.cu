@@ -1,8 +1,11 @@
 // mp_amg.cu -- smoothed-aggregation multigrid: host setup, GPU V-cycle.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <cstdlib>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <tuple>
 #include <type_traits>
 #include <cmath>
@@ -12,12 +15,75 @@
 
 namespace mp {
 
+// ------------------------------------------------------- host parallel loops
+// The host setup splits its row loops into fixed chunks of rows that worker
+// threads claim in any order; every chunk writes its own output range (or
+// partial sum, combined in chunk order), so the hierarchy is bit-identical for
+// any number of threads.  MP_HOST_THREADS overrides the thread count.
+static unsigned host_threads() {
+    static const unsigned n = [] {
+        const char *e = getenv("MP_HOST_THREADS");
+        long v = e ? strtol(e, nullptr, 10) : 0;
+        if (v <= 0)
+            v = (long)std::thread::hardware_concurrency();
+        return (unsigned)std::max(1L, std::min(v, 64L));
+    }();
+    return n;
+}
+
+constexpr int HOST_CHUNK = 16384;
+
+// fn(thread, chunk, first row, end row) for every chunk of [0, n)
+template <class F> static void par_chunks(int n, F &&fn) {
+    const int nch = (n + HOST_CHUNK - 1) / HOST_CHUNK;
+    const unsigned nt = std::min<unsigned>(host_threads(), (unsigned)std::max(nch, 1));
+    auto run = [&](unsigned t, std::atomic<int> &next) {
+        for (int c; (c = next.fetch_add(1)) < nch;)
+            fn(t, c, c * HOST_CHUNK, std::min(n, (c + 1) * HOST_CHUNK));
+    };
+    std::atomic<int> next{0};
+    if (nt <= 1) {
+        run(0, next);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; t++)
+        th.emplace_back(run, t, std::ref(next));
+    run(0, next);
+    for (auto &x : th)
+        x.join();
+}
+
+// rows produced chunk by chunk: per-chunk column/value lists and row lengths,
+// then concatenated in chunk order
+struct ChunkRows {
+    std::vector<std::vector<int>> ci;
+    std::vector<std::vector<double>> v;
+    explicit ChunkRows(int n) : ci((n + HOST_CHUNK - 1) / HOST_CHUNK), v(ci.size()) {}
+};
+
 // ================================================================ host setup
 struct Csr {
     int n = 0, m = 0;
     std::vector<int> rp, ci;
     std::vector<double> v;
 };
+
+// C.rp must hold the row lengths at rp[i + 1]; turns them into offsets and
+// gathers the chunks' entries
+static void concat_rows(Csr &C, ChunkRows &R) {
+    C.rp[0] = 0;
+    for (int i = 0; i < C.n; i++)
+        C.rp[i + 1] += C.rp[i];
+    C.ci.resize(C.rp[C.n]);
+    C.v.resize(C.rp[C.n]);
+    par_chunks(C.n, [&](unsigned, int c, int lo, int) {
+        std::copy(R.ci[c].begin(), R.ci[c].end(), C.ci.begin() + C.rp[lo]);
+        std::copy(R.v[c].begin(), R.v[c].end(), C.v.begin() + C.rp[lo]);
+        std::vector<int>().swap(R.ci[c]);
+        std::vector<double>().swap(R.v[c]);
+    });
+}
 
 static int csr_from_ell(const Ell &E, Csr &C) {
     const int np = ell_padded_rows(E.nrows), K = E.K;
@@ -28,35 +94,44 @@ static int csr_from_ell(const Ell &E, Csr &C) {
     C.n = E.nrows;
     C.m = E.nrows;
     C.rp.assign(C.n + 1, 0);
-    C.ci.clear();
-    C.v.clear();
-    C.ci.reserve((size_t)C.n * K);
-    C.v.reserve((size_t)C.n * K);
-    for (int i = 0; i < C.n; i++) {
-        // merge duplicate columns (setFromTriplets semantics)
-        const size_t base = (size_t)(i / SLICE) * K * SLICE + (i % SLICE);
-        const int start = (int)C.ci.size();
-        for (int k = 0; k < K; k++) {
-            const int c = cols[base + (size_t)k * SLICE];
-            const double a = vals[base + (size_t)k * SLICE];
-            if (a == 0.0 && c != i)
-                continue;
-            if (c < 0 || c >= C.m)
-                return fail(MP_BAD_ARG, "operator column %d out of range in row %d", c, i);
-            bool merged = false;
-            for (int t = start; t < (int)C.ci.size(); t++)
-                if (C.ci[t] == c) {
-                    C.v[t] += a;
-                    merged = true;
-                    break;
+    ChunkRows R(C.n);
+    std::atomic<int> bad{-1};
+    par_chunks(C.n, [&](unsigned, int c, int lo, int hi) {
+        std::vector<int> &ci = R.ci[c];
+        std::vector<double> &v = R.v[c];
+        ci.reserve((size_t)(hi - lo) * K);
+        v.reserve((size_t)(hi - lo) * K);
+        for (int i = lo; i < hi; i++) {
+            // merge duplicate columns (setFromTriplets semantics)
+            const size_t base = (size_t)(i / SLICE) * K * SLICE + (i % SLICE);
+            const size_t start = ci.size();
+            for (int k = 0; k < K; k++) {
+                const int col = cols[base + (size_t)k * SLICE];
+                const double a = vals[base + (size_t)k * SLICE];
+                if (a == 0.0 && col != i)
+                    continue;
+                if (col < 0 || col >= C.m) {
+                    bad.store(i);
+                    continue;
                 }
-            if (!merged) {
-                C.ci.push_back(c);
-                C.v.push_back(a);
+                bool merged = false;
+                for (size_t t = start; t < ci.size(); t++)
+                    if (ci[t] == col) {
+                        v[t] += a;
+                        merged = true;
+                        break;
+                    }
+                if (!merged) {
+                    ci.push_back(col);
+                    v.push_back(a);
+                }
             }
+            C.rp[i + 1] = (int)(ci.size() - start);
         }
-        C.rp[i + 1] = (int)C.ci.size();
-    }
+    });
+    if (bad.load() >= 0)
+        return fail(MP_BAD_ARG, "operator column out of range in row %d", bad.load());
+    concat_rows(C, R);
     return MP_OK;
 }
 
@@ -94,7 +169,8 @@ static Csr diff_form(const Csr &A) {
     return D;
 }
 
-// largest |eigenvalue| of D^-1 A by power iteration (deterministic start)
+// largest |eigenvalue| of D^-1 A by power iteration (deterministic start; the
+// norms are summed per row chunk, then over the chunks in order)
 static double lmax_power(const Csr &A, const std::vector<double> &dinv, int iters) {
     std::vector<double> x(A.n), y(A.n);
     uint64_t s = 0x9E3779B97F4A7C15ull;
@@ -104,123 +180,182 @@ static double lmax_power(const Csr &A, const std::vector<double> &dinv, int iter
         s ^= s << 17;
         x[i] = 0.5 + (double)(s >> 11) / 9007199254740992.0;
     }
+    const int nch = (A.n + HOST_CHUNK - 1) / HOST_CHUNK;
+    std::vector<double> py(nch), px(nch);
     double lam = 1.0;
     for (int it = 0; it < iters; it++) {
+        par_chunks(A.n, [&](unsigned, int c, int lo, int hi) {
+            double ny = 0.0, nx = 0.0;
+            for (int i = lo; i < hi; i++) {
+                double a = 0.0;
+                for (int t = A.rp[i]; t < A.rp[i + 1]; t++)
+                    a += A.v[t] * x[A.ci[t]];
+                y[i] = dinv[i] * a;
+                ny += y[i] * y[i];
+                nx += x[i] * x[i];
+            }
+            py[c] = ny;
+            px[c] = nx;
+        });
         double ny = 0.0, nx = 0.0;
-        for (int i = 0; i < A.n; i++) {
-            double a = 0.0;
-            for (int t = A.rp[i]; t < A.rp[i + 1]; t++)
-                a += A.v[t] * x[A.ci[t]];
-            y[i] = dinv[i] * a;
-            ny += y[i] * y[i];
-            nx += x[i] * x[i];
+        for (int c = 0; c < nch; c++) {
+            ny += py[c];
+            nx += px[c];
         }
         if (ny == 0.0)
             return 1.0;
         lam = std::sqrt(ny / nx);
         const double inv = 1.0 / std::sqrt(ny);
-        for (int i = 0; i < A.n; i++)
-            x[i] = y[i] * inv;
+        par_chunks(A.n, [&](unsigned, int, int lo, int hi) {
+            for (int i = lo; i < hi; i++)
+                x[i] = y[i] * inv;
+        });
     }
     return lam;
 }
+
+static void transpose(const Csr &A, Csr &T);
 
 // greedy aggregation on the symmetrised strong graph; isolated rows
 // (Dirichlet identities) get no aggregate
 static int aggregate(const Csr &A, double theta, std::vector<int> &agg) {
     const int n = A.n;
-    std::vector<std::vector<int>> S(n);
-    for (int i = 0; i < n; i++) {
-        double mx = 0.0;
-        for (int t = A.rp[i]; t < A.rp[i + 1]; t++)
-            if (A.ci[t] != i)
-                mx = std::max(mx, std::fabs(A.v[t]));
-        if (mx == 0.0)
-            continue;
-        for (int t = A.rp[i]; t < A.rp[i + 1]; t++) {
-            const int j = A.ci[t];
-            if (j != i && std::fabs(A.v[t]) >= theta * mx) {
-                S[i].push_back(j);
-                S[j].push_back(i);
+    // strong entries per row, then S = their union with the transpose (sorted,
+    // duplicates removed)
+    Csr G;
+    G.n = G.m = n;
+    G.rp.assign(n + 1, 0);
+    {
+        ChunkRows R(n);
+        par_chunks(n, [&](unsigned, int c, int lo, int hi) {
+            for (int i = lo; i < hi; i++) {
+                double mx = 0.0;
+                for (int t = A.rp[i]; t < A.rp[i + 1]; t++)
+                    if (A.ci[t] != i)
+                        mx = std::max(mx, std::fabs(A.v[t]));
+                int cnt = 0;
+                if (mx > 0.0)
+                    for (int t = A.rp[i]; t < A.rp[i + 1]; t++) {
+                        const int j = A.ci[t];
+                        if (j != i && std::fabs(A.v[t]) >= theta * mx) {
+                            R.ci[c].push_back(j);
+                            R.v[c].push_back(0.0);
+                            cnt++;
+                        }
+                    }
+                G.rp[i + 1] = cnt;
             }
-        }
+        });
+        concat_rows(G, R);
     }
-    for (auto &s : S) {
-        std::sort(s.begin(), s.end());
-        s.erase(std::unique(s.begin(), s.end()), s.end());
+    Csr GT;
+    transpose(G, GT);
+    Csr S;
+    S.n = S.m = n;
+    S.rp.assign(n + 1, 0);
+    {
+        ChunkRows R(n);
+        par_chunks(n, [&](unsigned, int c, int lo, int hi) {
+            std::vector<int> row;
+            for (int i = lo; i < hi; i++) {
+                row.assign(G.ci.begin() + G.rp[i], G.ci.begin() + G.rp[i + 1]);
+                row.insert(row.end(), GT.ci.begin() + GT.rp[i], GT.ci.begin() + GT.rp[i + 1]);
+                std::sort(row.begin(), row.end());
+                row.erase(std::unique(row.begin(), row.end()), row.end());
+                R.ci[c].insert(R.ci[c].end(), row.begin(), row.end());
+                R.v[c].resize(R.ci[c].size());
+                S.rp[i + 1] = (int)row.size();
+            }
+        });
+        concat_rows(S, R);
     }
+    auto nbrs = [&](int i) {
+        return std::make_pair(S.ci.begin() + S.rp[i], S.ci.begin() + S.rp[i + 1]);
+    };
     agg.assign(n, -1);
     int na = 0;
     for (int i = 0; i < n; i++) {  // pass 1: roots whose neighbourhood is free
-        if (agg[i] >= 0 || S[i].empty())
+        const auto [b, e] = nbrs(i);
+        if (agg[i] >= 0 || b == e)
             continue;
         bool free_ = true;
-        for (int j : S[i])
-            if (agg[j] >= 0) {
+        for (auto it = b; it != e; ++it)
+            if (agg[*it] >= 0) {
                 free_ = false;
                 break;
             }
         if (!free_)
             continue;
         agg[i] = na;
-        for (int j : S[i])
-            agg[j] = na;
+        for (auto it = b; it != e; ++it)
+            agg[*it] = na;
         na++;
     }
     std::vector<int> pass1 = agg;
     for (int i = 0; i < n; i++) {  // pass 2: join a neighbouring pass-1 aggregate
-        if (agg[i] >= 0 || S[i].empty())
+        const auto [b, e] = nbrs(i);
+        if (agg[i] >= 0 || b == e)
             continue;
-        for (int j : S[i])
-            if (pass1[j] >= 0) {
-                agg[i] = pass1[j];
+        for (auto it = b; it != e; ++it)
+            if (pass1[*it] >= 0) {
+                agg[i] = pass1[*it];
                 break;
             }
     }
     for (int i = 0; i < n; i++) {  // pass 3: leftovers form new aggregates
-        if (agg[i] >= 0 || S[i].empty())
+        const auto [b, e] = nbrs(i);
+        if (agg[i] >= 0 || b == e)
             continue;
         agg[i] = na;
-        for (int j : S[i])
-            if (agg[j] < 0)
-                agg[j] = na;
+        for (auto it = b; it != e; ++it)
+            if (agg[*it] < 0)
+                agg[*it] = na;
         na++;
     }
     return na;
 }
 
-// C = A * B (Gustavson)
+// C = A * B (Gustavson, rows in parallel; columns of each row sorted)
 static void spgemm(const Csr &A, const Csr &B, Csr &C) {
     C.n = A.n;
     C.m = B.m;
     C.rp.assign(A.n + 1, 0);
-    C.ci.clear();
-    C.v.clear();
-    std::vector<int> mark(B.m, -1);
-    std::vector<double> acc(B.m, 0.0);
-    std::vector<int> cols;
-    for (int i = 0; i < A.n; i++) {
-        cols.clear();
-        for (int t = A.rp[i]; t < A.rp[i + 1]; t++) {
-            const int k = A.ci[t];
-            const double a = A.v[t];
-            for (int u = B.rp[k]; u < B.rp[k + 1]; u++) {
-                const int j = B.ci[u];
-                if (mark[j] != i) {
-                    mark[j] = i;
-                    acc[j] = 0.0;
-                    cols.push_back(j);
+    ChunkRows R(A.n);
+    const unsigned nt = host_threads();
+    std::vector<std::vector<int>> mark(nt);
+    std::vector<std::vector<double>> acc(nt);
+    par_chunks(A.n, [&](unsigned th, int c, int lo, int hi) {
+        std::vector<int> &mk = mark[th];
+        std::vector<double> &ac = acc[th];
+        if (mk.empty()) {
+            mk.assign(B.m, -1);
+            ac.assign(B.m, 0.0);
+        }
+        std::vector<int> cols;
+        for (int i = lo; i < hi; i++) {
+            cols.clear();
+            for (int t = A.rp[i]; t < A.rp[i + 1]; t++) {
+                const int k = A.ci[t];
+                const double a = A.v[t];
+                for (int u = B.rp[k]; u < B.rp[k + 1]; u++) {
+                    const int j = B.ci[u];
+                    if (mk[j] != i) {
+                        mk[j] = i;
+                        ac[j] = 0.0;
+                        cols.push_back(j);
+                    }
+                    ac[j] += a * B.v[u];
                 }
-                acc[j] += a * B.v[u];
             }
+            std::sort(cols.begin(), cols.end());
+            for (int j : cols) {
+                R.ci[c].push_back(j);
+                R.v[c].push_back(ac[j]);
+            }
+            C.rp[i + 1] = (int)cols.size();
         }
-        std::sort(cols.begin(), cols.end());
-        for (int j : cols) {
-            C.ci.push_back(j);
-            C.v.push_back(acc[j]);
-        }
-        C.rp[i + 1] = (int)C.ci.size();
-    }
+    });
+    concat_rows(C, R);
 }
 
 static void transpose(const Csr &A, Csr &T) {
@@ -258,19 +393,21 @@ static int upload_ell(const Csr &C, Ell &E, bool self_pad, cudaStream_t s) {
     const size_t tot = (size_t)soff[ns] * SLICE;
     std::vector<int> cols(tot);
     std::vector<double> vals(tot, 0.0);
-    for (int i = 0; i < ns * SLICE; i++) {
-        const int sl = i / SLICE, r = i % SLICE, w = soff[sl + 1] - soff[sl];
-        const int len = i < C.n ? C.rp[i + 1] - C.rp[i] : 0;
-        for (int k = 0; k < w; k++) {
-            const size_t o = (size_t)soff[sl] * SLICE + (size_t)k * SLICE + r;
-            if (k < len) {
-                cols[o] = C.ci[C.rp[i] + k];
-                vals[o] = C.v[C.rp[i] + k];
-            } else {
-                cols[o] = (self_pad && i < C.n && i < C.m) ? i : 0;
+    par_chunks(ns * SLICE, [&](unsigned, int, int lo, int hi) {
+        for (int i = lo; i < hi; i++) {
+            const int sl = i / SLICE, r = i % SLICE, w = soff[sl + 1] - soff[sl];
+            const int len = i < C.n ? C.rp[i + 1] - C.rp[i] : 0;
+            for (int k = 0; k < w; k++) {
+                const size_t o = (size_t)soff[sl] * SLICE + (size_t)k * SLICE + r;
+                if (k < len) {
+                    cols[o] = C.ci[C.rp[i] + k];
+                    vals[o] = C.v[C.rp[i] + k];
+                } else {
+                    cols[o] = (self_pad && i < C.n && i < C.m) ? i : 0;
+                }
             }
         }
-    }
+    });
     E.nrows = C.n;
     E.ncols = C.m;
     E.K = kmax;
@@ -468,8 +605,34 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
     a->store = store;
     a->cheb_ratio = 1.0 / cfg.cheb_lower;
     a->sweeps = std::max(1, cfg.smoother_sweeps);
+    // seconds per setup phase: operator download, aggregation, power iteration,
+    // products, uploads, autotuner (printed with MP_VERBOSE)
+    double ph[6] = {0, 0, 0, 0, 0, 0};
+    auto tick = std::chrono::steady_clock::now();
+    auto lap = [&](int q) {
+        const auto now = std::chrono::steady_clock::now();
+        ph[q] += std::chrono::duration<double>(now - tick).count();
+        tick = now;
+    };
+    // with MP_VERBOSE: FNV-1a checksum of every level's operator and prolongator
+    // (the host setup gives the same hierarchy for any number of threads)
+    const bool verbose = getenv("MP_VERBOSE") != nullptr;
+    uint64_t hsum = 0xcbf29ce484222325ull;
+    auto hash_csr = [&](const Csr &C) {
+        if (!verbose)
+            return;
+        auto mix = [&](const void *p, size_t n) {
+            const unsigned char *b = (const unsigned char *)p;
+            for (size_t q = 0; q < n; q++)
+                hsum = (hsum ^ b[q]) * 0x100000001b3ull;
+        };
+        mix(C.rp.data(), sizeof(int) * C.rp.size());
+        mix(C.ci.data(), sizeof(int) * C.ci.size());
+        mix(C.v.data(), sizeof(double) * C.v.size());
+    };
     Csr A;
     int rc = csr_from_ell(A0, A);
+    lap(0);
     if (rc != MP_OK) {
         delete a;
         return rc;
@@ -505,11 +668,14 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
         const bool coarsest = A.n <= coarse_size || lev + 1 >= cfg.amg_max_levels;
         if (!coarsest) {
             std::vector<int> agg;
+            lap(4);
             const int na = aggregate(A, theta, agg);
+            lap(1);
             if (na == 0 || na >= A.n) {
                 // cannot coarsen further: this level becomes the coarsest
             } else {
                 const double lam = lmax_power(A, dinv, 30);
+                lap(2);
                 L->lmax = lscale * lam;
                 const double w = 4.0 / (3.0 * lam);
                 // AT = A * T, then P = T - w D^-1 AT
@@ -552,6 +718,9 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
                 transpose(P, R);
                 spgemm(A, P, AP);
                 spgemm(R, AP, Ac);
+                lap(3);
+                hash_csr(A);
+                hash_csr(P);
                 if ((rc = upload_ell(P, L->P, false, s)) != MP_OK ||
                     (rc = upload_ell(R, L->R, false, s)) != MP_OK ||
                     (rc = upload_csr(P, L->Pc, s)) != MP_OK || (rc = upload_csr(R, L->Rc, s)) != MP_OK)
@@ -567,6 +736,7 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
             }
         }
         // coarsest level: bordered dense inverse
+        hash_csr(A);
         std::vector<double> inv;
         if ((rc = coarse_inverse(A, inv)) != MP_OK)
             return bail(rc);
@@ -613,12 +783,15 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
                     return bail(rc);
         }
     }
+    lap(4);
     if ((rc = amg_autotune(*a, s)) != MP_OK)
         return bail(rc);
     MP_CUDA(cudaStreamSynchronize(s));
+    lap(5);
     a->setup_seconds =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    if (getenv("MP_VERBOSE")) {
+    if (verbose) {
+        fprintf(stderr, "[memphys amg] hierarchy checksum %016llx\n", (unsigned long long)hsum);
         for (size_t l = 0; l < a->L.size(); l++) {
             const AmgLevel &L = *a->L[l];
             fprintf(stderr, "[memphys amg] level %zu n=%d A.K=%d", l, L.n, L.A64.K);
@@ -629,7 +802,10 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
                         (double)L.Rc.ci.n / L.Rc.n);
             fprintf(stderr, " sched A=%d P=%d R=%d\n", L.sA.mode, L.sP.mode, L.sR.mode);
         }
-        fprintf(stderr, "[memphys amg] coarse n=%d setup %.2f s\n", a->nc, a->setup_seconds);
+        fprintf(stderr,
+                "[memphys amg] coarse n=%d setup %.2f s (download %.2f aggregate %.2f power %.2f "
+                "products %.2f upload %.2f autotune %.2f; %u host threads)\n",
+                a->nc, a->setup_seconds, ph[0], ph[1], ph[2], ph[3], ph[4], ph[5], host_threads());
     }
     *out = a;
     return MP_OK;
