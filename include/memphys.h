@@ -185,7 +185,7 @@ enum { MP_PRECOND_NONE = 0, MP_PRECOND_JACOBI = 1, MP_PRECOND_AMG = 2 };
 /* initial guess of each fractional-step pressure solve: the previous pressure
  * (the reference's solveWithGuess(rhs, p_old)), zero, the linear extrapolation
  * 2 p^n - p^(n-1), the projection p^n + sum_j c_j (p^(j+1) - p^j) over the last
- * four increments with c minimising the guess's residual (Fischer's projection
+ * guess_vectors increments with c minimising the guess's residual (Fischer's projection
  * of successive right-hand sides; the increments' images are the differences of
  * successive right-hand sides, so it costs no extra matrix product), or that
  * projection plus the learned network's predicted correction, weighted to
@@ -204,6 +204,7 @@ typedef struct {
     int amg_coarse_size;  /* levels stop at or below this size; the coarsest is inverted densely */
     int smoother_sweeps;  /* degree-2 Chebyshev applications before and after each coarse correction */
     double cheb_lower;    /* Chebyshev interval [cheb_lower * lambda_max, 1.1 lambda_max] of D^-1 A */
+    int guess_vectors;    /* MP_GUESS_PROJECT / MP_GUESS_LEARNED: pressure increments kept, 1-8 (8) */
 } mp_solver_cfg;
 
 /* sensible defaults for the fields above */

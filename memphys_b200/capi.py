@@ -57,7 +57,8 @@ class SolverCfg(C.Structure):
     _fields_ = [("tol", C.c_double), ("maxit", C.c_int), ("precond", C.c_int),
                 ("precision", C.c_int), ("guess", C.c_int), ("inner_tol", C.c_double),
                 ("amg_max_levels", C.c_int), ("amg_coarse_size", C.c_int),
-                ("smoother_sweeps", C.c_int), ("cheb_lower", C.c_double)]
+                ("smoother_sweeps", C.c_int), ("cheb_lower", C.c_double),
+                ("guess_vectors", C.c_int)]
 
 
 class Fs1Cfg(C.Structure):

@@ -281,13 +281,13 @@ __global__ void k_hist_rotate(int nsys, const double *pcur, double *ph1, double 
 }
 
 // ------------------------------------------------------------ projection guess
-// Fischer's projection of successive right-hand sides: with D_j the last pressure
-// increments and W_j = A D_j (= b_j - b_{j-1}: each p^{j+1} solved A p = b_j to the
+// Fischer's projection of successive right-hand sides: with D_j the last m <= 8
+// pressure increments and W_j = A D_j (= b_j - b_{j-1}: each p^{j+1} solved A p = b_j to the
 // tolerance), the guess p^n + sum_j c_j D_j minimises ||(b_n - b_{n-1}) - sum_j
 // c_j W_j|| = ||b_n - A(p^n + sum c_j D_j)|| up to the tolerance.  One pass forms
 // the right-hand side and the Gram matrix of the W_j (normalised, with a small
 // ridge: successive increments are nearly parallel), the last block solves it.
-constexpr int PROJ_MAX = 4;
+constexpr int PROJ_MAX = 8;
 constexpr int PROJ_SUMS = PROJ_MAX + PROJ_MAX * (PROJ_MAX + 1) / 2;
 
 __global__ void __launch_bounds__(256)
@@ -408,10 +408,11 @@ __global__ void k_proj_push(int nsys, const double *x, const double *pcur, const
     }
 }
 
-__global__ void k_proj_advance(int *state) {
+// the ring holds m pairs
+__global__ void k_proj_advance(int *state, int m) {
     if (state[0] >= 0)
-        state[1] = (state[1] + 1) % PROJ_MAX;
-    state[0] = state[0] < 0 ? 0 : min(state[0] + 1, PROJ_MAX);
+        state[1] = (state[1] + 1) % m;
+    state[0] = state[0] < 0 ? 0 : min(state[0] + 1, m);
 }
 
 // the projected and the learned guesses keep the increment history
@@ -460,11 +461,12 @@ struct mp_fs1_s {
     // pressure history for the extrapolated and learned guesses
     dbuf<double> pcur, ph1, ph2, norms;
     dbuf<double> corr, flt1, flt_scale;  // learned correction and its coarse-level filter
-    // projection guess: the last PROJ_MAX increments D_j = p^{j+1} - p^j, their images
+    // projection guess: the last proj_m increments D_j = p^{j+1} - p^j, their images
     // W_j = A D_j = b_j - b_{j-1}, the previous right-hand side, and on the device the
     // number of valid columns (-1: no previous right-hand side yet), the ring head and
     // the coefficients of the last guess
     dbuf<double> pD, pW, pbprev, pcoef, ppart;
+    int proj_m = 0;    // ring length (pairs kept)
     dbuf<int> pstate;  // [0] valid columns, [1] ring head
     dbuf<unsigned> pticket;
     // learned guess
@@ -600,7 +602,7 @@ static int fs1_issue_post(mp_fs1_s *f, int cur, cudaStream_t s) {
         k_proj_push<<<g, 256, 0, s>>>(ns, f->P.W.x.p, f->pcur.p, f->P.W.b64.p, f->pbprev.p,
                                       f->pD.p, f->pW.p, f->pstate.p);
         MP_CHECK_LAUNCH();
-        k_proj_advance<<<1, 1, 0, s>>>(f->pstate.p);
+        k_proj_advance<<<1, 1, 0, s>>>(f->pstate.p, f->proj_m);
         MP_CHECK_LAUNCH();
     }
     if (f->guess != MP_GUESS_PREVIOUS || f->collect) {
@@ -654,9 +656,11 @@ static int fs1_step_once(mp_fs1_s *f, bool graph, cudaStream_t s) {
 // records its right-hand side)
 static int proj_reserve(mp_fs1 f) {
     const size_t ns = (size_t)f->P.sys.nsys;
-    if (!f->pD.p) {
-        MP_TRY(f->pD.alloc(ns * PROJ_MAX));
-        MP_TRY(f->pW.alloc(ns * PROJ_MAX));
+    const int m = std::min(std::max(f->P.cfg.guess_vectors, 1), PROJ_MAX);
+    if (!f->pD.p || f->proj_m != m) {
+        f->proj_m = m;
+        MP_TRY(f->pD.alloc(ns * m));
+        MP_TRY(f->pW.alloc(ns * m));
         MP_TRY(f->pbprev.alloc(ns));
         MP_TRY(f->pcoef.alloc(PROJ_MAX));
         MP_TRY(f->ppart.alloc((size_t)PROJ_SUMS * sm_count() * 4 + 64));

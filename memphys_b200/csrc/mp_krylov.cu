@@ -129,7 +129,14 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
         S->restarts = 0;
         S->need_restart = 0;
         S->maxit = maxit;
-        S->tol2 = tol * tol * bb;
+        // The inner solve of a refinement sweep (ZERO_X) asks for the smaller of
+        // the sweep's reduction `tol` and half the reduction the outer residual
+        // still needs (at most 2x per sweep): near convergence a sweep then stops
+        // once the outer tolerance is in reach instead of reducing by `tol`.
+        double t2 = tol * tol;
+        if (ZERO_X && S->rr_true > 0.0)
+            t2 = fmax(t2, fmin(0.25 * S->tol_outer2 * S->b64_sq / S->rr_true, 0.25));
+        S->tol2 = t2 * bb;
         S->zero_x = (bb == 0.0);
         int done = (bb == 0.0) || !(rr > S->tol2 && maxit > 0);
         S->status = MP_OK;
@@ -925,6 +932,9 @@ int solver_cfg_check(const mp_solver_cfg &c) {
         return fail(MP_BAD_ARG, "precision must be MP_FP64, MP_FP32 or MP_MG32");
     if (c.precond < MP_PRECOND_NONE || c.precond > MP_PRECOND_AMG)
         return fail(MP_BAD_ARG, "unknown preconditioner %d", c.precond);
+    if (c.guess_vectors < 0 || c.guess_vectors > 8)
+        return fail(MP_BAD_ARG, "guess_vectors must be 1-8 (0 for the default 8), got %d",
+                    c.guess_vectors);
     if (c.precision == MP_MG32 && c.precond != MP_PRECOND_AMG)
         return fail(MP_BAD_ARG, "MP_MG32 stores the multigrid preconditioner in FP32: it needs "
                                 "MP_PRECOND_AMG");
@@ -944,6 +954,7 @@ Cfg Cfg::from(const mp_solver_cfg &c) {
     o.amg_coarse_size = c.amg_coarse_size > 0 ? c.amg_coarse_size : 512;
     o.smoother_sweeps = c.smoother_sweeps > 0 ? c.smoother_sweeps : 1;
     o.cheb_lower = c.cheb_lower > 0 && c.cheb_lower < 1 ? c.cheb_lower : 1.0 / 12.0;
+    o.guess_vectors = c.guess_vectors > 0 ? c.guess_vectors : 8;
     return o;
 }
 
@@ -964,6 +975,7 @@ extern "C" int mp_solver_cfg_default(mp_solver_cfg *c) {
     c->amg_coarse_size = 512;
     c->smoother_sweeps = 1;
     c->cheb_lower = 1.0 / 12.0;
+    c->guess_vectors = 8;
     return MP_OK;
 }
 

@@ -10,7 +10,7 @@ namespace mp {
 struct Cfg {
     double tol, inner_tol, cheb_lower;
     int maxit, precond, precision, guess, max_refine, amg_max_levels, amg_coarse_size,
-        smoother_sweeps;
+        smoother_sweeps, guess_vectors;
     static Cfg from(const mp_solver_cfg &c);
 };
 // MP_OK, or MP_BAD_ARG with the reason for an inconsistent solver configuration
