@@ -245,7 +245,8 @@ __global__ void k_step_log(int *step, const BicgScalars *S, double *log, int cap
                            int nv, int bordered, int mixed) {
     const int s = *step;
     double *e = log + MP_LOG_FIELDS * (size_t)(s % cap);
-    e[0] = mixed ? S->total_inner : S->it;
+    // iterations, a last half iteration counted as 0.5
+    e[0] = mixed ? S->total_inner - 0.5 * S->half_total : S->it - 0.5 * S->half;
     e[1] = S->b64_sq > 0 ? sqrt(S->rr_true / S->b64_sq) : 0.0;
     e[2] = sqrt(S->rr_true);
     e[3] = bordered ? x[nv] : 0.0;

@@ -126,6 +126,7 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
         S->alpha = 1.0;
         S->omega = 1.0;
         S->it = 0;
+        S->half = 0;
         S->restarts = 0;
         S->need_restart = 0;
         S->maxit = maxit;
@@ -330,26 +331,46 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
     }
 }
 
-// s = r - alpha v; z = M^-1 s for the fused preconditioners
+// s = r - alpha v; x += alpha y; z = M^-1 s for the fused preconditioners.
+// ||s||^2 decides the half-step exit: when s already meets the tolerance, x is
+// the solution (x + alpha y) and the iteration stops here, before the second
+// preconditioner application (the later kernels of the sweep see S->done).
 template <class T, int PK>
 __global__ void __launch_bounds__(KT, KT_BLOCKS)
-    k_update_s(int nv, int bordered, const T *r, const T *v, T *s, T *z, const T *dinv,
-               const BicgScalars *S) {
+    k_update_s(int nv, int bordered, const T *r, const T *v, T *s, T *z, const T *dinv, T *x,
+               const T *y, BicgScalars *S, RedBuf R, cudaGraphConditionalHandle h) {
+    KRYLOV_SMEM
     if (S->done)
         return;
     const T al = (T)S->alpha;
+    double acc[1] = {0};
     const int stride = gridDim.x * blockDim.x;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += stride) {
         const T si = r[i] - al * v[i];
         s[i] = si;
         if (PK == PK_JACOBI)
             z[i] = dinv[i] * si;
+        x[i] = x[i] + al * y[i];
+        acc[0] += (double)si * si;
     }
-    if (bordered && blockIdx.x == 0 && threadIdx.x == 0) {
-        const T si = r[nv] - al * v[nv];
-        s[nv] = si;
-        if (PK != PK_NONE)
-            z[nv] = si;
+    if (grid_reduce<1>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
+        double ss = acc[0];
+        if (bordered) {
+            const T si = r[nv] - al * v[nv];
+            s[nv] = si;
+            if (PK != PK_NONE)
+                z[nv] = si;
+            x[nv] = x[nv] + al * y[nv];
+            ss += (double)si * si;
+        }
+        if (ss <= S->tol2) {  // converged at the half step (NaN compares false)
+            S->rr = ss;
+            S->it += 1;
+            S->half = 1;
+            S->done = 1;
+            if (h)
+                cudaGraphSetConditional(h, 0u);
+        }
     }
 }
 
@@ -396,19 +417,20 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
     }
 }
 
-// x += alpha y + omega z; r = s - omega t; convergence test for the next sweep
+// x += omega z (alpha y was added with s); r = s - omega t; convergence test for
+// the next sweep
 template <class T>
 __global__ void __launch_bounds__(KT, KT_BLOCKS)
-    k_update_xr(int nsys, T *x, const T *y, const T *z, const T *s, const T *t, T *r, const T *r0,
+    k_update_xr(int nsys, T *x, const T *z, const T *s, const T *t, T *r, const T *r0,
                 BicgScalars *S, RedBuf R, cudaGraphConditionalHandle h) {
     KRYLOV_SMEM
     if (S->done)
         return;
-    const T al = (T)S->alpha, om = (T)S->omega;
+    const T om = (T)S->omega;
     double acc[2] = {0, 0};
     const int stride = gridDim.x * blockDim.x;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += stride) {
-        x[i] = x[i] + (al * y[i] + om * z[i]);
+        x[i] = x[i] + om * z[i];
         const T ri = s[i] - om * t[i];
         r[i] = ri;
         acc[0] += (double)ri * ri;
@@ -521,6 +543,7 @@ __global__ void k_ir_update(int nsys, double *x, const float *e32, BicgScalars *
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         S->outer_it += 1;
         S->total_inner += S->it;
+        S->half_total += S->half;
     }
 }
 
@@ -640,17 +663,20 @@ static int issue_iteration(const PpeSystem &P, const EllView<T> &A, const T *din
     k_spmv_alpha<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, yy, v, r0, S, R);
     MP_CHECK_LAUNCH();
     if (pk == PK_JACOBI)
-        k_update_s<T, PK_JACOBI><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, S);
+        k_update_s<T, PK_JACOBI><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, x, yy,
+                                                                S, R, h);
     else if (pk == PK_NONE)
-        k_update_s<T, PK_NONE><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, S);
+        k_update_s<T, PK_NONE><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, x, yy, S,
+                                                              R, h);
     else
-        k_update_s<T, PK_EXTERNAL><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, S);
+        k_update_s<T, PK_EXTERNAL><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, x,
+                                                                  yy, S, R, h);
     MP_CHECK_LAUNCH();
     if (pk == PK_EXTERNAL)
         MP_TRY(amg_apply<T>(*P.amg, s_, zz, &S->done, st));
     k_spmv_omega<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, zz, t, s_, S, R);
     MP_CHECK_LAUNCH();
-    k_update_xr<T><<<vec_blocks(nsys), KT, 0, st>>>(nsys, x, yy, zz, s_, t, r, r0, S, R, h);
+    k_update_xr<T><<<vec_blocks(nsys), KT, 0, st>>>(nsys, x, zz, s_, t, r, r0, S, R, h);
     MP_CHECK_LAUNCH();
     return MP_OK;
 }
@@ -716,6 +742,7 @@ __global__ void k_ir_setup(BicgScalars *S, double tol, int outer_max) {
     S->outer_it = 0;
     S->outer_max = outer_max;
     S->total_inner = 0;
+    S->half_total = 0;
     S->status = MP_OK;
 }
 

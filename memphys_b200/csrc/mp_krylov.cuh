@@ -25,9 +25,11 @@ struct BicgScalars {
     double dot_rv, dot_tt, dot_ts;
     double scale;       // mixed precision: norm of the FP64 residual being solved for
     double rr_true;     // ||b - A x||^2 recomputed in FP64
-    int it, maxit, restarts, need_restart, done, status, zero_x, pad;
-    // iterative refinement (outer) state
-    int outer_it, outer_max, outer_done, total_inner;
+    int it, maxit, restarts, need_restart, done, status, zero_x;
+    int half;  // 1 when the solve stopped after the first half of its last iteration
+    // iterative refinement (outer) state; half_total counts the inner solves that
+    // stopped after a half iteration
+    int outer_it, outer_max, outer_done, total_inner, half_total;
     double tol_outer2, b64_sq;
     double relres0;     // ||b - A x0|| / ||b|| of the initial guess (first residual of a solve)
     double guess_theta; // weight of the learned correction in the last initial guess
