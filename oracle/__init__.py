@@ -78,6 +78,8 @@ def lib():
                                   C.POINTER(C.c_double)]
         L.mo_fs1_destroy.argtypes = [C.c_void_p]
         L.mo_fs1_destroy.restype = None
+        L.mo_set_threads.argtypes = [C.c_int]
+        L.mo_set_threads.restype = C.c_int
         _lib = L
     return _lib
 
@@ -87,6 +89,12 @@ def _ptr(a):
 
 
 # ---------------------------------------------------------------- parameters
+def set_threads(n: int) -> int:
+    """Threads of the oracle's row-parallel loops (OpenMP); returns the previous
+    count.  Dot products and ILUT solves stay serial, so results do not change."""
+    return lib().mo_set_threads(int(n))
+
+
 def num_poly_terms(dim: int, poly_deg: int) -> int:
     """parameters.cpp:122-130."""
     return lib().mo_num_poly_terms(dim, poly_deg)

@@ -22,6 +22,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <pthread.h>
 
 /* ------------------------------------------------------------------ */
 /* parameters.cpp:122-130 -- number of appended monomials and cloud size */
@@ -641,16 +642,90 @@ int mo_knn_stencils(const double *xyz, const unsigned char *bflag, int nv, int d
 }
 
 /* ------------------------------------------------------------------ */
+/* Row-parallel loops on host threads (pthreads): the rows [0, n) are split into
+ * one contiguous range per thread; every row is computed exactly as in the
+ * serial loop, so results do not depend on the thread count.  Dot products and
+ * the ILUT triangular solves stay serial, as in Eigen. */
+static int g_threads = 1;
+#define MO_MAX_THREADS 128
+
+typedef void (*mo_rows_fn)(void *ctx, int lo, int hi);
+typedef struct {
+    mo_rows_fn fn;
+    void *ctx;
+    int lo, hi;
+} mo_rows_job;
+
+static void *mo_rows_worker(void *a)
+{
+    mo_rows_job *j = (mo_rows_job *)a;
+    j->fn(j->ctx, j->lo, j->hi);
+    return NULL;
+}
+
+static void par_rows(int n, mo_rows_fn fn, void *ctx)
+{
+    int T = g_threads;
+    if (T > n / 2048)
+        T = n / 2048;
+    if (T <= 1) {
+        fn(ctx, 0, n);
+        return;
+    }
+    pthread_t th[MO_MAX_THREADS];
+    int started[MO_MAX_THREADS];
+    mo_rows_job job[MO_MAX_THREADS];
+    const int chunk = (n + T - 1) / T;
+    for (int t = 0; t < T; t++) {
+        job[t].fn = fn;
+        job[t].ctx = ctx;
+        job[t].lo = t * chunk < n ? t * chunk : n;
+        job[t].hi = (t + 1) * chunk < n ? (t + 1) * chunk : n;
+        started[t] = t > 0 && pthread_create(&th[t], NULL, mo_rows_worker, &job[t]) == 0;
+    }
+    fn(ctx, job[0].lo, job[0].hi);
+    for (int t = 1; t < T; t++) {
+        if (started[t])
+            pthread_join(th[t], NULL);
+        else
+            fn(ctx, job[t].lo, job[t].hi); /* no thread: run the range here */
+    }
+}
+
+/* Threads of the row-parallel loops (SpMV rows, fractional-step row loops);
+ * returns the previous count. */
+int mo_set_threads(int n)
+{
+    const int old = g_threads;
+    if (n > 0)
+        g_threads = n < MO_MAX_THREADS ? n : MO_MAX_THREADS;
+    return old;
+}
+
+/* ------------------------------------------------------------------ */
 /* CSR helpers */
+typedef struct {
+    const int *rp, *ci;
+    const double *val, *x;
+    double *y;
+} mo_spmv_ctx;
+
+static void spmv_rows(void *c, int lo, int hi)
+{
+    const mo_spmv_ctx *a = (const mo_spmv_ctx *)c;
+    for (int i = lo; i < hi; i++) {
+        double s = 0.0;
+        for (int k = a->rp[i]; k < a->rp[i + 1]; k++)
+            s += a->val[k] * a->x[a->ci[k]];
+        a->y[i] = s;
+    }
+}
+
 void mo_spmv_csr(int nrows, const int *rp, const int *ci, const double *val, const double *x,
                  double *y)
 {
-    for (int i = 0; i < nrows; i++) {
-        double s = 0.0;
-        for (int k = rp[i]; k < rp[i + 1]; k++)
-            s += val[k] * x[ci[k]];
-        y[i] = s;
-    }
+    mo_spmv_ctx c = {rp, ci, val, x, y};
+    par_rows(nrows, spmv_rows, &c);
 }
 
 /*
@@ -1075,20 +1150,69 @@ static double row_dot(const mo_fs1 *f, const double *w, int iv, const double *x)
  * from time level n to n+1.  it = timestep index (Euler at it == 0).
  * Returns BiCGSTAB iterations; relres = recomputed ||A p - b|| / ||b||.
  */
+/* the row loops of one step, split over threads by par_rows */
+typedef struct {
+    const mo_fs1 *f;
+    double **vel;
+    double *p;
+    int d;
+} mo_step_ctx;
+
+static void vel_src_rows(void *c, int lo, int hi)
+{
+    const mo_step_ctx *a = (const mo_step_ctx *)c;
+    const mo_fs1 *f = a->f;
+    const double *q = a->vel[a->d];
+    for (int i = lo; i < hi; i++) {
+        double conv = 0.0;
+        for (int k = 0; k < f->dim; k++)
+            conv += a->vel[k][i] * row_dot(f, f->g[k], i, q);
+        double src = f->rho * (-conv) + f->mu * row_dot(f, f->lap, i, q);
+        f->src_old[a->d][i] = src;
+    }
+}
+
+static void p_rhs_rows(void *c, int lo, int hi)
+{
+    const mo_step_ctx *a = (const mo_step_ctx *)c;
+    const mo_fs1 *f = a->f;
+    const int dim = f->dim;
+    for (int i = lo; i < hi; i++) {
+        if (!f->bflag[i]) {
+            double s = 0.0;
+            for (int d = 0; d < dim; d++)
+                s += row_dot(f, f->g[d], i, f->hat[d]);
+            f->psrc[i] = s * f->rho / f->dt;
+        } else if (f->pdir[i]) {
+            f->psrc[i] = a->p[i];
+        } else {
+            double s = 0.0;
+            for (int d = 0; d < dim; d++)
+                s += (a->vel[d][i] - f->hat[d][i]) * f->normal[dim * i + d];
+            f->psrc[i] = -f->rho * s / f->dt;
+        }
+    }
+}
+
+static void vel_corr_rows(void *c, int lo, int hi)
+{
+    const mo_step_ctx *a = (const mo_step_ctx *)c;
+    const mo_fs1 *f = a->f;
+    double *q = a->vel[a->d];
+    for (int i = lo; i < hi; i++)
+        q[i] = f->hat[a->d][i] - f->dt * row_dot(f, f->g[a->d], i, a->p) / f->rho;
+}
+
 int mo_fs1_step(mo_fs1 *f, double **vel, double *p, int it, double *relres)
 {
     int nv = f->nv, dim = f->dim;
-    double rho = f->rho, mu = f->mu, dt = f->dt;
+    double rho = f->rho, dt = f->dt;
+    mo_step_ctx ctx = {f, vel, p, 0};
     /* calc_vel_hat :120-134 */
     for (int d = 0; d < dim; d++) {
         const double *q = vel[d];
-        for (int i = 0; i < nv; i++) {
-            double conv = 0.0;
-            for (int k = 0; k < dim; k++)
-                conv += vel[k][i] * row_dot(f, f->g[k], i, q);
-            double src = rho * (-conv) + mu * row_dot(f, f->lap, i, q);
-            f->src_old[d][i] = src;
-        }
+        ctx.d = d;
+        par_rows(nv, vel_src_rows, &ctx);
         for (int i = 0; i < nv; i++) {
             if (f->temporal_order == 1 || it == 0)
                 f->hat[d][i] = q[i] + (dt / rho) * f->src_old[d][i];
@@ -1097,21 +1221,7 @@ int mo_fs1_step(mo_fs1 *f, double **vel, double *p, int it, double *relres)
         }
     }
     /* calc_pressure :136-151 */
-    for (int i = 0; i < nv; i++) {
-        if (!f->bflag[i]) {
-            double s = 0.0;
-            for (int d = 0; d < dim; d++)
-                s += row_dot(f, f->g[d], i, f->hat[d]);
-            f->psrc[i] = s * rho / dt;
-        } else if (f->pdir[i]) {
-            f->psrc[i] = p[i];
-        } else {
-            double s = 0.0;
-            for (int d = 0; d < dim; d++)
-                s += (vel[d][i] - f->hat[d][i]) * f->normal[dim * i + d];
-            f->psrc[i] = -rho * s / dt;
-        }
-    }
+    par_rows(nv, p_rhs_rows, &ctx);
     if (f->nsys == nv + 1)
         f->psrc[nv] = 0.0;
     int iters = mo_bicgstab(f->nsys, f->rp, f->ci, f->val, f->ilu, f->psrc, p, f->tol, f->maxit,
@@ -1121,8 +1231,8 @@ int mo_fs1_step(mo_fs1 *f, double **vel, double *p, int it, double *relres)
         double *q = vel[d];
         for (int i = 0; i < nv; i++)
             f->tmp[i] = q[i]; /* u_old for Dirichlet copies */
-        for (int i = 0; i < nv; i++)
-            q[i] = f->hat[d][i] - dt * row_dot(f, f->g[d], i, p) / rho;
+        ctx.d = d;
+        par_rows(nv, vel_corr_rows, &ctx);
         for (int i = 0; i < nv; i++) {
             if (!f->bflag[i] || f->pdir[i])
                 continue;

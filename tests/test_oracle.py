@@ -207,3 +207,26 @@ def test_fs1_oracles_agree():
     for d in range(2):
         assert np.abs(va[d] - vb[d]).max() <= 1e-9 * np.abs(vb[d]).max()
     assert np.abs(pa - pb).max() <= 1e-7 * np.abs(pb).max()
+
+
+def test_oracle_threads_do_not_change_results():
+    # the row-parallel loops (SpMV rows, fractional-step row loops) compute every
+    # row as the serial loop does; dot products and ILUT solves stay serial
+    cl = clouds.cavity_2d(64, seed=5)
+    nb = oracle.knn_stencils(cl.xyz, cl.boundary, 20)
+    w = oracle.cloud_weights(cl.xyz, nb, 3, 3, cond=False)
+    out = []
+    prev = oracle.set_threads(1)
+    try:
+        for threads in (1, 4):
+            oracle.set_threads(threads)
+            f = oracle.FS1(cl, nb, w, 1.0, 0.01, 1e-4, 2, 1e-8, 30, 1e-6, 50)
+            vel = [cl.vel_bc[0].copy(), cl.vel_bc[1].copy()]
+            p = np.zeros(f.nsys)
+            for it in range(3):
+                f.step(vel, p, it)
+            out.append((vel[0], vel[1], p))
+    finally:
+        oracle.set_threads(prev)
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
