@@ -100,6 +100,25 @@ int mp_knn_stencils_noalloc(const double *xyz, const uint8_t *boundary, int nv, 
                             int *nb_col, mp_stream s);
 
 /*
+ * Node orderings.  order[i] = new index of node i (a permutation of 0..nv-1).
+ * mp_order_rcm: CLOUD::re_order_points_reverse_cuthill_mckee (cloud.cpp:315-335)
+ *   = reverse_cuthill_mckee_ordering (general_functions.cpp:806-879) on the
+ *   stencil graph nb (nv x n), the order CLOUD::CLOUD applies (cloud.cpp:37);
+ *   host computation (a breadth-first search), host or device pointers.
+ * mp_order_morton: GPU Z-order of the points (no reference counterpart; the
+ *   locality of RCM without its sequential search).
+ * mp_permute_stencils: CLOUD::re_order_points (cloud.cpp:337-439) on a stencil
+ *   table: nb_out row order[i] = row i with every member j replaced by order[j].
+ * mp_permute_rows: out row order[i] = in row i, row_bytes bytes per row (points,
+ *   normals, flags, weights).  in and out must not alias.
+ */
+int mp_order_rcm(const int *nb, int nv, int n, int *order);
+int mp_order_morton(const double *xyz, int nv, int dim, int *order, mp_stream s);
+int mp_permute_stencils(const int *nb, int nv, int n, const int *order, int *nb_out, mp_stream s);
+int mp_permute_rows(const void *in, void *out, int nv, int row_bytes, const int *order,
+                    mp_stream s);
+
+/*
  * PHS-RBF-FD weights of every stencil of a cloud, replacing the loop of
  * CLOUD::calc_grad_laplace_coeffs (cloud.cpp:207-279) over
  * calc_PHS_RBF_grad_laplace_single_vert (coefficient_computations.cpp:294-328).

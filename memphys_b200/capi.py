@@ -34,6 +34,7 @@ EXPORTS = [
     "mp_free_host", "mp_memcpy", "mp_memset", "mp_stream_create", "mp_stream_destroy",
     "mp_stream_sync", "mp_timer_start", "mp_timer_stop", "mp_profiler", "mp_launch_count", "mp_num_poly_terms",
     "mp_cloud_size", "mp_poly_exponents", "mp_knn_stencils", "mp_knn_stencils_noalloc",
+    "mp_order_rcm", "mp_order_morton", "mp_permute_stencils", "mp_permute_rows",
     "mp_stencil_weights",
     "mp_stencil_weights_batched", "mp_cloud_create", "mp_cloud_create_stencils", "mp_cloud_info",
     "mp_cloud_get", "mp_cloud_destroy", "mp_op_create_ell", "mp_op_from_cloud", "mp_op_apply",
@@ -90,6 +91,9 @@ def lib() -> C.CDLL:
             "mp_num_poly_terms": [i, i], "mp_cloud_size": [i, i, d], "mp_poly_exponents": [i, i, vp],
             "mp_knn_stencils": [vp, vp, i, i, i, vp, vp],
             "mp_knn_stencils_noalloc": [vp, vp, i, i, i, vp, vp],
+            "mp_order_rcm": [vp, i, i, vp], "mp_order_morton": [vp, i, i, vp, vp],
+            "mp_permute_stencils": [vp, i, i, vp, vp, vp],
+            "mp_permute_rows": [vp, vp, i, i, vp, vp],
             "mp_stencil_weights": [vp, i, i, vp, i, i, i, vp, vp, vp, vp, vp, vp],
             "mp_stencil_weights_batched": [i, vp, vp, vp, i, i, i, vp, vp, vp],
             "mp_cloud_create": [vp, vp, i, i, i, i, d, i, vp, C.POINTER(vp)],

@@ -118,15 +118,64 @@ class POINTS:
         self.xyz = np.ascontiguousarray(cloud.xyz, np.float64)
         self.boundary_flag = np.ascontiguousarray(cloud.boundary, np.uint8)
         self.normal = np.ascontiguousarray(cloud.normal, np.float64)
+        self.order = None  # new index of every input node once a CLOUD reorders them
+
+    def permute(self, a: np.ndarray) -> np.ndarray:
+        """A per-node array of the input order in this POINTS' current order."""
+        a = np.asarray(a)
+        if self.order is None:
+            return a
+        out = np.empty_like(a)
+        out[self.order] = a
+        return out
+
+    def _reorder(self, order: np.ndarray):
+        # re_order_points (cloud.cpp:337-439): coordinates, normals and flags move to
+        # their new rows on the GPU
+        order = np.ascontiguousarray(order, np.int32)
+        L = capi.lib()
+        for name in ("xyz", "normal", "boundary_flag"):
+            a = np.ascontiguousarray(getattr(self, name))
+            out = np.empty_like(a)
+            row = a.nbytes // self.nv
+            check(L.mp_permute_rows(ptr(a), ptr(out), self.nv, row, ptr(order), None),
+                  "mp_permute_rows")
+            setattr(self, name, out)
+        self.order = order if self.order is None else order[self.order]
 
 
 class CLOUD:
     """CLOUD::CLOUD (cloud.cpp:29-48) on the GPU: stencils, weights, operators."""
 
     def __init__(self, points: POINTS, parameters: PARAMETERS, compute_cond: bool = True,
-                 nb_col: np.ndarray | None = None):
+                 nb_col: np.ndarray | None = None, reorder: str | None = None):
+        """reorder: None keeps the input order; "rcm" renumbers the points and stencils
+        by reverse Cuthill-McKee as the reference's constructor always does
+        (cloud.cpp:37, mp_order_rcm); "morton" by the GPU Z-order (mp_order_morton).
+        Reordering permutes `points` in place (points.order, points.permute)."""
         self.points = points
         h = C.c_void_p()
+        if reorder is not None:
+            if reorder not in ("rcm", "morton"):
+                raise ValueError(f"reorder must be None, 'rcm' or 'morton', not {reorder!r}")
+            L = capi.lib()
+            if nb_col is None:
+                n = L.mp_cloud_size(points.dim, parameters.poly_deg,
+                                    C.c_double(parameters.cloud_size_multiplier))
+                nb_col = np.zeros((points.nv, n), np.int32)
+                check(L.mp_knn_stencils(ptr(points.xyz), ptr(points.boundary_flag), points.nv,
+                                        points.dim, n, ptr(nb_col), None), "mp_knn_stencils")
+            nb = np.ascontiguousarray(nb_col, np.int32)
+            order = np.zeros(points.nv, np.int32)
+            if reorder == "rcm":
+                check(L.mp_order_rcm(ptr(nb), points.nv, nb.shape[1], ptr(order)), "mp_order_rcm")
+            else:
+                check(L.mp_order_morton(ptr(points.xyz), points.nv, points.dim, ptr(order), None),
+                      "mp_order_morton")
+            nb_col = np.zeros_like(nb)
+            check(L.mp_permute_stencils(ptr(nb), points.nv, nb.shape[1], ptr(order), ptr(nb_col),
+                                        None), "mp_permute_stencils")
+            points._reorder(order)
         if nb_col is None:
             rc = capi.lib().mp_cloud_create(ptr(points.xyz), ptr(points.boundary_flag), points.nv,
                                             points.dim, parameters.phs_deg, parameters.poly_deg,

@@ -182,6 +182,39 @@ def batched_weights(sizes, offsets, pts, dim, phs=3, poly_deg=3, cond=False):
 
 
 # ---------------------------------------------------------------- operators
+def rcm_order(nb_col: np.ndarray) -> np.ndarray:
+    """reverse_cuthill_mckee_ordering (general_functions.cpp:806-879) on the stencil
+    graph, as CLOUD::re_order_points_reverse_cuthill_mckee builds it (cloud.cpp:315-335):
+    adjacency of node i = its stencil row; breadth-first from the first node of least
+    degree, each node's unvisited neighbours appended sorted by (degree, index); then
+    order[i] = nv - 1 - position.  Pure Python: small clouds only."""
+    nb = np.asarray(nb_col)
+    nv = nb.shape[0]
+    degree = [len(row) for row in nb]
+    visited = [False] * nv
+    start = min(range(nv), key=lambda i: (degree[i], i))
+    numbering = [start]
+    visited[start] = True
+    index = 0
+    while len(numbering) < nv:
+        if index == len(numbering):  # not reached from the start (the reference reads past)
+            nxt = min((i for i in range(nv) if not visited[i]), key=lambda i: (degree[i], i))
+            visited[nxt] = True
+            numbering.append(nxt)
+        v = numbering[index]
+        index += 1
+        fresh = []
+        for w in nb[v]:
+            w = int(w)
+            if not visited[w]:
+                visited[w] = True
+                fresh.append((degree[w], w))
+        numbering.extend(w for _, w in sorted(fresh))
+    order = np.empty(nv, np.int32)
+    order[np.asarray(numbering)] = np.arange(nv, dtype=np.int32)
+    return (nv - 1 - order).astype(np.int32)
+
+
 def ell_to_csr(nb_col: np.ndarray):
     nv, n = nb_col.shape
     return np.arange(nv + 1, dtype=np.int32) * n, np.ascontiguousarray(nb_col.ravel(), np.int32)
