@@ -297,6 +297,41 @@ int mp_fs1_log(mp_fs1 f, int first, int count, double *out);
 int mp_fs1_kernel_counts(mp_fs1 f, int *fixed, int *per_sweep, int *per_refine);
 int mp_fs1_destroy(mp_fs1 f);
 
+/* ------------------------------------------- semi-implicit split solver */
+/*
+ * SEMI_IMPLICIT_SPLIT_SOLVER (semi_implicit_split_solver.cpp, 2D): BDF2 implicit
+ * velocity with outer iterations of velocity solve -> pressure correction ->
+ * velocity correction until the L1 change of (u, v) is <= iterative_tolerance or
+ * n_outer_iter iterations ran (single_timestep_2d :376-421).  vel_solver solves
+ * the velocity matrices, which change every outer iteration (MP_PRECOND_JACOBI or
+ * MP_PRECOND_NONE, MP_FP64); p_solver the pressure correction (any).
+ * precond_freq_it is accepted for the reference's signature: the Jacobi
+ * preconditioner is rebuilt at every outer iteration.
+ */
+typedef struct mp_sis_s *mp_sis;
+typedef struct {
+    double rho, mu, dt;
+    int n_outer_iter;
+    double iterative_tolerance;
+    int precond_freq_it;
+} mp_sis_cfg;
+int mp_sis_create(mp_cloud c, const uint8_t *boundary, const double *normal,
+                  const uint8_t *u_dir, const uint8_t *v_dir, const uint8_t *p_dir,
+                  const mp_sis_cfg *cfg, const mp_solver_cfg *vel_solver,
+                  const mp_solver_cfg *p_solver, mp_sis *out);
+/* nv + 1 when the pressure is full Neumann (bordered), else nv */
+int mp_sis_system_size(mp_sis s, int *nsys);
+/* solves launched as CUDA graphs (1, default) or kernel by kernel (0) */
+int mp_sis_set_graph(mp_sis s, int use_graph);
+/* single_timestep_2d (:376-421): vel_old = {u_old, v_old} (nv each), p_old
+ * (system size) -> vel_new, p_new; it = timestep index (BDF1 at 0); the solver
+ * keeps u_old, v_old of the call for the next BDF2 step.  Host or device
+ * pointers.  Returns the outer iterations run and the last L1 / max changes. */
+int mp_sis_single_timestep(mp_sis s, const double *const *vel_old, const double *p_old,
+                           double *const *vel_new, double *p_new, int it, int *n_outer,
+                           double *l1_err, double *max_err, mp_stream stream);
+int mp_sis_destroy(mp_sis s);
+
 /* ------------------------------------------------------- learned guess */
 /*
  * Per-node network predicting the pressure increment of a fractional step

@@ -35,6 +35,8 @@ EXPORTS = [
     "mp_stream_sync", "mp_timer_start", "mp_timer_stop", "mp_profiler", "mp_launch_count", "mp_num_poly_terms",
     "mp_cloud_size", "mp_poly_exponents", "mp_knn_stencils", "mp_knn_stencils_noalloc",
     "mp_order_rcm", "mp_order_morton", "mp_permute_stencils", "mp_permute_rows",
+    "mp_sis_create", "mp_sis_system_size", "mp_sis_set_graph", "mp_sis_single_timestep",
+    "mp_sis_destroy",
     "mp_stencil_weights",
     "mp_stencil_weights_batched", "mp_cloud_create", "mp_cloud_create_stencils", "mp_cloud_info",
     "mp_cloud_get", "mp_cloud_destroy", "mp_op_create_ell", "mp_op_from_cloud", "mp_op_apply",
@@ -52,6 +54,12 @@ class MemphysError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
         self.status = status
+
+
+class SisCfg(C.Structure):
+    _fields_ = [("rho", C.c_double), ("mu", C.c_double), ("dt", C.c_double),
+                ("n_outer_iter", C.c_int), ("iterative_tolerance", C.c_double),
+                ("precond_freq_it", C.c_int)]
 
 
 class SolverCfg(C.Structure):
@@ -94,6 +102,11 @@ def lib() -> C.CDLL:
             "mp_order_rcm": [vp, i, i, vp], "mp_order_morton": [vp, i, i, vp, vp],
             "mp_permute_stencils": [vp, i, i, vp, vp, vp],
             "mp_permute_rows": [vp, vp, i, i, vp, vp],
+            "mp_sis_create": [vp, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(vp)],
+            "mp_sis_system_size": [vp, C.POINTER(i)], "mp_sis_set_graph": [vp, i],
+            "mp_sis_single_timestep": [vp, vp, vp, vp, vp, i, C.POINTER(i), C.POINTER(d),
+                                       C.POINTER(d), vp],
+            "mp_sis_destroy": [vp],
             "mp_stencil_weights": [vp, i, i, vp, i, i, i, vp, vp, vp, vp, vp, vp],
             "mp_stencil_weights_batched": [i, vp, vp, vp, i, i, i, vp, vp, vp],
             "mp_cloud_create": [vp, vp, i, i, i, i, d, i, vp, C.POINTER(vp)],

@@ -875,9 +875,18 @@ int Ppe::read_stats(cudaStream_t st, SolveStats *out) {
     return MP_OK;
 }
 
+int Ppe::refresh_diag(cudaStream_t st) {
+    if (sys.amg)
+        return fail(MP_BAD_ARG, "refresh_diag: the multigrid hierarchy would be stale");
+    k_jacobi_dinv<<<(sys.nv + 255) / 256, 256, 0, st>>>(sys.A.view64(), sys.dinv.p,
+                                                       sys.dinv32.p ? sys.dinv32.p : nullptr);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
 int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet,
                 const double *normal, double unsteady, double conv, double diff,
-                const mp_solver_cfg &cfg_in, cudaStream_t st) {
+                const mp_solver_cfg &cfg_in, cudaStream_t st, int border_rule) {
     cfg = Cfg::from(cfg_in);
     CloudView cv = cloud_view(c);
     const int nv = cv.nv, K = cv.n, dim = cv.dim;
@@ -885,12 +894,10 @@ int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet
     std::vector<uint8_t> hb(nv), hd(nv);
     MP_CUDA(cudaMemcpy(hb.data(), boundary, nv, cudaMemcpyDefault));
     MP_CUDA(cudaMemcpy(hd.data(), dirichlet, nv, cudaMemcpyDefault));
-    int bordered = 1;
-    for (int i = 0; i < nv; i++)
-        if (hb[i] && hd[i]) {
+    int bordered = border_rule;
+    for (int i = 0; i < nv && bordered; i++)
+        if (hb[i] && hd[i])
             bordered = 0;
-            break;
-        }
     sys.nv = nv;
     sys.K = K;
     sys.bordered = bordered;

@@ -40,9 +40,14 @@ struct Ppe {
     std::shared_ptr<Ell> shared_cols;
     cudaStream_t capture_stream = nullptr;
     ~Ppe();
+    // border_rule 1: bordered unless a boundary node is Dirichlet (solver.cpp:29-38);
+    // 0: never bordered (systems with a nonsingular diagonal, e.g. implicit velocity)
     int create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet,
                const double *normal, double unsteady, double conv, double diff,
-               const mp_solver_cfg &cfg, cudaStream_t st);
+               const mp_solver_cfg &cfg, cudaStream_t st, int border_rule = 1);
+    // after the operator's values changed in place: the Jacobi diagonal again
+    // (systems without a multigrid hierarchy only)
+    int refresh_diag(cudaStream_t st);
     int pk() const {
         return cfg.precond == MP_PRECOND_AMG ? PK_EXTERNAL
                                              : (cfg.precond == MP_PRECOND_JACOBI ? PK_JACOBI : PK_NONE);

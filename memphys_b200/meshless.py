@@ -413,6 +413,75 @@ class FRACTIONAL_STEP_1:
             pass
 
 
+class SEMI_IMPLICIT_SPLIT_SOLVER:
+    """SEMI_IMPLICIT_SPLIT_SOLVER (semi_implicit_split_solver.cpp:22-50, 2D) on the GPU
+    (mp_sis_*).  The velocity matrices are solved by BiCGSTAB with a Jacobi
+    preconditioner rebuilt at every outer iteration (to the parameters' tolerance);
+    the pressure correction by the solver type's configuration."""
+
+    def __init__(self, points: POINTS, cloud: CLOUD, parameters: PARAMETERS, u_dirichlet_flag,
+                 v_dirichlet_flag, p_dirichlet_flag, n_outer_iter: int,
+                 iterative_tolerance: float, precond_freq_it: int, use_graph: bool = True,
+                 **p_cfg):
+        if parameters.dt is None or parameters.rho < 0 or parameters.mu < 0:  # check_bc :65-70
+            raise capi.MemphysError(capi.MP_BAD_ARG, "set parameters.rho, mu and dt first")
+        cfg = capi.SisCfg(parameters.rho, parameters.mu, parameters.dt, int(n_outer_iter),
+                          float(iterative_tolerance), int(precond_freq_it))
+        vel = parameters.solver_cfg(precond=capi.MP_PRECOND_JACOBI, precision=capi.MP_FP64)
+        pc = parameters.solver_cfg(**p_cfg)
+        flags = [np.ascontiguousarray(f, np.uint8) for f in
+                 (u_dirichlet_flag, v_dirichlet_flag, p_dirichlet_flag)]
+        h = C.c_void_p()
+        check(capi.lib().mp_sis_create(cloud.handle, ptr(points.boundary_flag), ptr(points.normal),
+                                       ptr(flags[0]), ptr(flags[1]), ptr(flags[2]), C.byref(cfg),
+                                       C.byref(vel), C.byref(pc), C.byref(h)), "mp_sis_create")
+        self.handle = h
+        self.cloud = cloud
+        ns = C.c_int()
+        check(capi.lib().mp_sis_system_size(h, C.byref(ns)))
+        self.system_size = ns.value
+        self.nv = points.nv
+        check(capi.lib().mp_sis_set_graph(h, int(use_graph)))
+
+    def single_timestep_2d(self, u_new, v_new, p_new, u_old, v_old, p_old, it,
+                           n_outer_iter_log=None, iterative_l1_err_log=None,
+                           iterative_max_err_log=None):
+        """single_timestep_2d (:376-421): the new fields into u_new, v_new, p_new
+        (arrays of nv, nv and system_size entries, written in place); the logs, when
+        given, get the outer iterations and the last L1 / max changes appended."""
+        ns = self.system_size
+        uo, vo = (np.ascontiguousarray(a, np.float64) for a in (u_old, v_old))
+        po = np.ascontiguousarray(p_old, np.float64)
+        if po.shape[0] != ns:  # :380-383
+            po = np.zeros(ns)
+        for a, m in ((u_new, self.nv), (v_new, self.nv), (p_new, ns)):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.shape == (m,)
+                    and a.flags.c_contiguous):
+                raise capi.MemphysError(capi.MP_BAD_ARG, "u_new, v_new, p_new: float64 arrays of "
+                                                    f"{self.nv}, {self.nv}, {ns} entries")
+        vin = (C.c_void_p * 2)(uo.ctypes.data, vo.ctypes.data)
+        vout = (C.c_void_p * 2)(u_new.ctypes.data, v_new.ctypes.data)
+        n, l1, mx = C.c_int(), C.c_double(), C.c_double()
+        check(capi.lib().mp_sis_single_timestep(self.handle, vin, ptr(po), vout, ptr(p_new),
+                                                int(it), C.byref(n), C.byref(l1), C.byref(mx),
+                                                None), "mp_sis_single_timestep")
+        if n_outer_iter_log is not None:
+            n_outer_iter_log.append(n.value)
+        if iterative_l1_err_log is not None:
+            iterative_l1_err_log.append(l1.value)
+        if iterative_max_err_log is not None:
+            iterative_max_err_log.append(mx.value)
+        return n.value, l1.value, mx.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                capi.lib().mp_sis_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
 class MLP:
     """The learned pressure-increment network (mp_mlp): 64 -> 128 -> 128 -> 128 -> 1."""
 
