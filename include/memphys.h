@@ -332,6 +332,26 @@ int mp_sis_single_timestep(mp_sis s, const double *const *vel_old, const double 
                            double *l1_err, double *max_err, mp_stream stream);
 int mp_sis_destroy(mp_sis s);
 
+/*
+ * IMPLICIT_SCALAR_TRANSPORT_SOLVER (implicit_scalar_transport_solver.cpp, 2D):
+ * unsteady dphi/dt + conv (u . grad) phi + diff L phi with the reference's
+ * coefficient convention (interior rows diff L + conv (u_i Gx + v_i Gy) +
+ * a1 unsteady I, a1 = 1 at it = 0 else 1.5), boundary rows identity
+ * (Dirichlet) or n . G; one solve per step from phi_old (Jacobi or no
+ * preconditioner, MP_FP64).  precond_freq_it is accepted for the signature.
+ */
+typedef struct mp_ist_s *mp_ist;
+int mp_ist_create(mp_cloud c, const uint8_t *boundary, const double *normal,
+                  const uint8_t *dirichlet, int precond_freq_it, double unsteady_coeff,
+                  double conv_coeff, double diff_coeff, const mp_solver_cfg *solver, mp_ist *out);
+int mp_ist_set_graph(mp_ist s, int use_graph);
+/* single_timestep_2d (:136-174): phi_old, u_new, v_new (nv each) -> phi_new;
+ * keeps phi_old for the next BDF2 step.  Host or device pointers. */
+int mp_ist_single_timestep(mp_ist s, const double *phi_old, const double *u_new,
+                           const double *v_new, double *phi_new, int it, int *iters,
+                           double *relres, mp_stream stream);
+int mp_ist_destroy(mp_ist s);
+
 /* ------------------------------------------------------- learned guess */
 /*
  * Per-node network predicting the pressure increment of a fractional step

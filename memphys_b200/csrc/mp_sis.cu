@@ -211,6 +211,41 @@ __global__ void k_sis_err_final(int nb, const double *part, int nv, double *out)
     out[1] = mu / 2.0 + mv / 2.0;
 }
 
+// IMPLICIT_SCALAR_TRANSPORT_SOLVER::modify_matrix (implicit_scalar_transport_solver.cpp:87-109):
+// interior rows diff L + conv (u_i Gx + v_i Gy) + unsteady_factor unsteady I
+__global__ void k_ist_values(int nv, int K, const int *cols, const double *gx, const double *gy,
+                             const double *lap, const uint8_t *bflag, const double *u,
+                             const double *v, double diff, double conv, double diag, double *A) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)ell_padded_rows(nv) * K)
+        return;
+    int row;
+    if (!ell_slot(t, nv, K, row) || bflag[row])
+        return;
+    double val = diff * lap[t];
+    val = val + (u[row] * conv * gx[t]);
+    val = val + (v[row] * conv * gy[t]);
+    if (cols[t] == row)
+        val = val + diag;
+    A[t] = val;
+}
+
+// single_timestep_2d source (:153-165): unsteady phi_old (BDF1) or
+// -(a2 unsteady) phi_old - (a3 unsteady) phi_old_old; boundary rows phi_old
+// (Dirichlet) or 0
+__global__ void k_ist_source(int nv, const uint8_t *bflag, const uint8_t *dir, const double *po,
+                             const double *poo, double unsteady, int bdf1, double *src) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv)
+        return;
+    if (bflag[i])
+        src[i] = dir[i] ? po[i] : 0.0;
+    else if (bdf1)
+        src[i] = unsteady * po[i];
+    else
+        src[i] = -((-2.0 * unsteady) * po[i]) - ((0.5 * unsteady) * poo[i]);
+}
+
 }  // namespace mp
 
 using namespace mp;
@@ -425,6 +460,121 @@ extern "C" int mp_sis_single_timestep(mp_sis s, const double *const *vel_old,
 }
 
 extern "C" int mp_sis_destroy(mp_sis s) {
+    delete s;
+    return MP_OK;
+}
+
+// ------------------------------------------- implicit scalar transport
+// IMPLICIT_SCALAR_TRANSPORT_SOLVER (implicit_scalar_transport_solver.cpp, 2D): one
+// implicit convection-diffusion solve per step, BDF1 at it = 0 then BDF2, the
+// matrix's interior rows rebuilt from the given velocity every step (:140-151);
+// BiCGSTAB with the Jacobi diagonal of that matrix, from phi_old.
+struct mp_ist_s {
+    mp_cloud c = nullptr;
+    int nv = 0, K = 0;
+    double unsteady = 0, conv = 0, diff = 0;
+    dbuf<uint8_t> dir;
+    dbuf<double> po, poo, u, v;
+    Ppe T;
+    bool use_graph = true;
+};
+
+extern "C" int mp_ist_create(mp_cloud c, const uint8_t *boundary, const double *normal,
+                             const uint8_t *dirichlet, int precond_freq_it, double unsteady_coeff,
+                             double conv_coeff, double diff_coeff, const mp_solver_cfg *solver,
+                             mp_ist *out) {
+    if (!c || !boundary || !normal || !dirichlet || !solver || !out)
+        return fail(MP_BAD_ARG, "mp_ist_create: null argument");
+    (void)precond_freq_it;
+    int nv, n, dim;
+    MP_TRY(mp_cloud_info(c, &nv, &n, &dim));
+    if (dim != 2)
+        return fail(MP_BAD_ARG, "the implicit scalar transport solver is 2D (single_timestep_2d)");
+    if (solver->precond == MP_PRECOND_AMG || solver->precision != MP_FP64)
+        return fail(MP_BAD_ARG, "the transport matrix changes every step: its solver takes "
+                                "MP_PRECOND_JACOBI or MP_PRECOND_NONE in MP_FP64");
+    MP_TRY(solver_cfg_check(*solver));
+    std::vector<uint8_t> hb(nv), hd(nv);
+    MP_CUDA(cudaMemcpy(hb.data(), boundary, nv, cudaMemcpyDefault));
+    MP_CUDA(cudaMemcpy(hd.data(), dirichlet, nv, cudaMemcpyDefault));
+    bool any_dir = false;  // :28-39: full Neumann is not permitted
+    for (int i = 0; i < nv && !any_dir; i++)
+        any_dir = hb[i] && hd[i];
+    if (!any_dir)
+        return fail(MP_BAD_ARG, "full Neumann BC is not permitted for the transported scalar");
+    mp_ist_s *s = new mp_ist_s;
+    auto bail = [&](int rc) {
+        delete s;
+        return rc;
+    };
+    s->c = c;
+    s->nv = nv;
+    s->K = n;
+    s->unsteady = unsteady_coeff;
+    s->conv = conv_coeff;
+    s->diff = diff_coeff;
+    int rc;
+    if ((rc = s->T.create(c, boundary, dirichlet, normal, 0.0, 0.0, 0.0, *solver, 0, 0)) != MP_OK)
+        return bail(rc);
+    if ((rc = s->dir.alloc(nv)) != MP_OK)
+        return bail(rc);
+    MP_CUDA(cudaMemcpy(s->dir.p, dirichlet, nv, cudaMemcpyDefault));
+    for (dbuf<double> *d : {&s->po, &s->poo, &s->u, &s->v})
+        if ((rc = d->alloc(nv)) != MP_OK)
+            return bail(rc);
+    MP_CUDA(cudaMemset(s->poo.p, 0, sizeof(double) * nv));
+    MP_CUDA(cudaDeviceSynchronize());
+    *out = s;
+    return MP_OK;
+}
+
+extern "C" int mp_ist_set_graph(mp_ist s, int use_graph) {
+    if (!s)
+        return fail(MP_BAD_ARG, "null transport solver");
+    s->use_graph = use_graph != 0;
+    return MP_OK;
+}
+
+extern "C" int mp_ist_single_timestep(mp_ist s, const double *phi_old, const double *u_new,
+                                      const double *v_new, double *phi_new, int it, int *iters,
+                                      double *relres, mp_stream stream) {
+    if (!s || !phi_old || !u_new || !v_new || !phi_new || it < 0)
+        return fail(MP_BAD_ARG, "mp_ist_single_timestep: bad arguments");
+    cudaStream_t st = S(stream);
+    const int nv = s->nv, K = s->K;
+    const size_t vb = sizeof(double) * nv;
+    CloudView cv = cloud_view(s->c);
+    MP_CUDA(cudaMemcpyAsync(s->po.p, phi_old, vb, cudaMemcpyDefault, st));
+    MP_CUDA(cudaMemcpyAsync(s->u.p, u_new, vb, cudaMemcpyDefault, st));
+    MP_CUDA(cudaMemcpyAsync(s->v.p, v_new, vb, cudaMemcpyDefault, st));
+    const int bdf1 = it == 0;
+    const size_t tot = (size_t)ell_padded_rows(nv) * K;
+    k_ist_values<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(
+        nv, K, cv.cols, cv.w[0], cv.w[1], cv.w[3], cv.bflag, s->u.p, s->v.p, s->diff, s->conv,
+        (bdf1 ? 1.0 : 1.5) * s->unsteady, s->T.sys.A.v64.p);
+    MP_CHECK_LAUNCH();
+    MP_TRY(s->T.refresh_diag(st));
+    k_ist_source<<<(unsigned)((nv + 255) / 256), 256, 0, st>>>(
+        nv, cv.bflag, s->dir.p, s->po.p, s->poo.p, s->unsteady, bdf1, s->T.W.b64.p);
+    MP_CHECK_LAUNCH();
+    MP_CUDA(cudaMemcpyAsync(s->T.W.x.p, s->po.p, vb, cudaMemcpyDeviceToDevice, st));  // guess phi_old
+    MP_TRY(s->T.solve_resident(st, s->use_graph));
+    SolveStats ss;
+    MP_TRY(s->T.read_stats(st, &ss));
+    if (ss.status != MP_OK)
+        return fail(ss.status, "transport solve: status %d after %d iterations, relres %g",
+                    ss.status, ss.iters, ss.relres);
+    MP_CUDA(cudaMemcpyAsync(phi_new, s->T.W.x.p, vb, cudaMemcpyDefault, st));
+    MP_CUDA(cudaMemcpyAsync(s->poo.p, s->po.p, vb, cudaMemcpyDeviceToDevice, st));  // :172
+    MP_CUDA(cudaStreamSynchronize(st));
+    if (iters)
+        *iters = ss.iters;
+    if (relres)
+        *relres = ss.relres;
+    return MP_OK;
+}
+
+extern "C" int mp_ist_destroy(mp_ist s) {
     delete s;
     return MP_OK;
 }

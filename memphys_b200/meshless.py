@@ -482,6 +482,53 @@ class SEMI_IMPLICIT_SPLIT_SOLVER:
             pass
 
 
+class IMPLICIT_SCALAR_TRANSPORT_SOLVER:
+    """IMPLICIT_SCALAR_TRANSPORT_SOLVER (implicit_scalar_transport_solver.cpp:22-41, 2D)
+    on the GPU (mp_ist_*); with solver_log_flag the relative and absolute residuals
+    and iterations of every solve are appended to rel_res_log, abs_res_log and
+    n_iter_actual, as the reference appends them to its parameters."""
+
+    def __init__(self, points: POINTS, cloud: CLOUD, parameters: PARAMETERS, dirichlet_flag,
+                 precond_freq_it: int, unsteady_coeff: float, conv_coeff: float,
+                 diff_coeff: float, solver_log_flag: bool = False, use_graph: bool = True):
+        cfg = parameters.solver_cfg(precond=capi.MP_PRECOND_JACOBI, precision=capi.MP_FP64)
+        flag = np.ascontiguousarray(dirichlet_flag, np.uint8)
+        h = C.c_void_p()
+        check(capi.lib().mp_ist_create(cloud.handle, ptr(points.boundary_flag), ptr(points.normal),
+                                       ptr(flag), int(precond_freq_it), float(unsteady_coeff),
+                                       float(conv_coeff), float(diff_coeff), C.byref(cfg),
+                                       C.byref(h)), "mp_ist_create")
+        self.handle = h
+        self.cloud = cloud
+        self.nv = points.nv
+        self.solver_log_flag = solver_log_flag
+        self.rel_res_log, self.abs_res_log, self.n_iter_actual = [], [], []
+        check(capi.lib().mp_ist_set_graph(h, int(use_graph)))
+
+    def single_timestep_2d(self, phi_new, phi_old, u_new, v_new, it):
+        """single_timestep_2d (:136-174): phi_new (float64, nv entries) written in place."""
+        if not (isinstance(phi_new, np.ndarray) and phi_new.dtype == np.float64
+                and phi_new.shape == (self.nv,) and phi_new.flags.c_contiguous):
+            raise capi.MemphysError(capi.MP_BAD_ARG, f"phi_new: float64 array of {self.nv} entries")
+        po, u, v = (np.ascontiguousarray(a, np.float64) for a in (phi_old, u_new, v_new))
+        n, rr = C.c_int(), C.c_double()
+        check(capi.lib().mp_ist_single_timestep(self.handle, ptr(po), ptr(u), ptr(v), ptr(phi_new),
+                                                int(it), C.byref(n), C.byref(rr), None),
+              "mp_ist_single_timestep")
+        if self.solver_log_flag:
+            self.rel_res_log.append(rr.value)
+            self.n_iter_actual.append(n.value)
+        return n.value, rr.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                capi.lib().mp_ist_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
 class MLP:
     """The learned pressure-increment network (mp_mlp): 64 -> 128 -> 128 -> 128 -> 1."""
 

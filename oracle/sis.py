@@ -12,6 +12,7 @@ BiCGSTAB + ILUT and the pressure correction with its configured solver).
   SIS.calc_pressure       :131-186 (boundary rows in index order, as the loop runs)
   SIS.calc_vel_corr       :188-204
   SIS.single_timestep_2d  :376-421 (+ extras :206-216)
+  IST                     implicit_scalar_transport_solver.cpp:22-174 (one direct solve per step)
 """
 from __future__ import annotations
 
@@ -120,3 +121,36 @@ class SIS:
                 break
         self.uoo, self.voo = u_old.copy(), v_old.copy()
         return u, v, p, outer, l1, mx
+
+
+class IST:
+    """IMPLICIT_SCALAR_TRANSPORT_SOLVER: interior rows diff L + conv (u_i Gx + v_i Gy)
+    + a1 unsteady on the diagonal, boundary rows identity / n . G, BDF1 then BDF2."""
+
+    def __init__(self, cloud, nb_col, w, dirichlet, unsteady, conv, diff):
+        self.nb, self.w = np.asarray(nb_col), w
+        self.nv, self.n = self.nb.shape
+        self.bnd = np.asarray(cloud.boundary, bool)
+        self.normal = np.asarray(cloud.normal)
+        self.dir = np.asarray(dirichlet, bool)
+        self.unsteady, self.conv, self.diff = unsteady, conv, diff
+        self.rows = np.repeat(np.arange(self.nv), self.n)
+        self.poo = np.zeros(self.nv)
+
+    def single_timestep_2d(self, phi_old, u, v, it):
+        nb, w, b = self.nb, self.w, self.bnd
+        a1 = 1.0 if it == 0 else A1
+        vals = self.diff * w["lap"] + (u[:, None] * self.conv) * w["gx"] + (v[:, None] * self.conv) * w["gy"]
+        eye = nb == np.arange(self.nv)[:, None]
+        vals = vals + np.where(eye, a1 * self.unsteady, 0.0)
+        neu = self.normal[:, :1] * w["gx"] + self.normal[:, 1:2] * w["gy"]
+        vals = np.where(b[:, None], np.where(self.dir[:, None], eye * 1.0, neu), vals)
+        M = sp.csr_matrix((vals.ravel(), (self.rows, nb.ravel())), shape=(self.nv, self.nv))
+        if it == 0:
+            src = self.unsteady * phi_old
+        else:
+            src = -((A2 * self.unsteady) * phi_old) - ((A3 * self.unsteady) * self.poo)
+        src = np.where(b, np.where(self.dir, phi_old, 0.0), src)
+        phi = sla.spsolve(M.tocsc(), src)
+        self.poo = phi_old.copy()
+        return phi
