@@ -100,6 +100,18 @@ int mp_knn_stencils_noalloc(const double *xyz, const uint8_t *boundary, int nv, 
                             int *nb_col, mp_stream s);
 
 /*
+ * calc_interp_matrix (coefficient_computations.cpp:456-518): for each of np probe
+ * points its n nearest nodes of the cloud (calc_cloud_points_slow for probes,
+ * :373-428: no boundary rule; here in ascending distance, ties by index) and the
+ * PHS-RBF + polynomial interpolation weights (the stencil's saddle matrix with the
+ * basis evaluated at the probe, :430-454, probe scaled with its stencil).
+ * Row i of cols / w (np x n) is the sparse row i of the interpolation matrix.
+ * n <= 64.  Host or device pointers.
+ */
+int mp_interp_matrix(const double *xyz, int nv, int dim, const double *probe, int np, int n,
+                     int phs_deg, int poly_deg, int *cols, double *w, mp_stream s);
+
+/*
  * Node orderings.  order[i] = new index of node i (a permutation of 0..nv-1).
  * mp_order_rcm: CLOUD::re_order_points_reverse_cuthill_mckee (cloud.cpp:315-335)
  *   = reverse_cuthill_mckee_ordering (general_functions.cpp:806-879) on the

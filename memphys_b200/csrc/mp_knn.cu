@@ -54,22 +54,30 @@ __global__ void knn_cell_ranges(const unsigned int *cid_sorted, int nv, int *sta
         end[c] = i + 1;
 }
 
+// Stencil queries (probe == nullptr: query q is node q, boundary rule applied) or
+// probe queries (query q at probe[q], its n nearest nodes of the whole cloud, as
+// calc_cloud_points_slow for probes does, coefficient_computations.cpp:373-428).
 __global__ void __launch_bounds__(128)
     knn_query(const double *xyz, const uint8_t *bflag, int nv, int dim, int n, Grid G,
-              const int *order, const int *start, const int *end, int *nb_col, int *failed) {
+              const int *order, const int *start, const int *end, int *nb_col, int *failed,
+              const double *probe, int nq) {
     int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nv)
+    if (q >= (probe ? nq : nv))
         return;
     double bd[KNN_MAX];
     int bi[KNN_MAX];
-    const bool isb = bflag[q] != 0;
+    const bool isb = !probe && bflag[q] != 0;
     const int want = isb ? n - 1 : n;
     double xq[3] = {0, 0, 0};
     int qc[3] = {0, 0, 0};
+    bool inside = true;  // a query outside the grid scans until the grid is covered
     for (int d = 0; d < dim; d++) {
-        xq[d] = xyz[(size_t)q * dim + d];
-        int k = (int)((xq[d] - G.lo[d]) / G.cell);
-        qc[d] = k < 0 ? 0 : (k >= G.g[d] ? G.g[d] - 1 : k);
+        xq[d] = probe ? probe[(size_t)q * dim + d] : xyz[(size_t)q * dim + d];
+        const double t = (xq[d] - G.lo[d]) / G.cell;
+        if (!(t >= 0.0 && t <= (double)G.g[d]))
+            inside = false;
+        int k = (int)t;
+        qc[d] = t < 0 ? 0 : (k >= G.g[d] ? G.g[d] - 1 : k);
     }
     int cnt = 0;
     for (int R = 0;; R++) {
@@ -112,7 +120,7 @@ __global__ void __launch_bounds__(128)
         for (int d = 0; d < dim; d++)
             if (qc[d] - R > 0 || qc[d] + R < G.g[d] - 1)
                 covered = false;
-        if (cnt == want && bd[want - 1] <= reach * reach)
+        if (inside && cnt == want && bd[want - 1] <= reach * reach)
             break;
         if (covered)
             break;
@@ -134,8 +142,25 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+// probe == nullptr: the stencils of the nodes; else the n nearest nodes of each of
+// the np probes
+static int knn_run(const double *d_xyz, const uint8_t *d_bflag, int nv, int dim, int n, int *d_nb,
+                   const double *d_probe, int np, cudaStream_t s);
+
 int knn_device(const double *d_xyz, const uint8_t *d_bflag, int nv, int dim, int n, int *d_nb,
                cudaStream_t s) {
+    return knn_run(d_xyz, d_bflag, nv, dim, n, d_nb, nullptr, 0, s);
+}
+
+int knn_probe_device(const double *d_xyz, int nv, int dim, const double *d_probe, int np, int n,
+                     int *d_nb, cudaStream_t s) {
+    if (np <= 0 || n > nv)
+        return fail(MP_BAD_ARG, "probe kNN: np=%d, n=%d of %d nodes", np, n, nv);
+    return knn_run(d_xyz, nullptr, nv, dim, n, d_nb, d_probe, np, s);
+}
+
+static int knn_run(const double *d_xyz, const uint8_t *d_bflag, int nv, int dim, int n, int *d_nb,
+                   const double *d_probe, int np, cudaStream_t s) {
     if (nv <= 0 || (dim != 2 && dim != 3) || n < 2 || n > KNN_MAX)
         return fail(MP_BAD_ARG, "mp_knn_stencils: nv=%d dim=%d n=%d (n must be 2..%d)", nv, dim, n,
                     KNN_MAX);
@@ -195,8 +220,9 @@ int knn_device(const double *d_xyz, const uint8_t *d_bflag, int nv, int dim, int
     count_launch();
     knn_cell_ranges<<<nb, tb, 0, s>>>(cid2.p, nv, st.p, en.p);
     MP_CHECK_LAUNCH();
-    knn_query<<<(nv + 127) / 128, 128, 0, s>>>(d_xyz, d_bflag, nv, dim, n, G, idx2.p, st.p, en.p,
-                                                d_nb, failed.p);
+    const int nq = d_probe ? np : nv;
+    knn_query<<<(nq + 127) / 128, 128, 0, s>>>(d_xyz, d_bflag, nv, dim, n, G, idx2.p, st.p, en.p,
+                                                d_nb, failed.p, d_probe, np);
     MP_CHECK_LAUNCH();
     int bad = 0;
     MP_CUDA(cudaMemcpyAsync(&bad, failed.p, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -401,7 +427,7 @@ extern "C" int mp_knn_stencils_noalloc(const double *xyz, const uint8_t *boundar
     knn_cell_ranges<<<nb, tb, 0, st>>>(cid2, nv, cst, cen);
     MP_CHECK_LAUNCH();
     knn_query<<<(nv + 127) / 128, 128, 0, st>>>(xyz, boundary, nv, dim, n, G, idx2, cst, cen,
-                                                 nb_col, flags);
+                                                 nb_col, flags, nullptr, 0);
     MP_CHECK_LAUNCH();
     MP_CUDA(cudaMemcpyAsync(hf, flags, sizeof(int), cudaMemcpyDeviceToHost, st));
     MP_CUDA(cudaStreamSynchronize(st));

@@ -6,7 +6,9 @@
 //     P_ij = prod_d x_id^e_jd   (anisotropically scaled coordinates, :33-68)
 // with the dim+1 right-hand sides of :108-292 (d/dx, d/dy, [d/dz], Laplacian of
 // the basis at the centre node 0).  The weights are the first n rows of the
-// solution (:311-323).
+// solution (:311-323).  Interpolation mode (calc_interp_matrix, :456-518) has one
+// right-hand side instead: the basis evaluated at a probe point that is shifted
+// and scaled with its stencil (calc_PHS_RBF_interp_single_vert_rhs, :430-454).
 //
 // Weights kernel: one thread per matrix row, the augmented row [A_i | B_i]
 // held in registers; Gauss-Jordan with partial pivoting.  At step k every
@@ -47,6 +49,7 @@ struct StencilJob {
     double *cond;
     int *singular;               // count of singular systems
     unsigned int *queue;         // persistent work counter
+    const double *probe;         // interpolation mode: probe point of each system (count x dim)
 };
 
 __constant__ int c_exps[MAX_M * MAX_DIM];
@@ -89,7 +92,7 @@ __device__ __forceinline__ double monomial(const double *x, int j, int dim) {
 // Entry (r, j) of the augmented system [A | B] for a stencil with n nodes whose
 // scaled coordinates are in sp (n x dim) and per-axis scales in sc.
 __device__ double aug_entry(int r, int j, int n, int m, int dim, int phs, const double *sp,
-                            const double *sc) {
+                            const double *sc, const double *xp = nullptr) {
     const int S = n + m;
     if (j < S) {
         if (r < n && j < n) {
@@ -107,6 +110,17 @@ __device__ double aug_entry(int r, int j, int n, int m, int dim, int phs, const 
         if (j < n)
             return monomial(sp + j * dim, r - n, dim);
         return 0.0;
+    }
+    if (xp) {  // interpolation: r^phs to the scaled probe, monomials at it (:430-454)
+        if (r < n) {
+            double r2 = 0.0;
+            for (int d = 0; d < dim; d++) {
+                double t = sp[r * dim + d] - xp[d];
+                r2 += t * t;
+            }
+            return rpow_odd(r2, phs);
+        }
+        return monomial(xp, r - n, dim);
     }
     const int c = j - S;  // rhs column: 0..dim-1 gradient, dim Laplacian
     const double *x0 = sp;  // centre = local node 0
@@ -208,7 +222,7 @@ template <int G, int W> struct GJShape {
     static constexpr int SMAX = W - 3;               // rows available (R >= 3)
     static constexpr int LD = (W % 2) ? W : W + 1;   // odd leading dim: conflict-free row loads
     static constexpr int PTS = SMAX * MAX_DIM;
-    static constexpr int DOUBLES = PTS + 2 * MAX_DIM + W + 2 * G + SMAX * LD;
+    static constexpr int DOUBLES = PTS + 3 * MAX_DIM + W + 2 * G + SMAX * LD;
 };
 
 template <int G, int W>
@@ -219,7 +233,8 @@ __global__ void __launch_bounds__(GJShape<G, W>::CTA)
     const int grp = threadIdx.x / Sh::NT, tid = threadIdx.x % Sh::NT;
     const int lane = threadIdx.x & 31, warp_in_grp = tid >> 5;
     double *base = smem_raw + grp * Sh::DOUBLES;
-    double *sp = base, *sc = sp + Sh::PTS, *prow = sc + 2 * MAX_DIM;
+    // sc: scales, minima, scaled probe (interpolation mode)
+    double *sp = base, *sc = sp + Sh::PTS, *prow = sc + 3 * MAX_DIM;
     double *amax = prow + W;
     double *mat = amax + 2 * G;
     auto sync = [&]() {
@@ -228,7 +243,8 @@ __global__ void __launch_bounds__(GJShape<G, W>::CTA)
         else
             __syncthreads();
     };
-    const int dim = J.dim, m = J.m, R = dim + 1;
+    const int dim = J.dim, m = J.m, R = J.probe ? 1 : dim + 1;
+    double *xp = J.probe ? sc + 2 * MAX_DIM : nullptr;
     __shared__ int s_item[Sh::GROUPS];
     for (;;) {
         if (tid == 0)
@@ -241,9 +257,14 @@ __global__ void __launch_bounds__(GJShape<G, W>::CTA)
         const int id = sys_id(J, t);
         const int n = sys_n(J, id), S = n + m, SR = S + R;
         load_scaled_points(J, id, n, sp, sc, tid, Sh::NT, sync);
+        if (xp) {  // the probe shifted and scaled with its stencil (:23-30)
+            if (tid < dim)
+                xp[tid] = (J.probe[(size_t)id * dim + tid] - sc[MAX_DIM + tid]) / sc[tid];
+            sync();
+        }
         for (int q = tid; q < S * SR; q += Sh::NT) {
             int r = q / SR, j = q - r * SR;
-            mat[r * Sh::LD + j] = aug_entry(r, j, n, m, dim, J.phs, sp, sc);
+            mat[r * Sh::LD + j] = aug_entry(r, j, n, m, dim, J.phs, sp, sc, xp);
         }
         sync();
         double a[W];
@@ -304,7 +325,9 @@ __global__ void __launch_bounds__(GJShape<G, W>::CTA)
         // ---- results: thread that pivoted at step k holds solution row k
         if (my_step >= 0 && my_step < n) {
             const double inv = 1.0 / my_diag;
-            if (J.nb_col) {
+            if (J.probe) {
+                J.w0[(size_t)id * n + my_step] = a[0] * inv;
+            } else if (J.nb_col) {
                 size_t o = (size_t)id * n + my_step;
                 J.w0[o] = a[0] * inv;
                 J.w1[o] = a[1] * inv;
@@ -685,6 +708,45 @@ int cloud_weights_device(const double *d_xyz, int nv, int dim, const int *d_nb, 
     return MP_OK;
 }
 
+// interpolation weights of np probes from their stencils nb (np x n) of cloud xyz
+int interp_weights_device(const double *d_xyz, int dim, const double *d_probe, int np,
+                          const int *d_nb, int n, int phs, int poly_deg, double *w,
+                          cudaStream_t s) {
+    if (np <= 0 || n <= 1 || (dim != 2 && dim != 3))
+        return fail(MP_BAD_ARG, "mp_interp_matrix: np=%d n=%d dim=%d", np, n, dim);
+    if (phs != 3 && phs != 5 && phs != 7 && phs != 9 && phs != 11)
+        return fail(MP_BAD_ARG, "phs_deg should be 3, 5, 7, 9 or 11; got %d", phs);
+    int m = 0;
+    MP_TRY(upload_exponents(dim, poly_deg, &m));
+    const int cls = gj_class(n + m, 1);
+    if (cls < 0)
+        return fail(MP_BAD_ARG, "interpolation system %d x %d exceeds the supported %d", n + m,
+                    n + m, MAX_S);
+    StencilScratch scr;
+    StencilJob J{};
+    MP_TRY(scr.get(&J.queue, &J.singular));
+    MP_CUDA(cudaMemsetAsync(J.singular, 0, sizeof(int), s));
+    J.xyz = d_xyz;
+    J.nb_col = d_nb;
+    J.n_fixed = n;
+    J.count = np;
+    J.dim = dim;
+    J.m = m;
+    J.phs = phs;
+    J.w0 = w;
+    J.probe = d_probe;
+    MP_TRY(launch_class(cls, J, s));
+    int bad = 0;
+    MP_CUDA(cudaMemcpyAsync(&bad, J.singular, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    if (bad)
+        return fail(MP_SINGULAR_STENCIL, "%d interpolation systems had a zero pivot", bad);
+    return MP_OK;
+}
+
+int knn_probe_device(const double *d_xyz, int nv, int dim, const double *d_probe, int np, int n,
+                     int *d_nb, cudaStream_t s);
+
 }  // namespace mp
 
 using namespace mp;
@@ -851,4 +913,38 @@ extern "C" int mp_stencil_weights_batched(int nsys, const int *sizes, const int6
     if (bad_total)
         return fail(MP_SINGULAR_STENCIL, "%d stencil systems had a zero pivot", bad_total);
     return MP_OK;
+}
+
+extern "C" int mp_interp_matrix(const double *xyz, int nv, int dim, const double *probe, int np,
+                                int n, int phs_deg, int poly_deg, int *cols, double *w,
+                                mp_stream s) {
+    cudaStream_t st = S(s);
+    if (!xyz || !probe || !cols || !w || nv <= 0 || np <= 0)
+        return fail(MP_BAD_ARG, "mp_interp_matrix: bad arguments");
+    dbuf<double> tx, tp, tw;
+    dbuf<int> tc;
+    const double *dx, *dp;
+    MP_TRY(stage_in(xyz, (size_t)nv * dim, tx, &dx, st));
+    MP_TRY(stage_in(probe, (size_t)np * dim, tp, &dp, st));
+    int *dc = cols;
+    double *dw = w;
+    const bool hc = !is_device_ptr(cols), hw = !is_device_ptr(w);
+    if (hc) {
+        MP_TRY(tc.alloc((size_t)np * n));
+        dc = tc.p;
+    }
+    if (hw) {
+        MP_TRY(tw.alloc((size_t)np * n));
+        dw = tw.p;
+    }
+    MP_TRY(knn_probe_device(dx, nv, dim, dp, np, n, dc, st));
+    const int rc = interp_weights_device(dx, dim, dp, np, dc, n, phs_deg, poly_deg, dw, st);
+    if (rc != MP_OK && rc != MP_SINGULAR_STENCIL)
+        return rc;
+    if (hc)
+        MP_CUDA(cudaMemcpyAsync(cols, dc, sizeof(int) * np * n, cudaMemcpyDeviceToHost, st));
+    if (hw)
+        MP_CUDA(cudaMemcpyAsync(w, dw, sizeof(double) * np * n, cudaMemcpyDeviceToHost, st));
+    MP_CUDA(cudaStreamSynchronize(st));
+    return rc;
 }

@@ -182,6 +182,43 @@ def batched_weights(sizes, offsets, pts, dim, phs=3, poly_deg=3, cond=False):
 
 
 # ---------------------------------------------------------------- operators
+def interp_matrix(xyz: np.ndarray, probe: np.ndarray, n: int, phs: int = 3, poly_deg: int = 3):
+    """calc_interp_matrix (coefficient_computations.cpp:456-518) in numpy: each probe's n
+    nearest nodes (calc_cloud_points_slow for probes, :373-428; here ordered by distance,
+    ties by index), shifting_scaling of the stencil with the probe (:4-31), the saddle
+    matrix of :70-106 and the right-hand side of :430-454, solved by LAPACK.
+    Returns cols (np x n) and weights (np x n)."""
+    xyz = np.asarray(xyz, np.float64)
+    probe = np.asarray(probe, np.float64)
+    dim = xyz.shape[1]
+    e = poly_exponents(dim, poly_deg)
+    m = e.shape[0]
+    cols = np.zeros((len(probe), n), np.int32)
+    wts = np.zeros((len(probe), n))
+    idx = np.arange(len(xyz))
+    for q, p in enumerate(probe):
+        d2 = ((xyz - p) ** 2).sum(1)
+        nb = np.lexsort((idx, d2))[:n]
+        v = xyz[nb].copy()
+        lo, hi = v.min(0), v.max(0)
+        sc = hi - lo
+        v = (v - lo) / sc
+        xp = (p - lo) / sc
+        r2 = ((v[:, None, :] - v[None, :, :]) ** 2).sum(2)
+        A = np.zeros((n + m, n + m))
+        A[:n, :n] = r2 ** (phs / 2.0)
+        np.fill_diagonal(A[:n, :n], 0.0)
+        P = np.prod(v[:, None, :] ** e[None, :, :], axis=2)
+        A[:n, n:] = P
+        A[n:, :n] = P.T
+        rhs = np.zeros(n + m)
+        rhs[:n] = ((v - xp) ** 2).sum(1) ** (phs / 2.0)
+        rhs[n:] = np.prod(xp[None, :] ** e, axis=1)
+        cols[q] = nb
+        wts[q] = np.linalg.solve(A, rhs)[:n]
+    return cols, wts
+
+
 def rcm_order(nb_col: np.ndarray) -> np.ndarray:
     """reverse_cuthill_mckee_ordering (general_functions.cpp:806-879) on the stencil
     graph, as CLOUD::re_order_points_reverse_cuthill_mckee builds it (cloud.cpp:315-335):
