@@ -679,8 +679,8 @@ def run_reference(args, ws, rank):
     ms = (time.time() - t0) * 1e3 / args.steps
     sample = (f"{args.steps} timesteps of the {cl.nv}-node cavity, C restatement of "
               f"FRACTIONAL_STEP_1 + BiCGSTAB/ILUT capped at {cap} iterations per step "
-              f"(a lower bound of a converged step); SpMV rows, fractional-step row loops "
-              f"and vector updates on {cores} threads, dot products and ILUT solves serial "
+              f"(a lower bound of a converged step); SpMV rows and fractional-step row loops "
+              f"on {cores} threads, vector updates, dot products and ILUT solves serial "
               f"as in Eigen; weights on {cores} threads "
               f"({t_setup:.0f} s setup)")
     return {"metric": "ms/fractional-step at 1M pts (learned+mixed vs plain FP64 GPU); SpMV HBM GB/s",
