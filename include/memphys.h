@@ -110,6 +110,11 @@ int mp_knn_stencils_noalloc(const double *xyz, const uint8_t *boundary, int nv, 
  */
 int mp_interp_matrix(const double *xyz, int nv, int dim, const double *probe, int np, int n,
                      int phs_deg, int poly_deg, int *cols, double *w, mp_stream s);
+/* the n (1..64) nearest nodes of each probe (np x n, ascending distance, ties by
+ * index): the nearest-node lookup of read_restart_tecplot_file
+ * (postprocessing_functions.cpp:662-679, a nanoflann 1-NN query there) */
+int mp_knn_probe(const double *xyz, int nv, int dim, const double *probe, int np, int n,
+                 int *cols, mp_stream s);
 
 /*
  * Node orderings.  order[i] = new index of node i (a permutation of 0..nv-1).

@@ -34,7 +34,7 @@ EXPORTS = [
     "mp_free_host", "mp_memcpy", "mp_memset", "mp_stream_create", "mp_stream_destroy",
     "mp_stream_sync", "mp_timer_start", "mp_timer_stop", "mp_profiler", "mp_launch_count", "mp_num_poly_terms",
     "mp_cloud_size", "mp_poly_exponents", "mp_knn_stencils", "mp_knn_stencils_noalloc",
-    "mp_interp_matrix", "mp_order_rcm", "mp_order_morton", "mp_permute_stencils", "mp_permute_rows",
+    "mp_interp_matrix", "mp_knn_probe", "mp_order_rcm", "mp_order_morton", "mp_permute_stencils", "mp_permute_rows",
     "mp_sis_create", "mp_sis_system_size", "mp_sis_set_graph", "mp_sis_single_timestep",
     "mp_sis_destroy", "mp_ist_create", "mp_ist_set_graph", "mp_ist_single_timestep",
     "mp_ist_destroy",
@@ -101,6 +101,7 @@ def lib() -> C.CDLL:
             "mp_knn_stencils": [vp, vp, i, i, i, vp, vp],
             "mp_knn_stencils_noalloc": [vp, vp, i, i, i, vp, vp],
             "mp_interp_matrix": [vp, i, i, vp, i, i, i, i, vp, vp, vp],
+            "mp_knn_probe": [vp, i, i, vp, i, i, vp, vp],
             "mp_order_rcm": [vp, i, i, vp], "mp_order_morton": [vp, i, i, vp, vp],
             "mp_permute_stencils": [vp, i, i, vp, vp, vp],
             "mp_permute_rows": [vp, vp, i, i, vp, vp],

@@ -161,7 +161,7 @@ int knn_probe_device(const double *d_xyz, int nv, int dim, const double *d_probe
 
 static int knn_run(const double *d_xyz, const uint8_t *d_bflag, int nv, int dim, int n, int *d_nb,
                    const double *d_probe, int np, cudaStream_t s) {
-    if (nv <= 0 || (dim != 2 && dim != 3) || n < 2 || n > KNN_MAX)
+    if (nv <= 0 || (dim != 2 && dim != 3) || n < (d_probe ? 1 : 2) || n > KNN_MAX)
         return fail(MP_BAD_ARG, "mp_knn_stencils: nv=%d dim=%d n=%d (n must be 2..%d)", nv, dim, n,
                     KNN_MAX);
     // bounding box on the host (one small copy; setup path)
@@ -433,5 +433,30 @@ extern "C" int mp_knn_stencils_noalloc(const double *xyz, const uint8_t *boundar
     MP_CUDA(cudaStreamSynchronize(st));
     if (hf[0])
         return fail(MP_KNN_FAILED, "%d nodes found fewer than %d stencil candidates", hf[0], n);
+    return MP_OK;
+}
+
+// the n nearest nodes of each probe point, ascending distance, ties by index
+extern "C" int mp_knn_probe(const double *xyz, int nv, int dim, const double *probe, int np, int n,
+                            int *cols, mp_stream s) {
+    if (!xyz || !probe || !cols || np <= 0)
+        return fail(MP_BAD_ARG, "mp_knn_probe: bad arguments");
+    cudaStream_t st = S(s);
+    dbuf<double> tx, tp;
+    dbuf<int> tc;
+    const double *dx, *dp;
+    MP_TRY(stage_in(xyz, (size_t)nv * dim, tx, &dx, st));
+    MP_TRY(stage_in(probe, (size_t)np * dim, tp, &dp, st));
+    int *dc = cols;
+    const bool host_out = !is_device_ptr(cols);
+    if (host_out) {
+        MP_TRY(tc.alloc((size_t)np * n));
+        dc = tc.p;
+    }
+    MP_TRY(knn_probe_device(dx, nv, dim, dp, np, n, dc, st));
+    if (host_out) {
+        MP_CUDA(cudaMemcpyAsync(cols, dc, sizeof(int) * np * n, cudaMemcpyDeviceToHost, st));
+        MP_CUDA(cudaStreamSynchronize(st));
+    }
     return MP_OK;
 }

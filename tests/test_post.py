@@ -1,0 +1,62 @@
+"""Post-processing writers (postprocessing_functions.cpp formats) on the CPU."""
+import types
+
+import numpy as np
+
+from memphys_b200 import post
+
+
+def tiny_points(order=None):
+    xyz = np.array([[0.0, 0.0], [0.5, 0.25], [1.0, 1.0 / 3.0]])
+    return types.SimpleNamespace(nv=3, dim=2, xyz=xyz, order=order,
+                                 boundary_flag=np.array([1, 0, 1], np.uint8))
+
+
+def test_tecplot_steady_format(tmp_path):
+    pts = tiny_points()
+    path = post.write_tecplot_steady_variables(str(tmp_path / "run"), pts, ["u", "p"],
+                                               [np.array([1.0, 2.5, -3.0]), np.array([0.1, 0.2, 0.3])],
+                                               elements=[[0, 1, 2], [0, 1]])
+    lines = open(path).read().splitlines()
+    assert lines[0] == 'VARIABLES="x", "y", "u", "p"'      # :775-780
+    assert lines[1] == ('ZONE T="1"  DATAPACKING=POINT, NODES=3, ELEMENTS=1, ZONETYPE=FETRIANGLE')
+    assert lines[2] == "0 0 1 0.1 "                          # %.16g with a trailing blank
+    assert lines[3] == "0.5 0.25 2.5 0.2 "
+    assert lines[4] == "1 0.3333333333333333 -3 0.3 "
+    assert lines[5] == "1 2 3 "                              # 1-based triangle, the edge skipped
+    assert len(lines) == 6
+
+
+def test_tecplot_temporal_and_reordered_points(tmp_path):
+    # points renumbered by order: row i of the file is input node i, valued at order[i]
+    order = np.array([2, 0, 1])
+    pts = tiny_points(order)
+    pts.xyz = pts.xyz.copy()
+    pts.xyz[order] = tiny_points().xyz
+    prefix = str(tmp_path / "run")
+    post.write_tecplot_temporal_variables_header(prefix, 2, ["u"])
+    u_current = np.array([10.0, 20.0, 30.0])
+    post.write_tecplot_temporal_variables(prefix, pts, 0.5, ["u"], [u_current], 3)
+    lines = open(prefix + "_tecplot_temporal.plt").read().splitlines()
+    assert lines[0] == 'VARIABLES="x", "y", "u"'
+    assert lines[1].startswith('ZONE T="1.5"  DATAPACKING=POINT, NODES=3, ELEMENTS=0')
+    assert lines[2] == "0 0 30 "   # input node 0 lives at current index 2
+    assert lines[3] == "0.5 0.25 10 "
+
+
+def test_csv_writers(tmp_path):
+    p = tmp_path / "xyz.csv"
+    post.write_csv_xyz(np.array([0.0, 1.5, 2.0, -1.0]), 2, str(p))
+    assert open(p).read() == "no,x,y\n0,0,1.5\n1,2,-1\n"
+    q = tmp_path / "t.csv"
+    post.write_csv_temporal_data_init(3, str(q))
+    post.write_csv_temporal_data(np.array([1.0, 2.0, 0.125]), 0.25, str(q))
+    assert open(q).read() == "time(s),0,1,2\n0.25,1,2,0.125\n"
+
+
+def test_max_l1_error_split():
+    a = np.array([0.0, 1.0, -3.0, 2.0])
+    b = np.zeros(4)
+    assert post.calc_max_l1_error(b, a) == (3.0, 1.5)
+    mb, lb, mi, li = post.calc_max_l1_error(b, a, np.array([1, 0, 1, 0]))
+    assert (mb, lb, mi, li) == (3.0, 1.5, 2.0, 1.5)
