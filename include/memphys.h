@@ -369,6 +369,27 @@ int mp_ist_single_timestep(mp_ist s, const double *phi_old, const double *u_new,
                            double *relres, mp_stream stream);
 int mp_ist_destroy(mp_ist s);
 
+/* ---------------------------------------- Fourier-z fractional step */
+/*
+ * FRACTIONAL_STEP_FOURIER (fractional_step_fourier.cpp): a 2D cloud extruded
+ * periodically in z over N = 2 nw + 1 planes of `period`; fields are nv x N,
+ * column-major (plane c at offset c * nv), as the reference's Eigen::MatrixXd.
+ * The pressure of each z-Fourier mode is solved by `solver` (Helmholtz
+ * L - k^2 per mode; the first mode bordered under full-Neumann pressure).
+ */
+typedef struct mp_fsf_s *mp_fsf;
+int mp_fsf_create(mp_cloud c, const uint8_t *boundary, const double *normal, const uint8_t *u_dir,
+                  const uint8_t *v_dir, const uint8_t *w_dir, const uint8_t *p_dir, double period,
+                  int nw, int temporal_order, double rho, double mu, double dt,
+                  const mp_solver_cfg *solver, mp_fsf *out);
+int mp_fsf_set_graph(mp_fsf f, int use_graph);
+/* single_timestep (:250-266): vel_old = {u, v, w}, p_old -> vel_new, p_new (nv x N each);
+ * the Fourier coefficients are taken from the old fields at it = 0 and carried by
+ * the object afterwards, as the reference does.  Host or device pointers. */
+int mp_fsf_single_timestep(mp_fsf f, const double *const *vel_old, const double *p_old,
+                           double *const *vel_new, double *p_new, int it, mp_stream stream);
+int mp_fsf_destroy(mp_fsf f);
+
 /* ------------------------------------------------------- learned guess */
 /*
  * Per-node network predicting the pressure increment of a fractional step

@@ -37,7 +37,8 @@ EXPORTS = [
     "mp_interp_matrix", "mp_knn_probe", "mp_order_rcm", "mp_order_morton", "mp_permute_stencils", "mp_permute_rows",
     "mp_sis_create", "mp_sis_system_size", "mp_sis_set_graph", "mp_sis_single_timestep",
     "mp_sis_destroy", "mp_ist_create", "mp_ist_set_graph", "mp_ist_single_timestep",
-    "mp_ist_destroy",
+    "mp_ist_destroy", "mp_fsf_create", "mp_fsf_set_graph", "mp_fsf_single_timestep",
+    "mp_fsf_destroy",
     "mp_stencil_weights",
     "mp_stencil_weights_batched", "mp_cloud_create", "mp_cloud_create_stencils", "mp_cloud_info",
     "mp_cloud_get", "mp_cloud_destroy", "mp_op_create_ell", "mp_op_from_cloud", "mp_op_apply",
@@ -114,6 +115,9 @@ def lib() -> C.CDLL:
             "mp_ist_set_graph": [vp, i],
             "mp_ist_single_timestep": [vp, vp, vp, vp, vp, i, C.POINTER(i), C.POINTER(d), vp],
             "mp_ist_destroy": [vp],
+            "mp_fsf_create": [vp, vp, vp, vp, vp, vp, vp, d, i, i, d, d, d, vp, C.POINTER(vp)],
+            "mp_fsf_set_graph": [vp, i],
+            "mp_fsf_single_timestep": [vp, vp, vp, vp, vp, i, vp], "mp_fsf_destroy": [vp],
             "mp_stencil_weights": [vp, i, i, vp, i, i, i, vp, vp, vp, vp, vp, vp],
             "mp_stencil_weights_batched": [i, vp, vp, vp, i, i, i, vp, vp, vp],
             "mp_cloud_create": [vp, vp, i, i, i, i, d, i, vp, C.POINTER(vp)],

@@ -437,16 +437,32 @@ static int upload_csr(const Csr &C, DCsr &D, cudaStream_t s) {
 }
 
 // bordered dense inverse of the coarsest operator (LU with partial pivoting)
+// An operator whose rows all sum to zero (constants in its null space, the
+// all-Neumann pressure system) is bordered like solver.cpp:205-213; any other
+// (Dirichlet rows, a shifted diagonal such as the Helmholtz systems of the
+// Fourier modes) is inverted as [A 0; 0 1], so that the coarse correction keeps
+// the constant component, which such operators do not annihilate.
 static int coarse_inverse(const Csr &A, std::vector<double> &inv) {
     const int n = A.n, m = n + 1;
     std::vector<double> M((size_t)m * m, 0.0);
-    for (int i = 0; i < n; i++)
-        for (int t = A.rp[i]; t < A.rp[i + 1]; t++)
-            M[(size_t)i * m + A.ci[t]] += A.v[t];
+    double max_sum = 0.0, max_abs = 0.0;
     for (int i = 0; i < n; i++) {
-        M[(size_t)i * m + n] = 1.0;
-        M[(size_t)n * m + i] = 1.0;
+        double rs = 0.0, ra = 0.0;
+        for (int t = A.rp[i]; t < A.rp[i + 1]; t++) {
+            M[(size_t)i * m + A.ci[t]] += A.v[t];
+            rs += A.v[t];
+            ra += std::fabs(A.v[t]);
+        }
+        max_sum = std::max(max_sum, std::fabs(rs));
+        max_abs = std::max(max_abs, ra);
     }
+    const bool border = max_sum <= 1e-10 * max_abs;
+    for (int i = 0; i < n; i++) {
+        M[(size_t)i * m + n] = border ? 1.0 : 0.0;
+        M[(size_t)n * m + i] = border ? 1.0 : 0.0;
+    }
+    if (!border)
+        M[(size_t)n * m + n] = 1.0;
     inv.assign((size_t)m * m, 0.0);
     for (int i = 0; i < m; i++)
         inv[(size_t)i * m + i] = 1.0;
@@ -735,7 +751,7 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
                 continue;
             }
         }
-        // coarsest level: bordered dense inverse
+        // coarsest level: dense inverse (bordered when singular)
         hash_csr(A);
         std::vector<double> inv;
         if ((rc = coarse_inverse(A, inv)) != MP_OK)

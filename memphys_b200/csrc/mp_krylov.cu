@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
         double t2 = tol * tol;
         if (ZERO_X && S->rr_true > 0.0)
             t2 = fmax(t2, fmin(0.25 * S->tol_outer2 * S->b64_sq / S->rr_true, 0.25));
-        S->tol2 = t2 * bb;
+        S->tol2 = ZERO_X ? t2 * bb : fmax(t2 * bb, S->abs_tol2);
         S->zero_x = (bb == 0.0);
         int done = (bb == 0.0) || !(rr > S->tol2 && maxit > 0);
         S->status = MP_OK;
@@ -868,10 +868,18 @@ int Ppe::read_stats(cudaStream_t st, SolveStats *out) {
     out->abs_res = std::sqrt(hs.rr_true);
     out->relres = hs.b64_sq > 0 ? std::sqrt(hs.rr_true / hs.b64_sq) : 0.0;
     out->status = hs.status;
-    if (hs.status == MP_OK && out->relres > cfg.tol && hs.b64_sq > 0)
+    if (hs.status == MP_OK && out->relres > cfg.tol && hs.b64_sq > 0 &&
+        !(hs.rr_true <= hs.abs_tol2))
         out->status = MP_NOT_CONVERGED;
     if (hs.status == MP_OK && !std::isfinite(out->relres))
         out->status = MP_NAN_DETECTED;
+    return MP_OK;
+}
+
+int Ppe::set_abs_tol(double atol, cudaStream_t st) {
+    const double a2 = atol * atol;
+    MP_CUDA(cudaMemcpyAsync(&W.scal.p->abs_tol2, &a2, sizeof(double), cudaMemcpyHostToDevice, st));
+    MP_CUDA(cudaStreamSynchronize(st));  // a2 lives on this stack frame
     return MP_OK;
 }
 

@@ -32,6 +32,7 @@ struct BicgScalars {
     int outer_it, outer_max, outer_done, total_inner, half_total;
     double tol_outer2, b64_sq;
     double relres0;     // ||b - A x0|| / ||b|| of the initial guess (first residual of a solve)
+    double abs_tol2;    // absolute floor of the stopping ||r||^2 (0: the relative test alone)
     double guess_theta; // weight of the learned correction in the last initial guess
 };
 

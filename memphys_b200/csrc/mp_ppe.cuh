@@ -48,6 +48,8 @@ struct Ppe {
     // after the operator's values changed in place: the Jacobi diagonal again
     // (systems without a multigrid hierarchy only)
     int refresh_diag(cudaStream_t st);
+    // absolute floor of the stopping residual norm, kept until changed (default 0)
+    int set_abs_tol(double atol, cudaStream_t st);
     int pk() const {
         return cfg.precond == MP_PRECOND_AMG ? PK_EXTERNAL
                                              : (cfg.precond == MP_PRECOND_JACOBI ? PK_JACOBI : PK_NONE);

@@ -529,6 +529,54 @@ class IMPLICIT_SCALAR_TRANSPORT_SOLVER:
             pass
 
 
+class FRACTIONAL_STEP_FOURIER:
+    """FRACTIONAL_STEP_FOURIER (fractional_step_fourier.cpp:22-68) on the GPU (mp_fsf_*):
+    a 2D cloud extruded periodically in z over 2 nw + 1 planes of `period`; fields are
+    (nv, 2 nw + 1) arrays."""
+
+    def __init__(self, points: POINTS, cloud: CLOUD, parameters: PARAMETERS, u_dirichlet_flag,
+                 v_dirichlet_flag, w_dirichlet_flag, p_dirichlet_flag, period: float, nw: int,
+                 temporal_order: int, use_graph: bool = True, **cfg):
+        flags = [np.ascontiguousarray(f, np.uint8) for f in
+                 (u_dirichlet_flag, v_dirichlet_flag, w_dirichlet_flag, p_dirichlet_flag)]
+        sc = parameters.solver_cfg(**cfg)
+        h = C.c_void_p()
+        check(capi.lib().mp_fsf_create(cloud.handle, ptr(points.boundary_flag), ptr(points.normal),
+                                       *[ptr(f) for f in flags], float(period), int(nw),
+                                       int(temporal_order), float(parameters.rho),
+                                       float(parameters.mu), float(parameters.dt or 0.0),
+                                       C.byref(sc), C.byref(h)), "mp_fsf_create")
+        self.handle = h
+        self.cloud = cloud
+        self.nv, self.N = points.nv, 2 * int(nw) + 1
+        check(capi.lib().mp_fsf_set_graph(h, int(use_graph)))
+
+    def single_timestep(self, u_new, v_new, w_new, p_new, u_old, v_old, w_old, p_old, it):
+        """single_timestep (:250-266): (nv, 2 nw + 1) float64 arrays; the new fields are
+        written in place."""
+        shape = (self.nv, self.N)
+        # Eigen's MatrixXd is column-major: plane c is contiguous, i.e. the C-ordered
+        # (N, nv) transpose
+        olds = [np.ascontiguousarray(np.asarray(a, np.float64).reshape(shape).T) for a in
+                (u_old, v_old, w_old, p_old)]
+        outs = [np.zeros((self.N, self.nv)) for _ in range(4)]
+        vin = (C.c_void_p * 3)(*[a.ctypes.data for a in olds[:3]])
+        vout = (C.c_void_p * 3)(*[a.ctypes.data for a in outs[:3]])
+        check(capi.lib().mp_fsf_single_timestep(self.handle, vin, ptr(olds[3]), vout,
+                                                ptr(outs[3]), int(it), None),
+              "mp_fsf_single_timestep")
+        for dst, src in zip((u_new, v_new, w_new, p_new), outs):
+            dst[...] = src.T
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                capi.lib().mp_fsf_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
 class MLP:
     """The learned pressure-increment network (mp_mlp): 64 -> 128 -> 128 -> 128 -> 1."""
 
