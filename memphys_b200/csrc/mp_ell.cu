@@ -44,7 +44,7 @@ int ell_create(Ell &E, int nrows, int ncols, int K, const int *cols, const doubl
     const size_t tot = (size_t)np * K;
     dbuf<int> tc;
     dbuf<double> tv;
-    const int *dc;
+    const int *dc = nullptr;
     const double *dv = nullptr;
     MP_TRY(stage_in(cols, (size_t)nrows * K, tc, &dc, s));
     if (vals)
@@ -259,7 +259,7 @@ extern "C" int mp_op_info(mp_op op, int *nrows, int *ncols, int *width, int *pre
 
 template <class T>
 static int op_apply_t(mp_op op, const void *x, void *y, double alpha, double beta, cudaStream_t s) {
-    const T *dx;
+    const T *dx = nullptr;
     dbuf<T> tx, ty;
     MP_TRY(stage_in((const T *)x, (size_t)op->E.ncols, tx, &dx, s));
     T *dy = (T *)y;

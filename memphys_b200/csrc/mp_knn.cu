@@ -243,8 +243,8 @@ extern "C" int mp_knn_stencils(const double *xyz, const uint8_t *boundary, int n
     cudaStream_t st = S(s);
     dbuf<double> tx;
     dbuf<uint8_t> tb;
-    const double *dx;
-    const uint8_t *db;
+    const double *dx = nullptr;
+    const uint8_t *db = nullptr;
     MP_TRY(stage_in(xyz, (size_t)nv * dim, tx, &dx, st));
     MP_TRY(stage_in(boundary, (size_t)nv, tb, &db, st));
     int *dn = nb_col;
@@ -444,7 +444,7 @@ extern "C" int mp_knn_probe(const double *xyz, int nv, int dim, const double *pr
     cudaStream_t st = S(s);
     dbuf<double> tx, tp;
     dbuf<int> tc;
-    const double *dx, *dp;
+    const double *dx = nullptr, *dp = nullptr;
     MP_TRY(stage_in(xyz, (size_t)nv * dim, tx, &dx, st));
     MP_TRY(stage_in(probe, (size_t)np * dim, tp, &dp, st));
     int *dc = cols;

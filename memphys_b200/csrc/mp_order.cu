@@ -185,7 +185,7 @@ extern "C" int mp_order_morton(const double *xyz, int nv, int dim, int *order, m
         return fail(MP_BAD_ARG, "mp_order_morton: bad arguments");
     cudaStream_t st = S(s);
     dbuf<double> tx, box;
-    const double *dx;
+    const double *dx = nullptr;
     MP_TRY(stage_in(xyz, (size_t)nv * dim, tx, &dx, st));
     dbuf<uint64_t> key, key2;
     dbuf<int> idx, idx2, dord;
@@ -227,7 +227,7 @@ extern "C" int mp_permute_stencils(const int *nb, int nv, int n, const int *orde
         return fail(MP_BAD_ARG, "mp_permute_stencils: bad arguments");
     cudaStream_t st = S(s);
     dbuf<int> tn, to, tout, bad;
-    const int *dn, *dord;
+    const int *dn = nullptr, *dord = nullptr;
     MP_TRY(stage_in(nb, (size_t)nv * n, tn, &dn, st));
     MP_TRY(stage_in(order, (size_t)nv, to, &dord, st));
     int *dout = nb_out;
@@ -259,8 +259,8 @@ extern "C" int mp_permute_rows(const void *in, void *out, int nv, int row_bytes,
     const size_t tot = (size_t)nv * row_bytes;
     dbuf<unsigned char> ti, tout;
     dbuf<int> to;
-    const unsigned char *di;
-    const int *dord;
+    const unsigned char *di = nullptr;
+    const int *dord = nullptr;
     MP_TRY(stage_in((const unsigned char *)in, tot, ti, &di, st));
     MP_TRY(stage_in(order, (size_t)nv, to, &dord, st));
     unsigned char *dout = (unsigned char *)out;

@@ -759,8 +759,8 @@ extern "C" int mp_stencil_weights(const double *xyz, int nv, int dim, const int 
         return fail(MP_BAD_ARG, "mp_stencil_weights: null argument");
     dbuf<double> txyz;
     dbuf<int> tnb;
-    const double *dxyz;
-    const int *dnb;
+    const double *dxyz = nullptr;
+    const int *dnb = nullptr;
     MP_TRY(stage_in(xyz, (size_t)nv * dim, txyz, &dxyz, st));
     MP_TRY(stage_in(nb_col, (size_t)nv * n, tnb, &dnb, st));
     // outputs: device pointers written in place, host pointers staged back
@@ -829,9 +829,9 @@ extern "C" int mp_stencil_weights_batched(int nsys, const int *sizes, const int6
     dbuf<int> dsizes, dlist[3];
     dbuf<int64_t> doff;
     dbuf<double> dpts, dw, dcond;
-    const int *psz;
-    const int64_t *pof;
-    const double *ppts;
+    const int *psz = nullptr;
+    const int64_t *pof = nullptr;
+    const double *ppts = nullptr;
     MP_TRY(stage_in(sizes, nsys, dsizes, &psz, st));
     MP_TRY(stage_in(offsets, nsys, doff, &pof, st));
     MP_TRY(stage_in(pts, (size_t)npts * dim, dpts, &ppts, st));
@@ -923,7 +923,7 @@ extern "C" int mp_interp_matrix(const double *xyz, int nv, int dim, const double
         return fail(MP_BAD_ARG, "mp_interp_matrix: bad arguments");
     dbuf<double> tx, tp, tw;
     dbuf<int> tc;
-    const double *dx, *dp;
+    const double *dx = nullptr, *dp = nullptr;
     MP_TRY(stage_in(xyz, (size_t)nv * dim, tx, &dx, st));
     MP_TRY(stage_in(probe, (size_t)np * dim, tp, &dp, st));
     int *dc = cols;
