@@ -230,3 +230,21 @@ def test_oracle_threads_do_not_change_results():
         oracle.set_threads(prev)
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+def test_fourier_transforms_as_the_reference_writes_them():
+    # get_dft_matrix / get_idft_matrix (general_functions.cpp:1106-1123) divide the
+    # phase by the period: the pair inverts for period 1 only, and the step follows
+    # the matrices as written (the GPU path reproduces them for parity)
+    from oracle import fsf as ofsf
+    cl = clouds.cavity_2d(6, seed=1)
+    nb = oracle.knn_stencils(cl.xyz, cl.boundary, 20)
+    w = oracle.cloud_weights(cl.xyz, nb, 3, 3, cond=False)
+    x = np.random.default_rng(0).standard_normal((cl.nv, 5))
+    err = {}
+    for period in (1.0, 1.7):
+        f = ofsf.FSF(cl, nb, w, 1.0, 0.01, 1e-3, cl.u_dirichlet, cl.v_dirichlet,
+                     cl.u_dirichlet, cl.p_dirichlet, period, 2)
+        err[period] = np.abs(f.idft(f.dft(x)) - x).max()
+    assert err[1.0] < 1e-14
+    assert err[1.7] > 0.1
