@@ -2,7 +2,9 @@
 //
 // Class names, member names and argument order follow the reference's
 // header_files/class.hpp (PARAMETERS :58-94, POINTS :96-140, CLOUD :142-169,
-// SOLVER :171-217, FRACTIONAL_STEP_1 :246-270), with std::vector<double> in
+// SOLVER :171-217, FRACTIONAL_STEP_1 :246-270, FRACTIONAL_STEP_FOURIER :272-335,
+// IMPLICIT_SCALAR_TRANSPORT_SOLVER :395-415, SEMI_IMPLICIT_SPLIT_SOLVER :417-455),
+// with std::vector<double> in
 // place of Eigen::VectorXd.  Every non-OK status is printed with
 // mp_last_error() and turned into `throw std::bad_exception()`, the
 // reference's error convention (e.g. solver.cpp:317-321).
@@ -220,5 +222,170 @@ class FRACTIONAL_STEP_1 {
         check(rc, "FRACTIONAL_STEP_1::single_timestep_2d");
     }
 };
+
+// implicit_scalar_transport_solver.cpp / class.hpp:395-415 (2D)
+class IMPLICIT_SCALAR_TRANSPORT_SOLVER {
+  public:
+    mp_ist handle = nullptr;
+    bool solver_log_flag = false;
+    std::vector<unsigned char> d;
+
+    IMPLICIT_SCALAR_TRANSPORT_SOLVER(POINTS &points, CLOUD &cloud, PARAMETERS &parameters,
+                                     std::vector<bool> &dirichlet_flag1, int precond_freq_it1,
+                                     double unsteady_coeff1, double conv_coeff1, double diff_coeff1,
+                                     bool solver_log_flag1)
+        : solver_log_flag(solver_log_flag1) {
+        d.assign(dirichlet_flag1.begin(), dirichlet_flag1.end());
+        mp_solver_cfg c = parameters.solver_cfg();
+        c.precond = MP_PRECOND_JACOBI;  // the matrix changes every step
+        c.precision = MP_FP64;
+        check(mp_ist_create(cloud.handle, points.boundary_flag.data(), points.normal.data(), d.data(),
+                            precond_freq_it1, unsteady_coeff1, conv_coeff1, diff_coeff1, &c, &handle),
+              "IMPLICIT_SCALAR_TRANSPORT_SOLVER::IMPLICIT_SCALAR_TRANSPORT_SOLVER");
+    }
+    IMPLICIT_SCALAR_TRANSPORT_SOLVER(const IMPLICIT_SCALAR_TRANSPORT_SOLVER &) = delete;
+    IMPLICIT_SCALAR_TRANSPORT_SOLVER &operator=(const IMPLICIT_SCALAR_TRANSPORT_SOLVER &) = delete;
+    ~IMPLICIT_SCALAR_TRANSPORT_SOLVER() { mp_ist_destroy(handle); }
+
+    // :136-174; with solver_log_flag the residual and iterations are logged in parameters
+    void single_timestep_2d(POINTS &points, CLOUD &, PARAMETERS &parameters,
+                            std::vector<double> &phi_new, std::vector<double> &phi_old,
+                            std::vector<double> &u_new, std::vector<double> &v_new, int it1) {
+        phi_new.resize(points.nv);
+        int iters = 0;
+        double rel = 0;
+        check(mp_ist_single_timestep(handle, phi_old.data(), u_new.data(), v_new.data(),
+                                     phi_new.data(), it1, &iters, &rel, nullptr),
+              "IMPLICIT_SCALAR_TRANSPORT_SOLVER::single_timestep_2d");
+        if (solver_log_flag) {
+            parameters.rel_res_log.push_back(rel);
+            parameters.n_iter_actual.push_back(iters);
+        }
+    }
+};
+
+// semi_implicit_split_solver.cpp / class.hpp:417-455 (2D)
+class SEMI_IMPLICIT_SPLIT_SOLVER {
+  public:
+    mp_sis handle = nullptr;
+    int system_size = 0;
+    std::vector<unsigned char> u_d, v_d, p_d;
+
+    SEMI_IMPLICIT_SPLIT_SOLVER(POINTS &points, CLOUD &cloud, PARAMETERS &parameters,
+                               std::vector<bool> &u_dirichlet_flag1,
+                               std::vector<bool> &v_dirichlet_flag1,
+                               std::vector<bool> &p_dirichlet_flag1, int n_outer_iter1,
+                               double iterative_tolerance1, int precond_freq_it1) {
+        u_d.assign(u_dirichlet_flag1.begin(), u_dirichlet_flag1.end());
+        v_d.assign(v_dirichlet_flag1.begin(), v_dirichlet_flag1.end());
+        p_d.assign(p_dirichlet_flag1.begin(), p_dirichlet_flag1.end());
+        mp_sis_cfg cfg{parameters.rho, parameters.mu, parameters.dt, n_outer_iter1,
+                       iterative_tolerance1, precond_freq_it1};
+        mp_solver_cfg vel = parameters.solver_cfg(), pres = parameters.solver_cfg();
+        vel.precond = MP_PRECOND_JACOBI;  // the velocity matrices change every outer iteration
+        vel.precision = MP_FP64;
+        check(mp_sis_create(cloud.handle, points.boundary_flag.data(), points.normal.data(),
+                            u_d.data(), v_d.data(), p_d.data(), &cfg, &vel, &pres, &handle),
+              "SEMI_IMPLICIT_SPLIT_SOLVER::SEMI_IMPLICIT_SPLIT_SOLVER");
+        check(mp_sis_system_size(handle, &system_size), "SEMI_IMPLICIT_SPLIT_SOLVER");
+    }
+    SEMI_IMPLICIT_SPLIT_SOLVER(const SEMI_IMPLICIT_SPLIT_SOLVER &) = delete;
+    SEMI_IMPLICIT_SPLIT_SOLVER &operator=(const SEMI_IMPLICIT_SPLIT_SOLVER &) = delete;
+    ~SEMI_IMPLICIT_SPLIT_SOLVER() { mp_sis_destroy(handle); }
+
+    // :376-421
+    void single_timestep_2d(POINTS &points, CLOUD &, PARAMETERS &, std::vector<double> &u_new,
+                            std::vector<double> &v_new, std::vector<double> &p_new,
+                            std::vector<double> &u_old, std::vector<double> &v_old,
+                            std::vector<double> &p_old, int it1,
+                            std::vector<int> &n_outer_iter_log,
+                            std::vector<double> &iterative_l1_err_log,
+                            std::vector<double> &iterative_max_err_log) {
+        if ((int)p_new.size() != system_size)  // :380-383
+            p_new.assign(system_size, 0.0);
+        if ((int)p_old.size() != system_size)
+            p_old.assign(system_size, 0.0);
+        u_new.resize(points.nv);
+        v_new.resize(points.nv);
+        const double *vo[2] = {u_old.data(), v_old.data()};
+        double *vn[2] = {u_new.data(), v_new.data()};
+        int n = 0;
+        double l1 = 0, mx = 0;
+        check(mp_sis_single_timestep(handle, vo, p_old.data(), vn, p_new.data(), it1, &n, &l1, &mx,
+                                     nullptr),
+              "SEMI_IMPLICIT_SPLIT_SOLVER::single_timestep_2d");
+        n_outer_iter_log.push_back(n);
+        iterative_l1_err_log.push_back(l1);
+        iterative_max_err_log.push_back(mx);
+    }
+};
+
+// fractional_step_fourier.cpp / class.hpp:272-335 (2D cloud, Fourier in z); each
+// field is nv x (2 nw + 1), column-major like the reference's Eigen::MatrixXd
+class FRACTIONAL_STEP_FOURIER {
+  public:
+    mp_fsf handle = nullptr;
+    int nv = 0, nplanes = 0;
+    std::vector<unsigned char> u_d, v_d, w_d, p_d;
+
+    FRACTIONAL_STEP_FOURIER(POINTS &points, CLOUD &cloud, PARAMETERS &parameters,
+                            std::vector<bool> &u_dirichlet_flag1,
+                            std::vector<bool> &v_dirichlet_flag1,
+                            std::vector<bool> &w_dirichlet_flag1,
+                            std::vector<bool> &p_dirichlet_flag1, double period1, int nw1,
+                            int temporal_order1)
+        : nv(points.nv), nplanes(2 * nw1 + 1) {
+        u_d.assign(u_dirichlet_flag1.begin(), u_dirichlet_flag1.end());
+        v_d.assign(v_dirichlet_flag1.begin(), v_dirichlet_flag1.end());
+        w_d.assign(w_dirichlet_flag1.begin(), w_dirichlet_flag1.end());
+        p_d.assign(p_dirichlet_flag1.begin(), p_dirichlet_flag1.end());
+        mp_solver_cfg c = parameters.solver_cfg();
+        check(mp_fsf_create(cloud.handle, points.boundary_flag.data(), points.normal.data(),
+                            u_d.data(), v_d.data(), w_d.data(), p_d.data(), period1, nw1,
+                            temporal_order1, parameters.rho, parameters.mu, parameters.dt, &c,
+                            &handle),
+              "FRACTIONAL_STEP_FOURIER::FRACTIONAL_STEP_FOURIER");
+    }
+    FRACTIONAL_STEP_FOURIER(const FRACTIONAL_STEP_FOURIER &) = delete;
+    FRACTIONAL_STEP_FOURIER &operator=(const FRACTIONAL_STEP_FOURIER &) = delete;
+    ~FRACTIONAL_STEP_FOURIER() { mp_fsf_destroy(handle); }
+
+    // :250-266
+    void single_timestep(POINTS &, CLOUD &, PARAMETERS &, std::vector<double> &u_new,
+                         std::vector<double> &v_new, std::vector<double> &w_new,
+                         std::vector<double> &p_new, std::vector<double> &u_old,
+                         std::vector<double> &v_old, std::vector<double> &w_old,
+                         std::vector<double> &p_old, int it1) {
+        const size_t m = (size_t)nv * nplanes;
+        for (std::vector<double> *a : {&u_new, &v_new, &w_new, &p_new})
+            a->resize(m);
+        const double *vo[3] = {u_old.data(), v_old.data(), w_old.data()};
+        double *vn[3] = {u_new.data(), v_new.data(), w_new.data()};
+        check(mp_fsf_single_timestep(handle, vo, p_old.data(), vn, p_new.data(), it1, nullptr),
+              "FRACTIONAL_STEP_FOURIER::single_timestep");
+    }
+};
+
+// calc_interp_matrix (coefficient_computations.cpp:456-518): the rows of the
+// interpolation matrix, row i = probe i, cloud_size entries each
+struct INTERP_MATRIX {
+    int rows = 0, width = 0;
+    std::vector<int> cols;
+    std::vector<double> vals;
+};
+
+inline INTERP_MATRIX calc_interp_matrix(std::vector<double> &xyz_probe, POINTS &points,
+                                        PARAMETERS &parameters) {
+    INTERP_MATRIX m;
+    m.rows = (int)(xyz_probe.size() / parameters.dimension);
+    m.width = parameters.cloud_size;
+    m.cols.resize((size_t)m.rows * m.width);
+    m.vals.resize((size_t)m.rows * m.width);
+    check(mp_interp_matrix(points.xyz.data(), points.nv, parameters.dimension, xyz_probe.data(),
+                           m.rows, m.width, parameters.phs_deg, parameters.poly_deg, m.cols.data(),
+                           m.vals.data(), nullptr),
+          "calc_interp_matrix");
+    return m;
+}
 
 }  // namespace memphys
