@@ -11,8 +11,12 @@ reference checkout; the fixtures are committed so tests never need it).
   knn_cavity.npz      a 40x40 jittered cavity and its nanoflann stencils.
   lapack_stencils.npz 240 uneven independent PHS systems (2D and 3D) and
                       their weights from scipy's LAPACK dgesv.
+  couette_clouds.npz  the concentric annuli CAD_Mesh_files/ecc_ratio_0.0_r_i_0.5_n_100
+                      and _n_150.msh read by the restated gmsh reader (xyz,
+                      boundary flags, normals), for the concentric-Couette check
+                      against the analytic profile of the reference's driver.
 
-usage: python tests/golden/make_golden.py [reference_root]
+usage: python tests/golden/make_golden.py [reference_root] [--only couette]
 """
 from __future__ import annotations
 
@@ -155,7 +159,25 @@ def _lapack_weights(x, e, m, lapack):
     return sol[:n].T.copy()  # (dim+1, n)
 
 
-def main(ref_root="/root/reference"):
+def couette_clouds(ref_root):
+    out = {}
+    for n in (100, 150):
+        mesh = os.path.join(ref_root, "MeMPhyS Latest Version", "CAD_Mesh_files",
+                            f"ecc_ratio_0.0_r_i_0.5_n_{n}.msh")
+        xyz, bnd, nrm = msh.read_msh_2d(mesh)
+        out[f"xyz_{n}"], out[f"boundary_{n}"], out[f"normal_{n}"] = xyz, bnd, nrm
+    np.savez_compressed(os.path.join(HERE, "couette_clouds.npz"), **out)
+
+
+def main(ref_root="/root/reference", *flags):
+    if "--only" in flags:
+        what = flags[flags.index("--only") + 1]
+        if what == "couette":
+            couette_clouds(ref_root)
+            print("couette_clouds.npz written to", HERE)
+            return
+        raise SystemExit(f"unknown fixture {what}")
+    couette_clouds(ref_root)
     stats = sample_stats(ref_root)
     with open(os.path.join(HERE, "sample_stats.json"), "w") as f:
         json.dump(stats, f, indent=1)
