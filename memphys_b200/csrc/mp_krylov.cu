@@ -1,6 +1,7 @@
 // mp_krylov.cu -- pressure-Poisson system assembly and BiCGSTAB (FP64, and
 // FP32 inner iterations under FP64 iterative refinement), with the mp_ppe_*
 // C ABI (SOLVER::init / SOLVER::general_solve, solver.cpp:14-79, 283-363).
+#include <cstddef>
 #include <cmath>
 #include "mp_krylov.cuh"
 #include "mp_amg.cuh"
@@ -878,7 +879,8 @@ int Ppe::read_stats(cudaStream_t st, SolveStats *out) {
 
 int Ppe::set_abs_tol(double atol, cudaStream_t st) {
     const double a2 = atol * atol;
-    MP_CUDA(cudaMemcpyAsync(&W.scal.p->abs_tol2, &a2, sizeof(double), cudaMemcpyHostToDevice, st));
+    char *field = reinterpret_cast<char *>(W.scal.p) + offsetof(BicgScalars, abs_tol2);
+    MP_CUDA(cudaMemcpyAsync(field, &a2, sizeof(double), cudaMemcpyHostToDevice, st));
     MP_CUDA(cudaStreamSynchronize(st));  // a2 lives on this stack frame
     return MP_OK;
 }
