@@ -2,6 +2,9 @@
 
   calc_max_l1_error                   general_functions.cpp:940-1032
   calc_navier_stokes_residuals_2D     postprocessing_functions.cpp:182-208 (operators on the GPU)
+  write_navier_stokes_residuals_2D    :370-401
+  calc_navier_stokes_errors_2D / write_navier_stokes_errors_2D   :154-180, :336-368
+  write_iteration_details             :52-72
   write_tecplot_steady_variables      :765-805
   write_tecplot_temporal_variables_header / write_tecplot_temporal_variables   :403-416, :476-509
   read_restart_tecplot_file           :597-682 (nearest node by the GPU probe kNN)
@@ -60,6 +63,103 @@ def calc_navier_stokes_residuals_2D(points, cloud, parameters, u, v, p):
         m, l1 = calc_max_l1_error(zero, r)
         out[k] = {"internal": (mi, li), "boundary": (mb, lb), "overall": (m, l1)}
     return out
+
+
+_ERR_HEAD = ",max_internal,avg_internal,max_boundary,avg_boundary,max_overall,avg_overall\n"
+
+
+def _split_row(name, a1, a2, boundary_flag):
+    """name, then (max, mean) internal, boundary, overall; the split covers the first
+    nv entries (the reference indexes the flags past nv for a bordered pressure)."""
+    nv = len(boundary_flag)
+    mb, lb, mi, li = calc_max_l1_error(np.asarray(a1)[:nv], np.asarray(a2)[:nv], boundary_flag)
+    m, l1 = calc_max_l1_error(a1, a2)
+    return name, (mi, li, mb, lb, m, l1)
+
+
+def _row_text(name, vals):
+    return name + "".join(f",{v:.16g}" for v in vals) + "\n"
+
+
+def _residual_rows(points, cloud, parameters, u, v, p):
+    gx = cloud.operator(capi.MP_GRAD_X)
+    gy = cloud.operator(capi.MP_GRAD_Y)
+    lap = cloud.operator(capi.MP_LAPLACIAN)
+    u, v = np.asarray(u, np.float64), np.asarray(v, np.float64)
+    ph = np.asarray(p, np.float64)[: points.nv]
+    rho, mu = parameters.rho, parameters.mu
+    zero = np.zeros(points.nv)
+    return [
+        _split_row("continuity", zero, gx @ u + gy @ v, points.boundary_flag),
+        _split_row("X-mom", zero, u * (gx @ u) + v * (gy @ u) - (mu * (lap @ u) / rho)
+                   + (gx @ ph) / rho, points.boundary_flag),
+        _split_row("Y-mom", zero, u * (gx @ v) + v * (gy @ v) - (mu * (lap @ v) / rho)
+                   + (gy @ ph) / rho, points.boundary_flag),
+    ]
+
+
+def write_navier_stokes_residuals_2D(prefix, suffix, points, cloud, parameters, u, v, p):
+    """<prefix><suffix>: the residual table of :370-401 (GPU operators)."""
+    if parameters.rho < 0 or parameters.mu < 0:
+        raise capi.MemphysError(capi.MP_BAD_ARG, "write_navier_stokes_residuals_2D: set rho and mu")
+    path = prefix + suffix
+    with open(path, "w") as f:
+        f.write("Numerical,Residuals,wrt,Given,solution\n" + _ERR_HEAD)
+        for name, vals in _residual_rows(points, cloud, parameters, u, v, p):
+            f.write(_row_text(name, vals))
+    return path
+
+
+def calc_navier_stokes_errors_2D(points, cloud, u_ana, v_ana, p_ana, u_num, v_num, p_num):
+    """Continuity residual and the errors of u, v, p against an analytic solution
+    (:154-180), as {name: (max_internal, avg_internal, max_boundary, avg_boundary,
+    max_overall, avg_overall)}.  The pressure is shifted to the analytic level at
+    node 0 first; the inputs are not modified (the reference shifts p_num in place)."""
+    gx = cloud.operator(capi.MP_GRAD_X)
+    gy = cloud.operator(capi.MP_GRAD_Y)
+    zero = np.zeros(points.nv)
+    pn = np.asarray(p_num, np.float64).copy()
+    pa = np.asarray(p_ana, np.float64).copy()
+    pn = pn - (pn[0] - pa[0])
+    if len(pa) == points.nv + 1:
+        pa[points.nv] = 0.0
+        pn[points.nv] = 0.0
+    rows = [
+        _split_row("continuity", zero, gx @ np.asarray(u_num, np.float64)
+                   + gy @ np.asarray(v_num, np.float64), points.boundary_flag),
+        _split_row("U X-vel", u_ana, u_num, points.boundary_flag),
+        _split_row("V Y-vel", v_ana, v_num, points.boundary_flag),
+        _split_row("Pressure", pa, pn, points.boundary_flag),
+    ]
+    return dict(rows)
+
+
+def write_navier_stokes_errors_2D(prefix, points, cloud, u_ana, v_ana, p_ana, u_num, v_num,
+                                  p_num):
+    """<prefix>_navier_stokes_errors.csv: the table of :336-368."""
+    path = prefix + "_navier_stokes_errors.csv"
+    errs = calc_navier_stokes_errors_2D(points, cloud, u_ana, v_ana, p_ana, u_num, v_num, p_num)
+    with open(path, "w") as f:
+        f.write("Errors,wrt,Analytical,solution\n" + _ERR_HEAD)
+        for name, vals in errs.items():
+            f.write(_row_text(name, vals))
+    return path
+
+
+def write_iteration_details(prefix, n_iter_actual, rel_res_log, abs_res_log, regul_alpha_log=()):
+    """<prefix>_iteration_details.csv (:52-72): one row per logged solve."""
+    path = prefix + "_iteration_details.csv"
+    with open(path, "w") as f:
+        if len(regul_alpha_log) == 0:
+            f.write("it,n_iter_actual,rel_res_log,abs_res_log\n")
+            for it, (n, r, a) in enumerate(zip(n_iter_actual, rel_res_log, abs_res_log)):
+                f.write(f"{it},{int(n)},{r:.16g},{a:.16g}\n")
+        else:
+            f.write("it,n_iter_actual,rel_res_log,abs_res_log,regul_alpha_log\n")
+            for it, (n, r, a, g) in enumerate(zip(n_iter_actual, rel_res_log, abs_res_log,
+                                                   regul_alpha_log)):
+                f.write(f"{it},{int(n)},{r:.16g},{a:.16g},{g:.16g}\n")
+    return path
 
 
 def _original(points):

@@ -60,3 +60,53 @@ def test_max_l1_error_split():
     assert post.calc_max_l1_error(b, a) == (3.0, 1.5)
     mb, lb, mi, li = post.calc_max_l1_error(b, a, np.array([1, 0, 1, 0]))
     assert (mb, lb, mi, li) == (3.0, 1.5, 2.0, 1.5)
+
+
+class _CpuCloud:
+    """Operators as scipy matrices: the post-processing code only applies them."""
+
+    def __init__(self, ops):
+        self.ops = ops
+
+    def operator(self, which):
+        return self.ops[which]
+
+
+def test_error_and_residual_tables(tmp_path):
+    import scipy.sparse as sp
+    from memphys_b200 import capi
+    rng = np.random.default_rng(3)
+    nv = 6
+    gx, gy, lap = (sp.csr_matrix(rng.standard_normal((nv, nv))) for _ in range(3))
+    cloud = _CpuCloud({capi.MP_GRAD_X: gx, capi.MP_GRAD_Y: gy, capi.MP_LAPLACIAN: lap})
+    pts = types.SimpleNamespace(nv=nv, dim=2, boundary_flag=np.array([1, 0, 0, 1, 0, 0], np.uint8))
+    u, v = rng.standard_normal(nv), rng.standard_normal(nv)
+    p = np.append(rng.standard_normal(nv), 0.7)         # bordered pressure
+    ua, va, pa = u + 0.01, v - 0.02, p + 5.0             # a level shift of p is no error
+    e = post.calc_navier_stokes_errors_2D(pts, cloud, ua, va, pa, u, v, p)
+    assert np.allclose(e["U X-vel"], (0.01, 0.01, 0.01, 0.01, 0.01, 0.01))
+    assert np.allclose(e["Pressure"], 0.0, atol=1e-14)
+    cont = gx @ u + gy @ v
+    b = pts.boundary_flag.astype(bool)
+    assert np.isclose(e["continuity"][0], np.abs(cont[~b]).max())
+    path = post.write_navier_stokes_errors_2D(str(tmp_path / "r"), pts, cloud, ua, va, pa, u, v, p)
+    lines = open(path).read().splitlines()
+    assert lines[0] == "Errors,wrt,Analytical,solution"
+    assert lines[1] == ",max_internal,avg_internal,max_boundary,avg_boundary,max_overall,avg_overall"
+    assert [l.split(",")[0] for l in lines[2:]] == ["continuity", "U X-vel", "V Y-vel", "Pressure"]
+    prm = types.SimpleNamespace(rho=2.0, mu=0.5)
+    path = post.write_navier_stokes_residuals_2D(str(tmp_path / "r"), "_res.csv", pts, cloud, prm,
+                                                 u, v, p)
+    rows = open(path).read().splitlines()
+    xm = u * (gx @ u) + v * (gy @ u) - 0.5 * (lap @ u) / 2.0 + (gx @ p[:nv]) / 2.0
+    assert rows[3].startswith("X-mom,")
+    vals = [float(x) for x in rows[3].split(",")[1:]]
+    assert np.isclose(vals[4], np.abs(xm).max()) and np.isclose(vals[5], np.abs(xm).mean())
+
+
+def test_iteration_details(tmp_path):
+    path = post.write_iteration_details(str(tmp_path / "r"), [12, 9], [1e-9, 2.5e-9], [0.5, 0.25])
+    assert open(path).read() == ("it,n_iter_actual,rel_res_log,abs_res_log\n"
+                                 "0,12,1e-09,0.5\n1,9,2.5e-09,0.25\n")
+    path = post.write_iteration_details(str(tmp_path / "s"), [3], [1e-9], [0.5], [0.125])
+    assert open(path).read().splitlines()[1] == "0,3,1e-09,0.5,0.125"
