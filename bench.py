@@ -379,12 +379,20 @@ def run_ours(args, ws, rank, local, pg):
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(cl, cld)
+    # supplementary workloads: a failure in one is reported in its own field and
+    # does not cost the headline line
+    legs = []
     if args.batched > 0:
-        out["batched_stencils"] = batched_stencils(args.batched)
+        legs.append(("batched_stencils", lambda: batched_stencils(args.batched)))
     if ws == 1 and not args.no_cube:
-        out["cube3d_mixed"] = cube_mixed(args, stream)
+        legs.append(("cube3d_mixed", lambda: cube_mixed(args, stream)))
     if ws == 1 and not args.no_channel:
-        out["channel_learned"] = channel_learned(args, stream)
+        legs.append(("channel_learned", lambda: channel_learned(args, stream)))
+    for name, run in legs:
+        try:
+            out[name] = run()
+        except Exception as e:  # noqa: BLE001 -- any failure is reported, not raised
+            out[name] = {"error": f"{type(e).__name__}: {e}"[:400]}
     return out
 
 
