@@ -212,12 +212,29 @@ int mp_op_apply(mp_op op, const void *x, void *y, double alpha, double beta, mp_
 /* y_k = A_k x for up to 4 operators sharing one column structure (one pass over the indices) */
 int mp_op_apply_multi(int nops, const mp_op *ops, const void *x, void *const *ys, mp_stream s);
 int mp_op_info(mp_op op, int *nrows, int *ncols, int *width, int *precision);
+/*
+ * calc_largest_magnitude_eigenvalue (general_functions.cpp:4-24; Spectra
+ * GenEigsSolver, LARGEST_MAGN), used by PARAMETERS::calc_dt (parameters.cpp:269-296):
+ * the eigenvalue of largest magnitude of a square FP64 operator, by explicitly
+ * restarted Arnoldi with ncv vectors (>= 3; 30 is a good default) on the GPU.  It
+ * stops once the Ritz residual is <= tol * |lambda| (MP_OK) or after max_restarts
+ * cycles (MP_NOT_CONVERGED, with the last estimate written).  Of a complex-conjugate
+ * pair the member with positive imaginary part is returned.  The start vector is a
+ * fixed function of `seed`.  Allocates (ncv + 2) work vectors; synchronises `s`.
+ */
+int mp_op_largest_eig(mp_op op, int ncv, double tol, int max_restarts, uint64_t seed,
+                      double *re, double *im, int *restarts, mp_stream s);
 int mp_op_destroy(mp_op op);
 
 /* --------------------------------------------------------- pressure solve */
 typedef struct mp_ppe_s *mp_ppe;
 
-enum { MP_PRECOND_NONE = 0, MP_PRECOND_JACOBI = 1, MP_PRECOND_AMG = 2 };
+/* MP_PRECOND_SOR is the reference's `sor` solver type (SOLVER::SOR, solver.cpp:243-281):
+ * no Krylov method, SOR sweeps with relaxation sor_omega on the unbordered system
+ * (solver.cpp:30-31), rows in multicolour order; maxit sweeps at most, stopping once
+ * ||b - A x|| / ||b|| <= tol.  FP64 only; accepted by mp_ppe_* (SOLVER), not by the
+ * graph-captured integrators. */
+enum { MP_PRECOND_NONE = 0, MP_PRECOND_JACOBI = 1, MP_PRECOND_AMG = 2, MP_PRECOND_SOR = 3 };
 /* initial guess of each fractional-step pressure solve: the previous pressure
  * (the reference's solveWithGuess(rhs, p_old)), zero, the linear extrapolation
  * 2 p^n - p^(n-1), the projection p^n + sum_j c_j (p^(j+1) - p^j) over the last
@@ -241,6 +258,7 @@ typedef struct {
     int smoother_sweeps;  /* degree-2 Chebyshev applications before and after each coarse correction */
     double cheb_lower;    /* Chebyshev interval [cheb_lower * lambda_max, 1.1 lambda_max] of D^-1 A */
     int guess_vectors;    /* MP_GUESS_PROJECT / MP_GUESS_LEARNED: pressure increments kept, 1-8 (8) */
+    double sor_omega;     /* MP_PRECOND_SOR relaxation, (0, 2); 1.4 as class.hpp:212 */
 } mp_solver_cfg;
 
 /* sensible defaults for the fields above */

@@ -20,7 +20,7 @@ MP_OK, MP_NOT_CONVERGED, MP_BREAKDOWN, MP_NAN_DETECTED, MP_SINGULAR_STENCIL, MP_
 MP_FP64, MP_FP32, MP_MG32 = 0, 1, 2
 MP_GRAD_X, MP_GRAD_Y, MP_GRAD_Z, MP_LAPLACIAN = range(4)
 MP_ROWS_ALL, MP_ROWS_INTERNAL, MP_ROWS_BOUNDARY = range(3)
-MP_PRECOND_NONE, MP_PRECOND_JACOBI, MP_PRECOND_AMG = range(3)
+MP_PRECOND_NONE, MP_PRECOND_JACOBI, MP_PRECOND_AMG, MP_PRECOND_SOR = range(4)
 MP_GUESS_PREVIOUS, MP_GUESS_ZERO, MP_GUESS_LEARNED, MP_GUESS_EXTRAPOLATE, MP_GUESS_PROJECT = range(5)
 MP_LOG_FIELDS = 8
 
@@ -42,7 +42,7 @@ EXPORTS = [
     "mp_stencil_weights",
     "mp_stencil_weights_batched", "mp_cloud_create", "mp_cloud_create_stencils", "mp_cloud_info",
     "mp_cloud_get", "mp_cloud_destroy", "mp_op_create_ell", "mp_op_from_cloud", "mp_op_apply",
-    "mp_op_apply_multi", "mp_op_info", "mp_op_destroy", "mp_solver_cfg_default", "mp_ppe_create",
+    "mp_op_apply_multi", "mp_op_info", "mp_op_largest_eig", "mp_op_destroy", "mp_solver_cfg_default", "mp_ppe_create",
     "mp_ppe_system_size", "mp_ppe_solve", "mp_ppe_destroy", "mp_fs1_create",
     "mp_fs1_system_size", "mp_fs1_set_state", "mp_fs1_get_state", "mp_fs1_step",
     "mp_fs1_single_timestep", "mp_fs1_last_stats", "mp_fs1_log", "mp_fs1_kernel_counts",
@@ -69,7 +69,7 @@ class SolverCfg(C.Structure):
                 ("precision", C.c_int), ("guess", C.c_int), ("inner_tol", C.c_double),
                 ("amg_max_levels", C.c_int), ("amg_coarse_size", C.c_int),
                 ("smoother_sweeps", C.c_int), ("cheb_lower", C.c_double),
-                ("guess_vectors", C.c_int)]
+                ("guess_vectors", C.c_int), ("sor_omega", C.c_double)]
 
 
 class Fs1Cfg(C.Structure):
@@ -128,6 +128,8 @@ def lib() -> C.CDLL:
             "mp_op_from_cloud": [vp, i, i, i, C.POINTER(vp)],
             "mp_op_apply": [vp, vp, vp, d, d, vp], "mp_op_apply_multi": [i, vp, vp, vp, vp],
             "mp_op_info": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)],
+            "mp_op_largest_eig": [vp, i, d, i, C.c_uint64, C.POINTER(d), C.POINTER(d),
+                                  C.POINTER(i), vp],
             "mp_op_destroy": [vp], "mp_solver_cfg_default": [C.POINTER(SolverCfg)],
             "mp_ppe_create": [vp, vp, vp, vp, d, d, d, C.POINTER(SolverCfg), C.POINTER(vp)],
             "mp_ppe_system_size": [vp],

@@ -191,6 +191,15 @@ struct mp_op_s {
     const int *cols() const { return shared_cols ? shared_cols->cols.p : E.cols.p; }
 };
 
+namespace mp {
+int op_view64(mp_op op, EllView<double> *view) {
+    if (!op || op->precision != MP_FP64 || !op->E.v64.p)
+        return fail(MP_BAD_ARG, "an FP64 operator is required");
+    *view = EllView<double>{op->E.nrows, op->E.ncols, op->E.K, op->cols(), op->E.v64.p, nullptr};
+    return MP_OK;
+}
+}  // namespace mp
+
 extern "C" int mp_op_create_ell(int nrows, int ncols, int width, const int *cols,
                                 const double *vals, int precision, mp_op *out) {
     if (!out || !cols || !vals)

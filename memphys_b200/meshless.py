@@ -29,6 +29,8 @@ SOLVER_TYPES = {
     "cuda_bicgstab_jacobi": dict(precond=capi.MP_PRECOND_JACOBI, precision=capi.MP_FP64),
     "cuda_bicgstab_jacobi_mixed": dict(precond=capi.MP_PRECOND_JACOBI, precision=capi.MP_FP32),
     "cuda_bicgstab": dict(precond=capi.MP_PRECOND_NONE, precision=capi.MP_FP64),
+    # SOLVER::SOR (solver.cpp:243-281): SOR sweeps, omega 1.4, unbordered system
+    "sor": dict(precond=capi.MP_PRECOND_SOR, precision=capi.MP_FP64),
 }
 
 
@@ -85,7 +87,7 @@ class PARAMETERS:
             raise capi.MemphysError(capi.MP_BAD_ARG, f"phs_deg should be 3, 5, 7, 9, or 11; "
                                                      f"current value: {self.phs_deg}")
         self.solver_type = self.solver_type.lower()
-        if self.solver_type not in SOLVER_TYPES and self.solver_type != "sor":
+        if self.solver_type not in SOLVER_TYPES:
             raise capi.MemphysError(capi.MP_BAD_ARG,
                                     f"solver_type should be one of {sorted(SOLVER_TYPES)}; "
                                     f"current value: {self.solver_type}")
@@ -106,6 +108,17 @@ class PARAMETERS:
         kw = dict(tol=self.solver_tolerance, maxit=self.n_iter, **st)
         kw.update(overrides)
         return capi.solver_cfg(**kw)
+
+    def integrator_cfg(self, **overrides) -> capi.SolverCfg:
+        """The solver configuration of a time integrator's pressure solve.  The SOR
+        sweeps of the `sor` type run through SOLVER only (the integrators capture their
+        solves in CUDA graphs); an integrator given `sor` solves with BiCGSTAB + multigrid
+        to the same tolerance and says so."""
+        if self.solver_type == "sor" and "precond" not in overrides:
+            print("PARAMETERS: solver_type sor -> the time integrator's pressure solve runs "
+                  "BiCGSTAB + multigrid (SOR sweeps are available through SOLVER)")
+            overrides = dict(overrides, precond=capi.MP_PRECOND_AMG)
+        return self.solver_cfg(**overrides)
 
 
 class POINTS:
@@ -305,6 +318,13 @@ class SOLVER:
         rc = capi.lib().mp_ppe_solve(self.handle, ptr(b), ptr(x), C.byref(it), C.byref(rr),
                                      C.byref(ar), None)
         field_new[:] = x
+        if self.cfg.precond == capi.MP_PRECOND_SOR:
+            # solver.cpp:352-356: the SOR branch logs nothing into the parameters and
+            # returns after its sweeps whether or not they reached the tolerance
+            self.last_sor = (it.value, rr.value, rc)
+            if rc not in (capi.MP_OK, capi.MP_NOT_CONVERGED):
+                check(rc, "SOLVER::general_solve")
+            return it.value, rr.value
         if self.log_flag:
             parameters.rel_res_log.append(rr.value)
             parameters.abs_res_log.append(ar.value)
@@ -340,7 +360,7 @@ class FRACTIONAL_STEP_1:
                        p_dirichlet_flag)]
         self.cfg = capi.Fs1Cfg(parameters.rho, parameters.mu, parameters.dt or 0.0,
                                temporal_order)
-        self.scfg = parameters.solver_cfg(**cfg_overrides)
+        self.scfg = parameters.integrator_cfg(**cfg_overrides)
         h = C.c_void_p()
         check(capi.lib().mp_fs1_create(cloud.handle, ptr(points.boundary_flag), ptr(points.normal),
                                        ptr(self.flags[0]), ptr(self.flags[1]),
@@ -428,7 +448,7 @@ class SEMI_IMPLICIT_SPLIT_SOLVER:
         cfg = capi.SisCfg(parameters.rho, parameters.mu, parameters.dt, int(n_outer_iter),
                           float(iterative_tolerance), int(precond_freq_it))
         vel = parameters.solver_cfg(precond=capi.MP_PRECOND_JACOBI, precision=capi.MP_FP64)
-        pc = parameters.solver_cfg(**p_cfg)
+        pc = parameters.integrator_cfg(**p_cfg)
         flags = [np.ascontiguousarray(f, np.uint8) for f in
                  (u_dirichlet_flag, v_dirichlet_flag, p_dirichlet_flag)]
         h = C.c_void_p()
@@ -539,7 +559,7 @@ class FRACTIONAL_STEP_FOURIER:
                  temporal_order: int, use_graph: bool = True, **cfg):
         flags = [np.ascontiguousarray(f, np.uint8) for f in
                  (u_dirichlet_flag, v_dirichlet_flag, w_dirichlet_flag, p_dirichlet_flag)]
-        sc = parameters.solver_cfg(**cfg)
+        sc = parameters.integrator_cfg(**cfg)
         h = C.c_void_p()
         check(capi.lib().mp_fsf_create(cloud.handle, ptr(points.boundary_flag), ptr(points.normal),
                                        *[ptr(f) for f in flags], float(period), int(nw),
@@ -675,36 +695,45 @@ def cavity_setup(nx: int, solver_type="cuda_bicgstab_amg", dt=None, rho=1.0, mu=
     return cl, prm, pts, cld, fs
 
 
-def largest_eig_magnitude(op: "Operator", iters: int = 60, seed: int = 1) -> float:
-    """|lambda_max| of an operator by power iteration on the GPU (SpMV through the C ABI).
-    Stands in for the Arnoldi eigensolve of general_functions.cpp:4-24; the ratio
-    ||A^2 x|| / ||x|| is used so that a complex-conjugate dominant pair converges too."""
-    n = op.nrows
-    x = np.random.default_rng(seed).random(n) + 0.5
-    dx = capi.DeviceArray.from_host(x / np.linalg.norm(x))
-    dy = capi.DeviceArray((n,))
-    lam = 0.0
-    for _ in range(iters):
-        op.apply(dx, dy)
-        op.apply(dy, dx)
-        v = dx.to_host()
-        nv2 = np.linalg.norm(v)
-        if nv2 == 0 or not np.isfinite(nv2):
-            break
-        lam = np.sqrt(nv2)
-        dx.upload(v / nv2)
-    return float(lam)
+def calc_largest_magnitude_eigenvalue(op: "Operator", ncv: int = 30, tol: float = 1e-10,
+                                      max_restarts: int = 300, seed: int = 1) -> complex:
+    """calc_largest_magnitude_eigenvalue (general_functions.cpp:4-24): the eigenvalue of
+    largest magnitude of an operator, by restarted Arnoldi on the GPU (mp_op_largest_eig)
+    to a Ritz residual of tol * |lambda|; raises MemphysError(NOT_CONVERGED) otherwise, as
+    the reference throws when Spectra does not converge."""
+    re, im, nr = C.c_double(), C.c_double(), C.c_int()
+    check(capi.lib().mp_op_largest_eig(op.handle, ncv, tol, max_restarts, seed, C.byref(re),
+                                       C.byref(im), C.byref(nr), None),
+          "calc_largest_magnitude_eigenvalue")
+    return complex(re.value, im.value)
 
 
-def calc_dt(cloud: CLOUD, u0: float, v0: float, w0: float, alpha: float, courant: float) -> float:
+def largest_eig_magnitude(op: "Operator", **kw) -> float:
+    return abs(calc_largest_magnitude_eigenvalue(op, **kw))
+
+
+def calc_dt(cloud: CLOUD, u0: float, v0: float, w0: float, alpha: float, courant: float,
+            parameters: PARAMETERS | None = None) -> float:
     """PARAMETERS::calc_dt (parameters.cpp:269-296): dt = Courant * 2 /
-    (u0|l_x| + v0|l_y| [+ w0|l_z|] + alpha|l_L|) from the largest-magnitude eigenvalues."""
-    ev = u0 * largest_eig_magnitude(cloud.operator(capi.MP_GRAD_X))
-    ev += v0 * largest_eig_magnitude(cloud.operator(capi.MP_GRAD_Y))
+    (u0|l_x| + v0|l_y| [+ w0|l_z|] + alpha|l_L|) from the largest-magnitude eigenvalues.
+    With `parameters` the eigenvalues are stored there as the reference stores them
+    (grad_x_eigval_real/imag, ..., laplace_eigval_real/imag) and dt is set."""
+    names = [("grad_x", capi.MP_GRAD_X, u0), ("grad_y", capi.MP_GRAD_Y, v0)]
     if cloud.dim == 3:
-        ev += w0 * largest_eig_magnitude(cloud.operator(capi.MP_GRAD_Z))
-    ev += alpha * largest_eig_magnitude(cloud.operator(capi.MP_LAPLACIAN))
-    return courant * 2.0 / ev
+        names.append(("grad_z", capi.MP_GRAD_Z, w0))
+    names.append(("laplace", capi.MP_LAPLACIAN, alpha))
+    ev = 0.0
+    for name, which, coef in names:
+        lam = calc_largest_magnitude_eigenvalue(cloud.operator(which))
+        if parameters is not None:
+            setattr(parameters, f"{name}_eigval_real", lam.real)
+            setattr(parameters, f"{name}_eigval_imag", lam.imag)
+        ev += coef * abs(lam)
+    dt = courant * 2.0 / ev
+    if parameters is not None:
+        parameters.Courant = courant
+        parameters.dt = dt
+    return dt
 
 
 def stable_dt(h: float, nu: float, lid: float = 1.0, safety: float = 0.5) -> float:

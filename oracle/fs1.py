@@ -24,7 +24,10 @@ from . import ppe_assemble
 
 
 class FS1:
-    def __init__(self, cloud, nb_col, w, rho, mu, dt, temporal_order=2):
+    def __init__(self, cloud, nb_col, w, rho, mu, dt, temporal_order=2, factor=True):
+        """factor=False skips the direct factorisation: the instance then only forms
+        the right-hand sides and corrections around pressures supplied by the caller
+        (step_with_pressure), which is how the full-size configurations are checked."""
         nv, n = nb_col.shape
         self.nv, self.dim = nv, cloud.dim
         self.rho, self.mu, self.dt, self.order = rho, mu, dt, temporal_order
@@ -46,7 +49,7 @@ class FS1:
         rp, ci, val, ns = ppe_assemble(nb_col, w, cloud.boundary, cloud.p_dirichlet, cloud.normal)
         self.A = sp.csr_matrix((val, ci, rp), shape=(ns, ns))
         self.nsys = ns
-        self.lu = sla.splu(self.A.tocsc())
+        self.lu = sla.splu(self.A.tocsc()) if factor else None
         self.src_old = [np.zeros(nv) for _ in range(self.dim)]
         self.src_oldold = [np.zeros(nv) for _ in range(self.dim)]
 
@@ -65,7 +68,8 @@ class FS1:
                 hat.append(q + (self.dt / self.rho) * (1.5 * src - 0.5 * self.src_oldold[d]))
         return hat
 
-    def calc_pressure(self, vel, hat, p_old):
+    def pressure_rhs(self, vel, hat, p_old):
+        """fractional_step_1.cpp:136-149: the right-hand side of the pressure system."""
         nv = self.nv
         s = self.G_int[0] @ hat[0]
         for d in range(1, self.dim):
@@ -82,6 +86,10 @@ class FS1:
         src[:nv][nm] = (-self.rho * acc / self.dt)[nm]
         if self.nsys == nv + 1:
             src[nv] = 0.0
+        return src
+
+    def calc_pressure(self, vel, hat, p_old):
+        src = self.pressure_rhs(vel, hat, p_old)
         p = self.lu.solve(src)
         self.last_rhs = src
         self.last_relres = np.linalg.norm(self.A @ p - src) / np.linalg.norm(src)
@@ -102,6 +110,21 @@ class FS1:
                 q[i] = -(cf[~self_] * q[cols[~self_]]).sum() / cf[self_][0]
             new.append(q)
         return new
+
+    def step_with_pressure(self, vel, p, it, p_new):
+        """One step whose pressure solve is replaced by `p_new` (a solution from
+        elsewhere): returns ||A p_new - b|| / ||b|| with the oracle's own A and b
+        (recomputed in FP64), then advances (vel, p) in place with that pressure."""
+        hat = self.calc_vel_hat(vel, it)
+        b = self.pressure_rhs(vel, hat, p)
+        relres = np.linalg.norm(self.A @ p_new - b) / np.linalg.norm(b)
+        new = self.calc_vel_corr(vel, hat, p_new)
+        if self.order == 2:
+            self.src_oldold = [s.copy() for s in self.src_old]
+        for d in range(self.dim):
+            vel[d][:] = new[d]
+        p[:] = p_new
+        return relres
 
     def step(self, vel, p, it):
         """Advance (vel, p) by one step in place; returns the pressure relative residual."""

@@ -209,6 +209,38 @@ def test_fs1_oracles_agree():
     assert np.abs(pa - pb).max() <= 1e-7 * np.abs(pb).max()
 
 
+def test_c1_configured_dt_is_unstable():
+    """C1's configured dt = 1e-3 is above the explicit limit of the AB2 step on the
+    100 x 100 jittered cavity: the largest-magnitude eigenvalues (ARPACK) are
+    grad_x -388.9, grad_y 307.2 and laplacian -4.112e5, so calc_dt's rule
+    (parameters.cpp:269-296) gives dt = Courant * 4.16e-4, and mu * dt * |lambda_L| =
+    4.1 at dt = 1e-3 (AB2 needs < 1).  The oracle blows up within 10 steps there
+    (|u| ~ 5e7 at step 6) and stays bounded over 50 steps at the calc_dt step of
+    Courant 0.25 that the GPU tests and the benchmark use."""
+    cl = clouds.cavity_2d(100)
+    nb = oracle.knn_stencils(cl.xyz, cl.boundary, 20)
+    w = oracle.cloud_weights(cl.xyz, nb, 3, 3, cond=False)
+    nv = cl.nv
+    rows = np.repeat(np.arange(nv), 20)
+    lam = {}
+    for k in ("gx", "gy", "lap"):
+        A = sp.csr_matrix((w[k].ravel(), (rows, nb.ravel())), shape=(nv, nv))
+        lam[k] = abs(sla.eigs(A, k=1, which="LM", ncv=30, return_eigenvectors=False)[0])
+    assert lam["gx"] == pytest.approx(388.93, rel=1e-4)
+    assert lam["lap"] == pytest.approx(4.1122e5, rel=1e-4)
+    dt_calc = 0.25 * 2.0 / (lam["gx"] + lam["gy"] + 0.01 * lam["lap"])
+    assert 0.01 * 1e-3 * lam["lap"] > 4.0
+    for dt, nsteps, bounded in ((1e-3, 10, False), (dt_calc, 50, True)):
+        f = ofs1.FS1(cl, nb, w, 1.0, 0.01, dt, 2)
+        vel = [cl.vel_bc[0].copy(), cl.vel_bc[1].copy()]
+        p = np.zeros(f.nsys)
+        umax = 0.0
+        for it in range(nsteps):
+            f.step(vel, p, it)
+            umax = max(umax, float(np.nan_to_num(np.abs(vel[0]).max(), nan=np.inf)))
+        assert (umax <= 1.0 + 1e-9) == bounded, (dt, umax)
+
+
 def test_oracle_threads_do_not_change_results():
     # the row-parallel loops (SpMV rows, fractional-step row loops) compute every
     # row as the serial loop does; dot products and ILUT solves stay serial
@@ -248,3 +280,32 @@ def test_fourier_transforms_as_the_reference_writes_them():
         err[period] = np.abs(f.idft(f.dft(x)) - x).max()
     assert err[1.0] < 1e-14
     assert err[1.7] > 0.1
+
+
+def test_sor_orders_converge_to_the_same_solution():
+    """SOLVER::SOR (solver.cpp:243-281) in the reference's index order and in the
+    multicolour order of the GPU sweeps: the colouring is proper (no row reads a row of
+    its own colour), and on an implicit velocity-type system (rho/dt I - mu L inside,
+    identity on the Dirichlet boundary, solver.cpp:165-204) both orders converge to the
+    direct solution."""
+    cl = clouds.cavity_2d(12, seed=2)
+    nb = oracle.knn_stencils(cl.xyz, cl.boundary, 20)
+    w = oracle.cloud_weights(cl.xyz, nb, 3, 3, cond=False)
+    rp, ci, val, ns = oracle.ppe_assemble(nb, w, cl.boundary, cl.u_dirichlet, cl.normal,
+                                          unsteady=2000.0, conv=0.0, diff=-1.0, bordered=False)
+    assert ns == cl.nv
+    colour = oracle.sor_colouring(rp, ci, val, ns)
+    rows = np.repeat(np.arange(ns), np.diff(rp))
+    off = ci != rows
+    assert np.all(colour[rows[off]] != colour[ci[off]])
+    A = sp.csr_matrix((val, ci, rp), shape=(ns, ns))
+    b = np.random.default_rng(3).standard_normal(ns)
+    xd = sla.spsolve(A.tocsc(), b)
+    x_idx = oracle.sor_sweeps(rp, ci, val, b, np.zeros(ns), 1.4, 60)
+    x_mc = oracle.sor_sweeps(rp, ci, val, b, np.zeros(ns), 1.4, 60, colour)
+    for x in (x_idx, x_mc):
+        assert np.linalg.norm(A @ x - b) <= 1e-10 * np.linalg.norm(b)
+        assert np.abs(x - xd).max() <= 1e-10 * np.abs(xd).max()
+    assert not np.allclose(oracle.sor_sweeps(rp, ci, val, b, np.zeros(ns), 1.4, 2),
+                           oracle.sor_sweeps(rp, ci, val, b, np.zeros(ns), 1.4, 2, colour),
+                           rtol=1e-6)  # the iterates themselves differ
