@@ -442,7 +442,7 @@ static int upload_csr(const Csr &C, DCsr &D, cudaStream_t s) {
 // (Dirichlet rows, a shifted diagonal such as the Helmholtz systems of the
 // Fourier modes) is inverted as [A 0; 0 1], so that the coarse correction keeps
 // the constant component, which such operators do not annihilate.
-static int coarse_inverse(const Csr &A, std::vector<double> &inv) {
+static int coarse_inverse(const Csr &A, std::vector<double> &inv, bool *bordered) {
     const int n = A.n, m = n + 1;
     std::vector<double> M((size_t)m * m, 0.0);
     double max_sum = 0.0, max_abs = 0.0;
@@ -457,6 +457,7 @@ static int coarse_inverse(const Csr &A, std::vector<double> &inv) {
         max_abs = std::max(max_abs, ra);
     }
     const bool border = max_sum <= 1e-10 * max_abs;
+    *bordered = border;
     for (int i = 0; i < n; i++) {
         M[(size_t)i * m + n] = border ? 1.0 : 0.0;
         M[(size_t)n * m + i] = border ? 1.0 : 0.0;
@@ -754,7 +755,7 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
         // coarsest level: dense inverse (bordered when singular)
         hash_csr(A);
         std::vector<double> inv;
-        if ((rc = coarse_inverse(A, inv)) != MP_OK)
+        if ((rc = coarse_inverse(A, inv, &a->coarse_bordered)) != MP_OK)
             return bail(rc);
         a->nc = A.n;
         if ((rc = a->cinv.alloc(inv.size())) != MP_OK)
@@ -1008,20 +1009,21 @@ __global__ void k_cheb_start(int n, const T *b, const T *dinv, T *d, T inv_theta
         d[i] = dinv[i] * b[i] * inv_theta;
 }
 
-// coarsest level: x = first nc entries of Cinv [b; 0] (one warp per row)
+// coarsest level: x = first nc entries of Cinv [b; 0] (one warp per row); with
+// full = 1 all nc + 1 entries of Cinv [b; b_nc] (a one-level bordered hierarchy)
 template <class T>
 __global__ void k_coarse(int nc, const T *__restrict__ cinv, const T *__restrict__ b, T *x,
-                         const int *done) {
+                         const int *done, int full) {
     pdl_wait();
     pdl_trigger();
     if (*done)
         return;
     const int row = gwarp_a(), lane = threadIdx.x & 31;
-    if (row >= nc)
+    if (row >= nc + full)
         return;
     const T *ci = cinv + (size_t)row * (nc + 1);
     T acc = 0;
-    for (int j = lane; j < nc; j += 32)
+    for (int j = lane; j < nc + full; j += 32)
         acc = fma(ci[j], b[j], acc);
     acc = warp_sum(acc);
     if (lane == 0)
@@ -1116,8 +1118,9 @@ static int vcycle(const Amg &a, size_t l, const T *b, T *x, const int *done, cud
     using LO = LvlOps<V, DIFF>;
     AmgLevel &L = *a.L[l];
     if (l + 1 == a.L.size()) {
-        const cudaError_t e = launch_pdl(k_coarse<T>, dim3((unsigned)((a.nc + 7) / 8)), dim3(256), s,
-                                         a.nc, LV::cinv(a), b, x, done);
+        const int full = (l == 0 && a.coarse_bordered) ? 1 : 0;
+        const cudaError_t e = launch_pdl(k_coarse<T>, dim3((unsigned)((a.nc + full + 7) / 8)),
+                                         dim3(256), s, a.nc, LV::cinv(a), b, x, done, full);
         if (e != cudaSuccess)
             return fail(MP_CUDA_ERROR, "multigrid launch: %s", cudaGetErrorString(e));
         MP_CHECK_LAUNCH();

@@ -69,7 +69,10 @@ struct Amg {
     std::vector<AmgLevel *> L;
     int nc = 0;                       // coarsest size
     dbuf<double> cinv;                // (nc+1)^2 bordered inverse, row-major
+    // the coarsest operator annihilates constants and its inverse is bordered; with
+    // a single level that inverse is the bordered system's own, applied in full
     dbuf<float> cinv32;
+    bool coarse_bordered = false;
     double setup_seconds = 0;
     int store = AMG_F64;
     double cheb_ratio = 12.0;         // Chebyshev smoothing on [lmax / ratio, lmax]
@@ -94,7 +97,11 @@ int amg_filter(const Amg &a, const double *c, double *work1, const double *scale
 void amg_destroy(Amg *a);
 
 // out = V-cycle(in) on the first n0 entries (the border entry is handled by
-// the caller); kernels return immediately while *done is set.  FP64 vectors use
+// the caller); kernels return immediately while *done is set.  A one-level
+// hierarchy of an operator that annihilates constants is the exact inverse of the
+// bordered system: it then reads and writes entry n0 (the border) as well, since
+// the inverse on the first n0 entries alone maps every vector to zero mean and the
+// preconditioned system would lose its border row.  FP64 vectors use
 // the FP32 difference-form operators when the hierarchy was built with AMG_MG32.
 template <class T>
 int amg_apply(const Amg &a, const T *in, T *out, const int *done, cudaStream_t s);

@@ -712,7 +712,7 @@ extern "C" int mp_fs1_create(mp_cloud c, const uint8_t *boundary, const double *
                     cfg->temporal_order);
     if (!(cfg->dt > 0))
         return fail(MP_BAD_ARG, "dt must be positive");
-    MP_TRY(solver_cfg_check(*solver));
+    MP_TRY(integrator_cfg_check(*solver));
     mp_fs1 f = new mp_fs1_s;
     f->c = c;
     f->nv = nv;

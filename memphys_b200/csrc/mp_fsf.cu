@@ -286,7 +286,7 @@ extern "C" int mp_fsf_create(mp_cloud c, const uint8_t *boundary, const double *
         return fail(MP_BAD_ARG, "FRACTIONAL_STEP_FOURIER is defined for 2D clouds only");
     if (nw < 0 || !(period > 0) || !(dt > 0))
         return fail(MP_BAD_ARG, "nw >= 0, period > 0 and dt > 0 needed");
-    MP_TRY(solver_cfg_check(*solver));
+    MP_TRY(integrator_cfg_check(*solver));
     mp_fsf_s *f = new mp_fsf_s;
     auto bail = [&](int rc) {
         for (Ppe *p : f->P)

@@ -898,6 +898,8 @@ int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet
                 const double *normal, double unsteady, double conv, double diff,
                 const mp_solver_cfg &cfg_in, cudaStream_t st, int border_rule) {
     cfg = Cfg::from(cfg_in);
+    if (cfg.precond == MP_PRECOND_SOR)
+        border_rule = 0;  // solver.cpp:30-31: no regularisation for SOR
     CloudView cv = cloud_view(c);
     const int nv = cv.nv, K = cv.n, dim = cv.dim;
     // solver.cpp:29-38: bordered unless a boundary node is Dirichlet
@@ -956,6 +958,8 @@ int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet
         MP_TRY(amg_create(&sys.amg, sys.A, cfg,
                           mixed ? AMG_F32 : (cfg.precision == MP_MG32 ? AMG_MG32 : AMG_F64), st));
     }
+    if (cfg.precond == MP_PRECOND_SOR)
+        MP_TRY(sor_setup(*this, st));
     MP_TRY(W.alloc(nv, bordered, mixed, cfg.precond == MP_PRECOND_AMG));
     MP_CUDA(cudaStreamSynchronize(st));
     return MP_OK;
@@ -965,6 +969,8 @@ Ppe::~Ppe() {
     graph.reset();
     if (sys.amg)
         amg_destroy(sys.amg);
+    if (sor)
+        sor_destroy(sor);
     if (capture_stream)
         cudaStreamDestroy(capture_stream);
 }
@@ -974,14 +980,26 @@ int solver_cfg_check(const mp_solver_cfg &c) {
         return fail(MP_BAD_ARG, "solver tolerance and maxit must be positive");
     if (c.precision != MP_FP64 && c.precision != MP_FP32 && c.precision != MP_MG32)
         return fail(MP_BAD_ARG, "precision must be MP_FP64, MP_FP32 or MP_MG32");
-    if (c.precond < MP_PRECOND_NONE || c.precond > MP_PRECOND_AMG)
+    if (c.precond < MP_PRECOND_NONE || c.precond > MP_PRECOND_SOR)
         return fail(MP_BAD_ARG, "unknown preconditioner %d", c.precond);
+    if (c.precond == MP_PRECOND_SOR && c.precision != MP_FP64)
+        return fail(MP_BAD_ARG, "the sor solver type runs in FP64 only");
+    if (c.precond == MP_PRECOND_SOR && !(c.sor_omega > 0.0 && c.sor_omega < 2.0))
+        return fail(MP_BAD_ARG, "sor_omega must lie in (0, 2), got %g", c.sor_omega);
     if (c.guess_vectors < 0 || c.guess_vectors > 8)
         return fail(MP_BAD_ARG, "guess_vectors must be 1-8 (0 for the default 8), got %d",
                     c.guess_vectors);
     if (c.precision == MP_MG32 && c.precond != MP_PRECOND_AMG)
         return fail(MP_BAD_ARG, "MP_MG32 stores the multigrid preconditioner in FP32: it needs "
                                 "MP_PRECOND_AMG");
+    return MP_OK;
+}
+
+int integrator_cfg_check(const mp_solver_cfg &c) {
+    MP_TRY(solver_cfg_check(c));
+    if (c.precond == MP_PRECOND_SOR)
+        return fail(MP_BAD_ARG, "the sor solver type is available through SOLVER (mp_ppe_*); the "
+                                "time integrators need a Krylov solver type");
     return MP_OK;
 }
 
@@ -999,6 +1017,7 @@ Cfg Cfg::from(const mp_solver_cfg &c) {
     o.smoother_sweeps = c.smoother_sweeps > 0 ? c.smoother_sweeps : 1;
     o.cheb_lower = c.cheb_lower > 0 && c.cheb_lower < 1 ? c.cheb_lower : 1.0 / 12.0;
     o.guess_vectors = c.guess_vectors > 0 ? c.guess_vectors : 8;
+    o.sor_omega = c.sor_omega > 0 && c.sor_omega < 2 ? c.sor_omega : 1.4;
     return o;
 }
 
@@ -1020,6 +1039,7 @@ extern "C" int mp_solver_cfg_default(mp_solver_cfg *c) {
     c->smoother_sweeps = 1;
     c->cheb_lower = 1.0 / 12.0;
     c->guess_vectors = 8;
+    c->sor_omega = 1.4;
     return MP_OK;
 }
 
@@ -1053,10 +1073,16 @@ extern "C" int mp_ppe_solve(mp_ppe p, const double *rhs, double *x_inout, int *i
         MP_CUDA(cudaMemsetAsync(P.W.x.p, 0, sizeof(double) * n, st));
     else
         MP_CUDA(cudaMemcpyAsync(P.W.x.p, x_inout, sizeof(double) * n, cudaMemcpyDefault, st));
-    MP_TRY(P.solve_resident(st, p->use_graph));
-    MP_CUDA(cudaMemcpyAsync(x_inout, P.W.x.p, sizeof(double) * n, cudaMemcpyDefault, st));
     SolveStats ss;
-    MP_TRY(P.read_stats(st, &ss));
+    if (P.sor) {
+        MP_TRY(sor_solve(P, st, &ss));
+    } else {
+        MP_TRY(P.solve_resident(st, p->use_graph));
+    }
+    MP_CUDA(cudaMemcpyAsync(x_inout, P.W.x.p, sizeof(double) * n, cudaMemcpyDefault, st));
+    if (!P.sor)
+        MP_TRY(P.read_stats(st, &ss));
+    MP_CUDA(cudaStreamSynchronize(st));
     if (iters)
         *iters = ss.iters;
     if (relres)
@@ -1065,8 +1091,9 @@ extern "C" int mp_ppe_solve(mp_ppe p, const double *rhs, double *x_inout, int *i
         *abs_res = ss.abs_res;
     if (ss.status == MP_NOT_CONVERGED)
         return fail(MP_NOT_CONVERGED,
-                    "pressure solve did not converge in %d iterations, relative residual: %g",
-                    ss.iters, ss.relres);
+                    "%s did not converge in %d %s, relative residual: %g",
+                    P.sor ? "SOR" : "pressure solve", ss.iters, P.sor ? "sweeps" : "iterations",
+                    ss.relres);
     if (ss.status != MP_OK)
         return fail(ss.status, "pressure solve failed (status %d), relative residual: %g",
                     ss.status, ss.relres);

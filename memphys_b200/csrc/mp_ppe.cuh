@@ -8,18 +8,23 @@ struct mp_cloud_s;
 namespace mp {
 
 struct Cfg {
-    double tol, inner_tol, cheb_lower;
+    double tol, inner_tol, cheb_lower, sor_omega;
     int maxit, precond, precision, guess, max_refine, amg_max_levels, amg_coarse_size,
         smoother_sweeps, guess_vectors;
     static Cfg from(const mp_solver_cfg &c);
 };
 // MP_OK, or MP_BAD_ARG with the reason for an inconsistent solver configuration
 int solver_cfg_check(const mp_solver_cfg &c);
+// the same for the solvers inside a time integrator, which run as CUDA graphs:
+// the SOR sweeps (MP_PRECOND_SOR, SOLVER only) are refused there
+int integrator_cfg_check(const mp_solver_cfg &c);
 
 struct SolveStats {
     int iters = 0, outer = 0, status = MP_OK;
     double relres = 0, abs_res = 0;
 };
+
+struct Sor;  // multicolour SOR sweeps (mp_sor.cu)
 
 // Device vectors of one solve (FP64, and FP32 for mixed precision)
 struct Krylov {
@@ -39,6 +44,7 @@ struct Ppe {
     GraphExec graph;
     std::shared_ptr<Ell> shared_cols;
     cudaStream_t capture_stream = nullptr;
+    Sor *sor = nullptr;  // MP_PRECOND_SOR: the row colouring
     ~Ppe();
     // border_rule 1: bordered unless a boundary node is Dirichlet (solver.cpp:29-38);
     // 0: never bordered (systems with a nonsingular diagonal, e.g. implicit velocity)
@@ -73,6 +79,12 @@ struct Ppe {
     int read_stats(cudaStream_t st, SolveStats *out);
     cudaStream_t cap_stream();
 };
+
+// MP_PRECOND_SOR (mp_sor.cu): colour the rows once; sweep with W.x as the initial
+// guess and W.b64 as the right-hand side
+int sor_setup(Ppe &P, cudaStream_t st);
+int sor_solve(Ppe &P, cudaStream_t st, SolveStats *out);
+void sor_destroy(Sor *s);
 
 }  // namespace mp
 

@@ -288,8 +288,8 @@ extern "C" int mp_sis_create(mp_cloud c, const uint8_t *boundary, const double *
     if (vel_solver->precond == MP_PRECOND_AMG || vel_solver->precision != MP_FP64)
         return fail(MP_BAD_ARG, "the velocity matrices change every outer iteration: their solver "
                                 "takes MP_PRECOND_JACOBI or MP_PRECOND_NONE in MP_FP64");
-    MP_TRY(solver_cfg_check(*vel_solver));
-    MP_TRY(solver_cfg_check(*p_solver));
+    MP_TRY(integrator_cfg_check(*vel_solver));
+    MP_TRY(integrator_cfg_check(*p_solver));
     std::vector<uint8_t> hb(nv), hu(nv), hv(nv);
     MP_CUDA(cudaMemcpy(hb.data(), boundary, nv, cudaMemcpyDefault));
     MP_CUDA(cudaMemcpy(hu.data(), u_dir, nv, cudaMemcpyDefault));
@@ -493,7 +493,7 @@ extern "C" int mp_ist_create(mp_cloud c, const uint8_t *boundary, const double *
     if (solver->precond == MP_PRECOND_AMG || solver->precision != MP_FP64)
         return fail(MP_BAD_ARG, "the transport matrix changes every step: its solver takes "
                                 "MP_PRECOND_JACOBI or MP_PRECOND_NONE in MP_FP64");
-    MP_TRY(solver_cfg_check(*solver));
+    MP_TRY(integrator_cfg_check(*solver));
     std::vector<uint8_t> hb(nv), hd(nv);
     MP_CUDA(cudaMemcpy(hb.data(), boundary, nv, cudaMemcpyDefault));
     MP_CUDA(cudaMemcpy(hd.data(), dirichlet, nv, cudaMemcpyDefault));

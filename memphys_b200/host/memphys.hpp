@@ -49,10 +49,32 @@ struct PARAMETERS {
         mp_solver_cfg_default(&c);
         c.tol = solver_tolerance;
         c.maxit = n_iter;
+        // solver_type strings as PARAMETERS::verify_parameters accepts them
+        // (parameters.cpp:94-99), plus the GPU configurations by name
         if (solver_type == "cuda_bicgstab_amg_mixed")
             c.precision = MP_FP32;
+        else if (solver_type == "cuda_bicgstab_amg_mg32")
+            c.precision = MP_MG32;
         else if (solver_type == "cuda_bicgstab_jacobi")
             c.precond = MP_PRECOND_JACOBI;
+        else if (solver_type == "cuda_bicgstab_jacobi_mixed") {
+            c.precond = MP_PRECOND_JACOBI;
+            c.precision = MP_FP32;
+        } else if (solver_type == "cuda_bicgstab")
+            c.precond = MP_PRECOND_NONE;
+        else if (solver_type == "sor")
+            c.precond = MP_PRECOND_SOR;
+        return c;
+    }
+    // a time integrator's solver: the SOR sweeps run through SOLVER only, so `sor`
+    // gives the integrators BiCGSTAB + multigrid to the same tolerance
+    mp_solver_cfg integrator_cfg() const {
+        mp_solver_cfg c = solver_cfg();
+        if (c.precond == MP_PRECOND_SOR) {
+            std::printf("PARAMETERS: solver_type sor -> the time integrator's pressure solve runs "
+                        "BiCGSTAB + multigrid (SOR sweeps are available through SOLVER)\n");
+            c.precond = MP_PRECOND_AMG;
+        }
         return c;
     }
 };
@@ -184,7 +206,7 @@ class FRACTIONAL_STEP_1 {
         v_d.assign(v_dirichlet_flag1.begin(), v_dirichlet_flag1.end());
         p_d.assign(p_dirichlet_flag1.begin(), p_dirichlet_flag1.end());
         mp_fs1_cfg cfg{parameters.rho, parameters.mu, parameters.dt, temporal_order1};
-        mp_solver_cfg scfg = parameters.solver_cfg();
+        mp_solver_cfg scfg = parameters.integrator_cfg();
         check(mp_fs1_create(cloud.handle, points.boundary_flag.data(), points.normal.data(),
                             u_d.data(), v_d.data(), nullptr, p_d.data(), &cfg, &scfg, &handle),
               "FRACTIONAL_STEP_1::FRACTIONAL_STEP_1");
@@ -236,7 +258,7 @@ class IMPLICIT_SCALAR_TRANSPORT_SOLVER {
                                      bool solver_log_flag1)
         : solver_log_flag(solver_log_flag1) {
         d.assign(dirichlet_flag1.begin(), dirichlet_flag1.end());
-        mp_solver_cfg c = parameters.solver_cfg();
+        mp_solver_cfg c = parameters.integrator_cfg();
         c.precond = MP_PRECOND_JACOBI;  // the matrix changes every step
         c.precision = MP_FP64;
         check(mp_ist_create(cloud.handle, points.boundary_flag.data(), points.normal.data(), d.data(),
@@ -281,7 +303,7 @@ class SEMI_IMPLICIT_SPLIT_SOLVER {
         p_d.assign(p_dirichlet_flag1.begin(), p_dirichlet_flag1.end());
         mp_sis_cfg cfg{parameters.rho, parameters.mu, parameters.dt, n_outer_iter1,
                        iterative_tolerance1, precond_freq_it1};
-        mp_solver_cfg vel = parameters.solver_cfg(), pres = parameters.solver_cfg();
+        mp_solver_cfg vel = parameters.integrator_cfg(), pres = parameters.integrator_cfg();
         vel.precond = MP_PRECOND_JACOBI;  // the velocity matrices change every outer iteration
         vel.precision = MP_FP64;
         check(mp_sis_create(cloud.handle, points.boundary_flag.data(), points.normal.data(),
@@ -339,7 +361,7 @@ class FRACTIONAL_STEP_FOURIER {
         v_d.assign(v_dirichlet_flag1.begin(), v_dirichlet_flag1.end());
         w_d.assign(w_dirichlet_flag1.begin(), w_dirichlet_flag1.end());
         p_d.assign(p_dirichlet_flag1.begin(), p_dirichlet_flag1.end());
-        mp_solver_cfg c = parameters.solver_cfg();
+        mp_solver_cfg c = parameters.integrator_cfg();
         check(mp_fsf_create(cloud.handle, points.boundary_flag.data(), points.normal.data(),
                             u_d.data(), v_d.data(), w_d.data(), p_d.data(), period1, nw1,
                             temporal_order1, parameters.rho, parameters.mu, parameters.dt, &c,

@@ -17,6 +17,7 @@ import os
 import subprocess
 
 import numpy as np
+import scipy.sparse as sp
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libmemphys_oracle.so")
@@ -286,6 +287,55 @@ def ppe_assemble(nb_col, w, boundary, dirichlet, normal, unsteady=0.0, conv=0.0,
                                diff, int(bordered), rp, ci, val)
     rp = rp[: ns + 1].copy()
     return rp, ci[: rp[-1]].copy(), val[: rp[-1]].copy(), ns
+
+
+def sor_colouring(rp, ci, val, nv):
+    """The row colouring of the GPU's multicolour SOR, restated: rows in index order,
+    each taking the smallest colour held neither by a member of its own row nor by a
+    row that contains it (the graph of the nonzero coefficients made symmetric).
+    Returns the colour of every row."""
+    rp = np.asarray(rp)
+    ci = np.asarray(ci)
+    rows = np.repeat(np.arange(nv), np.diff(rp[: nv + 1]))
+    cols = ci[: rp[nv]]
+    keep = (cols != rows) & (cols < nv) & (np.asarray(val)[: rp[nv]] != 0.0)
+    fwd = [[] for _ in range(nv)]
+    for i, j in zip(rows[keep].tolist(), cols[keep].tolist()):
+        fwd[i].append(j)
+        fwd[j].append(i)
+    colour = [-1] * nv
+    for i in range(nv):
+        used = {colour[j] for j in fwd[i] if colour[j] >= 0}
+        c = 0
+        while c in used:
+            c += 1
+        colour[i] = c
+    return np.asarray(colour)
+
+
+def sor_sweeps(rp, ci, val, b, x, omega=1.4, sweeps=1, colour=None):
+    """SOLVER::SOR's update (solver.cpp:243-281): x_i = omega (b_i - sum_{j != i} a_ij
+    x_j) / a_ii + (1 - omega) x_i, rows in index order (colour None, the reference's
+    order, pure Python: small systems) or colour by colour (the GPU's order; rows of
+    one colour never read one another, so each colour is one vector update)."""
+    A = sp.csr_matrix((np.asarray(val), np.asarray(ci), np.asarray(rp)))
+    n = A.shape[0]
+    d = A.diagonal()
+    x = np.array(x, np.float64, copy=True)
+    if colour is None:
+        for _ in range(sweeps):
+            for i in range(n):
+                lo, hi = A.indptr[i], A.indptr[i + 1]
+                s = b[i] - A.data[lo:hi] @ x[A.indices[lo:hi]] + d[i] * x[i]
+                x[i] = omega * s / d[i] + (1.0 - omega) * x[i]
+        return x
+    groups = [np.nonzero(colour == c)[0] for c in range(int(colour.max()) + 1)]
+    blocks = [A[g] for g in groups]
+    for _ in range(sweeps):
+        for g, Ag in zip(groups, blocks):
+            s = b[g] - Ag @ x + d[g] * x[g]
+            x[g] = omega * s / d[g] + (1.0 - omega) * x[g]
+    return x
 
 
 class ILUT:
