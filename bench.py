@@ -417,10 +417,10 @@ def run_ours(args, ws, rank, local, pg):
         "clocks": clocks,
         "learned_mixed": variants.get("learned_mg32"),
         "variants": variants,
-        "learned_training": {"spinup_steps": args.spinup, "sample_nodes": min(args.samples, nv),
-                             "samples": min(args.samples, nv) * max(args.spinup - 2, 0),
-                             "epochs": args.epochs, "final_loss": train_loss,
-                             "train_s": round(t_train, 2)},
+        "learned_training": training_summary(min(args.samples, nv) * max(args.spinup - 2, 0),
+                                             args.epochs, train_loss, t_train,
+                                             spinup_steps=args.spinup,
+                                             sample_nodes=min(args.samples, nv)),
         "setup_s": {"cloud": round(t_cloud, 2), "fs1_and_multigrid": round(t_setup, 2)},
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -430,7 +430,7 @@ def run_ours(args, ws, rank, local, pg):
     # (a sticky error) stops the rest and is reported as context_error
     legs = []
     if args.batched > 0:
-        legs.append(("batched_stencils", lambda: batched_stencils(args.batched)))
+        legs.append(("batched_stencils", lambda: batched_stencils(args.batched, stream)))
     if ws == 1 and not args.no_cube:
         legs.append(("cube3d_mixed", lambda: cube_mixed(args, stream)))
     if ws == 1 and not args.no_channel:
@@ -444,6 +444,21 @@ def run_ours(args, ws, rank, local, pg):
                 out["context_error"] = f"{name}: {capi.last_error()}"[:400]
                 break
     return out
+
+
+def training_summary(samples, epochs, loss, secs, **extra):
+    """Training throughput of the network: forward + backward ~ 3 x 82,176 flop per
+    sample and epoch (the 41,088 multiply-adds of the forward, twice that backward),
+    against the measured sustained BF16 tensor peak (training runs for seconds)."""
+    flops = 3.0 * 82176.0 * samples * epochs
+    tf = flops / secs / 1e12 if secs > 0 else None
+    try:
+        peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops_sustained"])
+    except Exception:
+        peak = 1400.0
+    return {**extra, "samples": samples, "epochs": epochs, "final_loss": loss,
+            "train_s": round(secs, 2), "train_tflops": round(tf, 2) if tf else None,
+            "train_frac_of_bf16_sustained": round(tf / peak, 5) if tf else None}
 
 
 def steps_timed(f, stream, first, warmup, steps):
@@ -562,30 +577,39 @@ def channel_learned(args, stream):
     return {"workload": f"channel_2d h={args.channel_h} with cylinder, {cl.nv} nodes, Re 200, "
                         "BiCGSTAB + SA multigrid to 1e-8",
             "nodes": cl.nv, "dt": prm.dt,
-            "training": {"plain_steps": T, "sample_nodes": ns_, "samples": ns_ * (T - 2),
-                         "epochs": args.epochs, "final_loss": loss,
-                         "spinup_s": round(t_spin, 2), "train_s": round(t_train, 2),
-                         "plain_iters_last_steps": float(plain[:, 0].mean())},
+            "training": training_summary(ns_ * (T - 2), args.epochs, loss, t_train,
+                                         plain_steps=T, sample_nodes=ns_,
+                                         spinup_s=round(t_spin, 2),
+                                         plain_iters_last_steps=float(plain[:, 0].mean())),
             "second_difference_over_increment": rms(d2) / rms(inc),
             "increment_over_pressure": rms(inc) / rms(p[:cl.nv]),
             "guesses": res}
 
 
-def batched_stencils(nsys: int):
+FP64_PEAK_TFLOPS = 37.0  # B200 datasheet FP64 (non-tensor) per GPU; no measured FP64 peak
+
+
+def batched_stencils(nsys: int, stream):
     """The batched uneven stencil workload: nsys independent augmented PHS r^3 +
-    degree-3 systems per dimension, n from {20, 30, 40} for interior stencils and 60
-    for the 10 % marked boundary, offsets uniform in the unit ball scaled by h in
-    [1e-3, 1e-2]; one mp_stencil_weights_batched call on device arrays, timed by
-    wall clock around the (synchronous) call, best of two.  (The weights of this workload are
-    checked against per-stencil LAPACK in tests/test_gpu_parity.py.)
-    FLOPs count the useful FMAs of Gauss-Jordan on the s x (s + dim + 1) system."""
+    degree-3 systems per dimension; 90 % interior stencils with n drawn from {20, 30},
+    10 % boundary stencils with n from {40, 60}; offsets uniform in the unit ball
+    scaled by h in [1e-3, 1e-2], node 0 the centre.  A plan classifies the systems
+    once (host); each run is the persistent size-class kernels on the stream, timed
+    with CUDA events over `reps` runs after one untimed run (which also tunes the CTA
+    shapes).  FLOPs on the algorithmic basis (2/3) s^3 + 2 (dim + 1) s^2 per system,
+    s = n + m (LU and the triangular solves; the kernel's Gauss-Jordan does more).
+    The weights of this workload are checked against per-stencil LAPACK in the GPU
+    tests (tests/test_gpu_parity.py), not here."""
+    import ctypes as C
     from memphys_b200 import capi
     L = capi.lib()
     res = {}
+    reps = 3
     for dim, m in ((2, 10), (3, 20)):
         rng = np.random.default_rng(20261203 + dim)
         bnd = rng.random(nsys) < 0.1
-        sizes = np.where(bnd, 60, rng.choice([20, 30, 40], size=nsys)).astype(np.int32)
+        sizes = np.where(bnd, rng.choice([40, 60], size=nsys),
+                         rng.choice([20, 30], size=nsys)).astype(np.int32)
         off = np.zeros(nsys, np.int64)
         off[1:] = np.cumsum(sizes[:-1], dtype=np.int64)
         total = int(sizes.sum(dtype=np.int64))
@@ -599,23 +623,37 @@ def batched_stencils(nsys: int):
         d_pts = capi.DeviceArray.from_host(np.ascontiguousarray(pts))
         d_w = capi.DeviceArray(((dim + 1) * total,))
         del pts
-
-        def call():
-            capi.check(L.mp_stencil_weights_batched(nsys, capi.ptr(d_sizes), capi.ptr(d_off),
-                                                    capi.ptr(d_pts), dim, 3, 3, capi.ptr(d_w),
-                                                    None, None), "mp_stencil_weights_batched")
-        call()  # warm-up (first-use set-up of the kernels)
-        secs = 1e30
-        for _ in range(2):  # the call includes host-side work: best of two
-            t0 = time.time()
-            call()
-            secs = min(secs, time.time() - t0)
+        plan = C.c_void_p()
+        t0 = time.time()
+        capi.check(L.mp_stencil_plan_create(nsys, capi.ptr(d_sizes), capi.ptr(d_off), dim, 3,
+                                            C.byref(plan)), "mp_stencil_plan_create")
+        t_plan = time.time() - t0
+        try:
+            def run():
+                capi.check(L.mp_stencil_plan_run(plan, capi.ptr(d_pts), 3, capi.ptr(d_w), None,
+                                                 stream.handle), "mp_stencil_plan_run")
+            run()  # untimed: tunes the CTA shapes of each class on its first run
+            bad = C.c_int()
+            capi.check(L.mp_stencil_plan_singular(plan, C.byref(bad), stream.handle))
+            with capi.Timer(stream.handle) as tm:
+                for _ in range(reps):
+                    run()
+            secs = tm.ms / reps / 1e3
+            counts = (C.c_int * 7)()
+            shapes = (C.c_int * 7)()
+            capi.check(L.mp_stencil_plan_info(plan, counts, shapes))
+        finally:
+            L.mp_stencil_plan_destroy(plan)
         s_ = sizes.astype(np.float64) + m
-        fmas = float(np.sum(s_ * (s_ + dim + 1) * (s_ - 1)))
-        res[f"{dim}d"] = {"systems": nsys, "monomials": m, "seconds": round(secs, 4),
-                          "systems_per_s": round(nsys / secs),
-                          "gflops_fp64": round(2 * fmas / secs / 1e9, 1)}
+        flops = float(np.sum(2.0 / 3.0 * s_ ** 3 + 2.0 * (dim + 1) * s_ ** 2))
+        tf = flops / secs / 1e12
+        res[f"{dim}d"] = {"systems": nsys, "monomials": m, "seconds": round(secs, 5),
+                          "systems_per_s": round(nsys / secs), "tflops_fp64_algorithmic": round(tf, 3),
+                          "frac_of_fp64_datasheet": round(tf / FP64_PEAK_TFLOPS, 4),
+                          "singular": bad.value, "plan_s": round(t_plan, 2),
+                          "class_systems": list(counts), "class_systems_per_cta": list(shapes)}
         del d_w, d_pts
+    res["fp64_peak_tflops"] = f"{FP64_PEAK_TFLOPS} (B200 datasheet, FP64 non-tensor; not measured)"
     return res
 
 

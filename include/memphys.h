@@ -162,6 +162,28 @@ int mp_stencil_weights_batched(int nsys, const int *sizes, const int64_t *offset
                                const double *pts, int dim, int phs_deg, int poly_deg, double *w,
                                double *cond, mp_stream s);
 
+/*
+ * The same batch in two parts (no counterpart in the reference, which solves one
+ * stencil at a time): a plan classifies the systems by size once (host work: the
+ * sizes and offsets are read back), and each run launches the persistent kernels of
+ * the size classes on the caller's stream, asynchronously, device arrays only.  The
+ * first run of a plan whose class has at least 8 systems per SM also times the
+ * class's CTA shapes on a sample of its systems and keeps the fastest (cached per
+ * class and dimension in the process).  mp_stencil_plan_singular synchronises s and
+ * returns the number of systems of the last run with a zero pivot;
+ * mp_stencil_plan_info fills, for the 7 size classes (n + m + dim + 1 up to 36, 44,
+ * 56, 68, 76, 84, 100 with n + m up to 32, 64, 64, 64, 96, 96, 96), the systems of
+ * each class and the systems per CTA it runs with (arrays of 7, nullable).
+ */
+typedef struct mp_stencil_plan_s *mp_stencil_plan;
+int mp_stencil_plan_create(int nsys, const int *sizes, const int64_t *offsets, int dim,
+                           int poly_deg, mp_stencil_plan *out);
+int mp_stencil_plan_run(mp_stencil_plan p, const double *pts, int phs_deg, double *w,
+                        double *cond, mp_stream s);
+int mp_stencil_plan_singular(mp_stencil_plan p, int *count, mp_stream s);
+int mp_stencil_plan_info(mp_stencil_plan p, int *class_count, int *class_shape);
+int mp_stencil_plan_destroy(mp_stencil_plan p);
+
 /* ------------------------------------------------------------------ cloud */
 typedef struct mp_cloud_s *mp_cloud;
 
@@ -430,6 +452,11 @@ int mp_mlp_gradient(mp_mlp m, const float *X, const float *t, int n, double *los
 /* Adam, `epochs` passes over n rows in shuffled batches (batch a multiple of 128) */
 int mp_mlp_train(mp_mlp m, const float *X, const float *t, int n, int epochs, int batch,
                  double lr, uint64_t seed, double *loss);
+/* the polls of every tensor-core completion wait before the kernel gives up with
+ * MP_TIMEOUT (default 4194304; 0 gives up at once, a test of that path: the
+ * kernel still waits, bounded, for the MMA it already committed before it releases
+ * tensor memory, and the handle stays usable) */
+int mp_mlp_set_spin_limit(mp_mlp m, long long polls);
 int mp_mlp_destroy(mp_mlp m);
 
 /*

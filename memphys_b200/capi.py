@@ -40,14 +40,15 @@ EXPORTS = [
     "mp_ist_destroy", "mp_fsf_create", "mp_fsf_set_graph", "mp_fsf_single_timestep",
     "mp_fsf_destroy",
     "mp_stencil_weights",
-    "mp_stencil_weights_batched", "mp_cloud_create", "mp_cloud_create_stencils", "mp_cloud_info",
+    "mp_stencil_weights_batched", "mp_stencil_plan_create", "mp_stencil_plan_run",
+    "mp_stencil_plan_singular", "mp_stencil_plan_info", "mp_stencil_plan_destroy", "mp_cloud_create", "mp_cloud_create_stencils", "mp_cloud_info",
     "mp_cloud_get", "mp_cloud_destroy", "mp_op_create_ell", "mp_op_from_cloud", "mp_op_apply",
     "mp_op_apply_multi", "mp_op_info", "mp_op_largest_eig", "mp_op_destroy", "mp_solver_cfg_default", "mp_ppe_create",
     "mp_ppe_system_size", "mp_ppe_solve", "mp_ppe_destroy", "mp_fs1_create",
     "mp_fs1_system_size", "mp_fs1_set_state", "mp_fs1_get_state", "mp_fs1_step",
     "mp_fs1_single_timestep", "mp_fs1_last_stats", "mp_fs1_log", "mp_fs1_kernel_counts",
     "mp_fs1_destroy", "mp_mlp_create", "mp_mlp_num_params", "mp_mlp_get_params",
-    "mp_mlp_set_params", "mp_mlp_forward", "mp_mlp_gradient", "mp_mlp_train", "mp_mlp_destroy",
+    "mp_mlp_set_params", "mp_mlp_forward", "mp_mlp_gradient", "mp_mlp_train", "mp_mlp_set_spin_limit", "mp_mlp_destroy",
     "mp_fs1_attach_mlp", "mp_fs1_train_mlp", "mp_fs1_set_guess", "mp_fs1_samples",
 ]
 
@@ -120,6 +121,10 @@ def lib() -> C.CDLL:
             "mp_fsf_single_timestep": [vp, vp, vp, vp, vp, i, vp], "mp_fsf_destroy": [vp],
             "mp_stencil_weights": [vp, i, i, vp, i, i, i, vp, vp, vp, vp, vp, vp],
             "mp_stencil_weights_batched": [i, vp, vp, vp, i, i, i, vp, vp, vp],
+            "mp_stencil_plan_create": [i, vp, vp, i, i, C.POINTER(vp)],
+            "mp_stencil_plan_run": [vp, vp, i, vp, vp, vp],
+            "mp_stencil_plan_singular": [vp, C.POINTER(i), vp],
+            "mp_stencil_plan_info": [vp, vp, vp], "mp_stencil_plan_destroy": [vp],
             "mp_cloud_create": [vp, vp, i, i, i, i, d, i, vp, C.POINTER(vp)],
             "mp_cloud_create_stencils": [vp, vp, i, i, vp, i, i, i, i, vp, C.POINTER(vp)],
             "mp_cloud_info": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)],
@@ -149,7 +154,7 @@ def lib() -> C.CDLL:
             "mp_mlp_forward": [vp, vp, i, vp],
             "mp_mlp_gradient": [vp, vp, vp, i, C.POINTER(d), vp],
             "mp_mlp_train": [vp, vp, vp, i, i, i, d, C.c_uint64, C.POINTER(d)],
-            "mp_mlp_destroy": [vp],
+            "mp_mlp_set_spin_limit": [vp, C.c_longlong], "mp_mlp_destroy": [vp],
             "mp_fs1_attach_mlp": [vp, vp, i, i, i],
             "mp_fs1_train_mlp": [vp, i, i, d, C.c_uint64, C.POINTER(d)],
             "mp_fs1_set_guess": [vp, i],

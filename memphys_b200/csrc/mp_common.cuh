@@ -77,6 +77,8 @@ int sm_count();
 
 // true when p is device (or managed) memory
 bool is_device_ptr(const void *p);
+// true when p is memory of the current device (or managed memory)
+bool is_current_device_ptr(const void *p);
 
 // RAII device buffer (owned by handles)
 template <class T> struct dbuf {

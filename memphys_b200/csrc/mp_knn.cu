@@ -360,6 +360,11 @@ extern "C" int mp_knn_stencils_noalloc(const double *xyz, const uint8_t *boundar
     if (!is_device_ptr(xyz) || !is_device_ptr(boundary) || !is_device_ptr(nb_col))
         return fail(MP_BAD_ARG, "mp_knn_stencils_noalloc takes device pointers only (staging host "
                                 "arrays would allocate); use mp_knn_stencils for host arrays");
+    // the scratch and the launches belong to the current device
+    if (!is_current_device_ptr(xyz) || !is_current_device_ptr(boundary) ||
+        !is_current_device_ptr(nb_col))
+        return fail(MP_BAD_ARG, "mp_knn_stencils_noalloc: the arrays must live on the current "
+                                "device (mp_set_device)");
     // the four per-node arrays alone must fit before anything runs
     if ((size_t)nv * 16 + 4096 > KNN_SCRATCH_BYTES)
         return fail(MP_BAD_ARG, "mp_knn_stencils_noalloc: %d nodes exceed its %zu-byte scratch "

@@ -12,9 +12,20 @@
 // BF16 activations back to shared memory as the next layer's A operand.  The
 // output layer is a per-thread dot product on the FP32 activations.
 //
-// Backward (training): CUDA-core kernels on the stored activations (weight
-// gradients reduce over the batch), Adam on FP32 master weights, then the
-// BF16 operand copies are repacked.
+// Backward (training) on the tensor cores as well: the input gradients
+// D_prev = (D W^T) * relu'(H_prev) per 128-row tile, and the weight gradients
+// dW = A^T D as a product over the batch split into 64-row chunks across CTAs
+// (each CTA accumulates its chunks in tensor memory; a second kernel sums the CTAs'
+// partial products in a fixed order).  The FP32 gradients D enter the BF16 MMA as
+// two parts, D = hi + lo with hi = bf16(D) and lo = bf16(D - hi) (16 significant
+// bits), against operands that are exactly BF16 (the weights and activations the
+// forward used), so the products carry FP32-level accuracy.  Adam updates FP32
+// master weights, then the BF16 operand copies are repacked.
+//
+// Every mbarrier wait is bounded (the limit is a kernel argument).  A warpgroup
+// whose wait runs out stops issuing MMAs and skips its epilogues, waits once more
+// (bounded) for the MMA it already committed, and only then releases tensor memory;
+// the host sees MP_TIMEOUT.
 #include <cuda_bf16.h>
 #include <algorithm>
 #include <cmath>
@@ -26,6 +37,9 @@ namespace mp {
 struct Mlp {
     dbuf<float> theta, m1, m2, grad;
     dbuf<uint16_t> pack;  // W1t | W2t | W3t in core-matrix layout
+    dbuf<uint16_t> packn; // W2 | W3 untransposed in core-matrix layout (backward operands)
+    dbuf<float> wpart;    // weight-gradient partial products of the split batch
+    long long spin = 1ll << 22;  // mbarrier wait limit (polls)
     int adam_t = 0;
     // training scratch (sized for the largest batch seen)
     int cap = 0;
@@ -79,9 +93,12 @@ __device__ __forceinline__ void umma_commit(uint64_t *mbar) {
         smem_u32(mbar)));
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
+// after a wait ran out: the bound of the one further wait for the MMA already committed
+constexpr long long MLP_SPIN_DRAIN = 1ll << 24;
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, long long limit) {
     const uint32_t a = smem_u32(mbar);
-    for (int i = 0; i < (1 << 22); i++) {
+    for (long long i = 0; i < limit; i++) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred P1;\n\t"
@@ -139,6 +156,7 @@ struct MlpFwdArgs {
     uint16_t *h1, *h2;
     float *h3;
     int *err;
+    long long spin;          // mbarrier wait limit (polls)
 };
 
 // Four warpgroups per CTA work on four tiles at once, each with its own operand
@@ -163,6 +181,20 @@ struct MlpSmem {
 // barrier of one warpgroup (named barrier 1 + wg; 0 is __syncthreads)
 __device__ __forceinline__ void wg_sync(int wg) {
     asm volatile("bar.sync %0, 128;\n" ::"r"(1 + wg) : "memory");
+}
+
+// the same barrier, returning whether v holds in all 128 threads of the group
+__device__ __forceinline__ bool wg_all(int wg, bool v) {
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.b32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, 128, p;\n\t"
+        "selp.b32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((int)v), "r"(1 + wg)
+        : "memory");
+    return r != 0;
 }
 
 template <int MODE>
@@ -244,8 +276,12 @@ __global__ void __launch_bounds__(128 * MLP_WG, 1) k_mlp_forward(MlpFwdArgs A) {
                 }
                 umma_commit(mbar);
             }
-            if (!mbar_wait(mbar, phase))
+            // the group decides together: a wait that ran out anywhere stops the group
+            // before any thread reads the accumulator the MMA may still be writing
+            if (!wg_all(wg, mbar_wait(mbar, phase, A.spin))) {
                 ok = false;
+                break;
+            }
             phase ^= 1u;
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             // ---- epilogue: this thread's row of the accumulator
@@ -286,9 +322,15 @@ __global__ void __launch_bounds__(128 * MLP_WG, 1) k_mlp_forward(MlpFwdArgs A) {
             asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
             wg_sync(wg);
         }
+        if (!ok)
+            break;
         if (live)
             A.y[row] = out;
     }
+    // a group that gave up waits once more, bounded, for the MMA it committed
+    // (parity `phase`), so tensor memory is not released under it
+    if (!ok)
+        mbar_wait(mbar, phase, MLP_SPIN_DRAIN);
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (warp == 0)
@@ -299,11 +341,23 @@ __global__ void __launch_bounds__(128 * MLP_WG, 1) k_mlp_forward(MlpFwdArgs A) {
 }
 
 // ------------------------------------------------------------ small kernels
-// FP32 master weights -> transposed BF16 operand copies
-__global__ void k_mlp_pack(const float *theta, uint16_t *pack) {
+// FP32 master weights -> BF16 operand copies: transposed (forward B operands,
+// rows n) into pack; W2 and W3 as they are (rows k: the backward's B operands)
+// into packn
+constexpr int MLP_PACKN = 2 * MLP_H * MLP_H;
+__global__ void k_mlp_pack(const float *theta, uint16_t *pack, uint16_t *packn) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= MLP_PACK)
+    if (i >= MLP_PACK + MLP_PACKN)
         return;
+    if (i >= MLP_PACK) {
+        const int j = i - MLP_PACK;
+        const int which = j / (MLP_H * MLP_H), r = j % (MLP_H * MLP_H);
+        const int k = r / MLP_H, n = r % MLP_H;
+        const float w = theta[(which == 0 ? MLP_OFF_W2 : MLP_OFF_W3) + k * MLP_H + n];
+        __nv_bfloat16 h = __float2bfloat16_rn(w);
+        packn[which * MLP_H * MLP_H + cm_off(k, n, MLP_H)] = *reinterpret_cast<uint16_t *>(&h);
+        return;
+    }
     int n, k, K, off;
     float w;
     if (i < MLP_H * MLP_IN) {  // W1t[n][k] = W1[k][n]
@@ -329,11 +383,6 @@ __device__ __forceinline__ float bf(uint16_t u) {
     return __uint_as_float((uint32_t)u << 16);
 }
 
-// BF16-rounded weight W_l[k][n] as the forward pass used it
-__device__ __forceinline__ float wq(const float *theta, int off, int k, int n) {
-    return bf16_round(theta[off + k * MLP_H + n]);
-}
-
 // loss, output-layer gradients and dL/dh3 (pre-activation, masked by ReLU)
 __global__ void k_mlp_out_grad(int B, const float *y, const float *t, const int *tidx,
                                const float *h3, const float *theta, float *d3, float *grad,
@@ -350,36 +399,279 @@ __global__ void k_mlp_out_grad(int B, const float *y, const float *t, const int 
     }
 }
 
-// gW[k][n] = sum_b a[b][k] d[b][n], gb[n] = sum_b d[b][n]; a BF16 rows of width Kin
-__global__ void k_mlp_wgrad(int B, int Kin, const uint16_t *a, const int *aidx, const float *d,
-                            float *gW, float *gb) {
-    const int n = threadIdx.x;  // 128
-    const int k = blockIdx.x;   // Kin (+1 row for the bias)
-    float acc = 0.f;
-    if (k < Kin) {
-        for (int b = 0; b < B; b++) {
-            const int r = aidx ? aidx[b] : b;
-            acc = fmaf(bf(a[(size_t)r * Kin + k]), d[(size_t)b * MLP_H + n], acc);
-        }
-        gW[k * MLP_H + n] += acc;
-    } else {
-        for (int b = 0; b < B; b++)
-            acc += d[(size_t)b * MLP_H + n];
-        gb[n] += acc;
+// FP32 values -> BF16 high part and BF16 remainder, 8 at a time (one 16-byte
+// core-matrix row each)
+__device__ __forceinline__ void split_bf16x8(const float (&f)[8], uint4 &hi, uint4 &lo) {
+    float h[8], l[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        h[i] = bf16_round(f[i]);
+        l[i] = f[i] - h[i];
     }
+    hi = make_uint4(pack_bf16x2(h[0], h[1]), pack_bf16x2(h[2], h[3]), pack_bf16x2(h[4], h[5]),
+                    pack_bf16x2(h[6], h[7]));
+    lo = make_uint4(pack_bf16x2(l[0], l[1]), pack_bf16x2(l[2], l[3]), pack_bf16x2(l[4], l[5]),
+                    pack_bf16x2(l[6], l[7]));
 }
 
-// dprev[b][k] = (sum_n W[k][n] d[b][n]) * (h_prev[b][k] > 0)
-__global__ void k_mlp_dgrad(int B, const float *theta, int woff, const float *d,
-                            const uint16_t *hprev, float *dprev) {
-    const int b = blockIdx.x, k = threadIdx.x;  // blockDim 128
-    __shared__ float ds[MLP_H];
-    ds[k] = d[(size_t)b * MLP_H + k];
+struct MlpDgradSmem {
+    uint16_t ahi[MLP_TILE * MLP_H];  // D (hi), rows b, K = n
+    uint16_t alo[MLP_TILE * MLP_H];  // D (lo)
+    uint16_t w[MLP_H * MLP_H];       // W, rows k, K = n
+    uint64_t mbar;
+    uint32_t tmem;
+};
+
+// dprev[b][k] = (sum_n d[b][n] W[k][n]) * (hprev[b][k] > 0): one 128-row tile of the
+// batch per CTA, sixteen MMAs (M = N = 128, K = 16) over D's hi and lo parts
+__global__ void __launch_bounds__(128, 1)
+    k_mlp_dgrad_tc(int B, const float *__restrict__ d, const uint16_t *__restrict__ wn,
+                   const uint16_t *__restrict__ hprev, float *__restrict__ dprev, int *err,
+                   long long spin) {
+    extern __shared__ __align__(1024) unsigned char mlp_bw_raw[];
+    MlpDgradSmem &S = *reinterpret_cast<MlpDgradSmem *>(mlp_bw_raw);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int row = blockIdx.x * MLP_TILE + tid;
+    const bool live = row < B;
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(wn);
+        uint4 *dst = reinterpret_cast<uint4 *>(S.w);
+        for (int i = tid; i < MLP_H * MLP_H / 8; i += 128)
+            dst[i] = src[i];
+    }
+    const float4 *dr = reinterpret_cast<const float4 *>(d + (size_t)(live ? row : 0) * MLP_H);
+#pragma unroll 4
+    for (int c = 0; c < MLP_H; c += 8) {
+        float f[8];
+        const float4 x = live ? dr[c / 4] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 y = live ? dr[c / 4 + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+        f[0] = x.x, f[1] = x.y, f[2] = x.z, f[3] = x.w, f[4] = y.x, f[5] = y.y, f[6] = y.z, f[7] = y.w;
+        uint4 hi, lo;
+        split_bf16x8(f, hi, lo);
+        *reinterpret_cast<uint4 *>(&S.ahi[cm_off(tid, c, MLP_H)]) = hi;
+        *reinterpret_cast<uint4 *>(&S.alo[cm_off(tid, c, MLP_H)]) = lo;
+    }
+    if (tid == 0)
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&S.mbar)));
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_u32(&S.tmem)),
+                     "r"(MLP_H));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
-    float acc = 0.f;
-    for (int n = 0; n < MLP_H; n++)
-        acc = fmaf(wq(theta, woff, k, n), ds[n], acc);
-    dprev[(size_t)b * MLP_H + k] = bf(hprev[(size_t)b * MLP_H + k]) > 0.f ? acc : 0.f;
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = S.tmem;
+    if (tid == 0) {
+        const uint32_t ah = smem_u32(S.ahi), al = smem_u32(S.alo), bw = smem_u32(S.w);
+        for (int k0 = 0; k0 < MLP_H; k0 += 16) {
+            const uint32_t koff = (uint32_t)(k0 / 8) * 128u;
+            umma_bf16(tmem, umma_desc(ah + koff, MLP_H), umma_desc(bw + koff, MLP_H), k0 > 0);
+        }
+        for (int k0 = 0; k0 < MLP_H; k0 += 16) {
+            const uint32_t koff = (uint32_t)(k0 / 8) * 128u;
+            umma_bf16(tmem, umma_desc(al + koff, MLP_H), umma_desc(bw + koff, MLP_H), 1u);
+        }
+        umma_commit(&S.mbar);
+    }
+    const bool ok = __syncthreads_and(mbar_wait(&S.mbar, 0, spin)) != 0;
+    if (ok) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < MLP_H; c0 += 32) {
+            float v[32];
+            tmem_ld32(lane_addr + (uint32_t)c0, v);
+            if (live) {
+                const uint4 *hp = reinterpret_cast<const uint4 *>(hprev + (size_t)row * MLP_H + c0);
+                float4 *out = reinterpret_cast<float4 *>(dprev + (size_t)row * MLP_H + c0);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const uint4 hv = hp[q];
+                    const uint32_t w4[4] = {hv.x, hv.y, hv.z, hv.w};
+                    float m[8];
+#pragma unroll
+                    for (int t = 0; t < 4; t++) {
+                        m[2 * t] = bf((uint16_t)(w4[t] & 0xFFFFu)) > 0.f ? 1.f : 0.f;
+                        m[2 * t + 1] = bf((uint16_t)(w4[t] >> 16)) > 0.f ? 1.f : 0.f;
+                    }
+                    out[2 * q] = make_float4(v[8 * q] * m[0], v[8 * q + 1] * m[1],
+                                             v[8 * q + 2] * m[2], v[8 * q + 3] * m[3]);
+                    out[2 * q + 1] = make_float4(v[8 * q + 4] * m[4], v[8 * q + 5] * m[5],
+                                                 v[8 * q + 6] * m[6], v[8 * q + 7] * m[7]);
+                }
+            }
+        }
+    } else {
+        mbar_wait(&S.mbar, 0, MLP_SPIN_DRAIN);  // the committed MMA, before the release
+        if (tid == 0)
+            atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(S.tmem),
+                     "r"(MLP_H));
+}
+
+constexpr int MLP_WCHUNK = 64;   // batch rows per weight-gradient chunk (the MMA's K)
+constexpr int MLP_WSPLIT = 16;   // most CTAs per layer (partial products)
+
+struct MlpWgradSmem {
+    uint16_t a[MLP_H * MLP_WCHUNK];    // A^T chunk: rows k (M), K = batch rows
+    uint16_t bhi[MLP_H * MLP_WCHUNK];  // D^T chunk (hi): rows n (N), K = batch rows
+    uint16_t blo[MLP_H * MLP_WCHUNK];
+    uint64_t mbar;
+    uint32_t tmem;
+};
+
+struct MlpWgradArgs {
+    int B;
+    const uint16_t *X, *h1, *h2;  // layer inputs (features through idx)
+    const int *idx;
+    const float *d1, *d2, *d3;    // layer output gradients (pre-activation)
+    float *wpart, *bpart;         // [3][gridDim.x][128][128], [3][gridDim.x][128]
+    int *err;
+    long long spin;
+};
+
+// dW_L = A_L^T D_L over the batch: blockIdx.y = layer (0: features -> W1, 1: h1 -> W2,
+// 2: h2 -> W3), blockIdx.x = one of gridDim.x CTAs that take every gridDim.x-th
+// 64-row chunk; each CTA accumulates its chunks in tensor memory (M = N = 128; the
+// 64 feature rows of layer 0 padded with zero rows) and writes its partial product
+// and its column sums of D (the bias gradient)
+__global__ void __launch_bounds__(128, 1) k_mlp_wgrad_tc(MlpWgradArgs A) {
+    extern __shared__ __align__(1024) unsigned char mlp_bw_raw[];
+    MlpWgradSmem &S = *reinterpret_cast<MlpWgradSmem *>(mlp_bw_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, L = blockIdx.y;
+    const int Kin = L == 0 ? MLP_IN : MLP_H;
+    const uint16_t *act = L == 0 ? A.X : (L == 1 ? A.h1 : A.h2);
+    const int *aidx = L == 0 ? A.idx : nullptr;
+    const float *d = L == 0 ? A.d1 : (L == 1 ? A.d2 : A.d3);
+    if (tid == 0)
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&S.mbar)));
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_u32(&S.tmem)),
+                     "r"(MLP_H));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = S.tmem;
+    const int nchunks = (A.B + MLP_WCHUNK - 1) / MLP_WCHUNK;
+    float colsum = 0.f;
+    uint32_t phase = 0;
+    bool ok = true, any = false;
+    for (int ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+        const int b0 = ch * MLP_WCHUNK;
+        // thread t stages row t of A^T (activation column t) and row t of D^T
+#pragma unroll 1
+        for (int g = 0; g < MLP_WCHUNK; g += 8) {
+            uint32_t av[4];
+            float f[8];
+#pragma unroll
+            for (int j = 0; j < 8; j += 2) {
+                const int b = b0 + g + j;
+                uint32_t lo16 = 0, hi16 = 0;
+                if (tid < Kin) {
+                    if (b < A.B)
+                        lo16 = act[(size_t)(aidx ? aidx[b] : b) * Kin + tid];
+                    if (b + 1 < A.B)
+                        hi16 = act[(size_t)(aidx ? aidx[b + 1] : b + 1) * Kin + tid];
+                }
+                av[j / 2] = lo16 | (hi16 << 16);
+                f[j] = b < A.B ? d[(size_t)b * MLP_H + tid] : 0.f;
+                f[j + 1] = b + 1 < A.B ? d[(size_t)(b + 1) * MLP_H + tid] : 0.f;
+                colsum += f[j] + f[j + 1];
+            }
+            *reinterpret_cast<uint4 *>(&S.a[cm_off(tid, g, MLP_WCHUNK)]) =
+                make_uint4(av[0], av[1], av[2], av[3]);
+            uint4 hi, lo;
+            split_bf16x8(f, hi, lo);
+            *reinterpret_cast<uint4 *>(&S.bhi[cm_off(tid, g, MLP_WCHUNK)]) = hi;
+            *reinterpret_cast<uint4 *>(&S.blo[cm_off(tid, g, MLP_WCHUNK)]) = lo;
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        if (tid == 0) {
+            const uint32_t aa = smem_u32(S.a), bh = smem_u32(S.bhi), bl = smem_u32(S.blo);
+            for (int k0 = 0; k0 < MLP_WCHUNK; k0 += 16) {
+                const uint32_t koff = (uint32_t)(k0 / 8) * 128u;
+                umma_bf16(tmem, umma_desc(aa + koff, MLP_WCHUNK), umma_desc(bh + koff, MLP_WCHUNK),
+                          (any || k0 > 0) ? 1u : 0u);
+            }
+            for (int k0 = 0; k0 < MLP_WCHUNK; k0 += 16) {
+                const uint32_t koff = (uint32_t)(k0 / 8) * 128u;
+                umma_bf16(tmem, umma_desc(aa + koff, MLP_WCHUNK), umma_desc(bl + koff, MLP_WCHUNK),
+                          1u);
+            }
+            umma_commit(&S.mbar);
+        }
+        any = true;
+        // the operands are restaged only after the MMAs that read them completed
+        if (!__syncthreads_and(mbar_wait(&S.mbar, phase, A.spin))) {
+            ok = false;
+            break;
+        }
+        phase ^= 1u;
+    }
+    float *wp = A.wpart + ((size_t)L * gridDim.x + blockIdx.x) * MLP_H * MLP_H;
+    if (ok && any) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < MLP_H; c0 += 32) {
+            float v[32];
+            tmem_ld32(lane_addr + (uint32_t)c0, v);
+            float4 *out = reinterpret_cast<float4 *>(wp + (size_t)tid * MLP_H + c0);
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                out[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        }
+    } else if (ok) {
+        for (int c = 0; c < MLP_H; c++)
+            wp[(size_t)tid * MLP_H + c] = 0.f;
+    } else {
+        mbar_wait(&S.mbar, phase, MLP_SPIN_DRAIN);  // the committed MMAs, before the release
+        if (tid == 0)
+            atomicExch(A.err, 1);
+    }
+    A.bpart[((size_t)L * gridDim.x + blockIdx.x) * MLP_H + tid] = colsum;
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(S.tmem),
+                     "r"(MLP_H));
+}
+
+// the layers' weight and bias gradients: the partial products summed in CTA order
+__global__ void k_mlp_wgrad_reduce(int G, const float *__restrict__ wpart,
+                                   const float *__restrict__ bpart, float *grad) {
+    const int L = blockIdx.y;
+    const int Kin = L == 0 ? MLP_IN : MLP_H;
+    const int offW = L == 0 ? MLP_OFF_W1 : (L == 1 ? MLP_OFF_W2 : MLP_OFF_W3);
+    const int offB = L == 0 ? MLP_OFF_B1 : (L == 1 ? MLP_OFF_B2 : MLP_OFF_B3);
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;  // k * 128 + n, plus 128 bias rows
+    if (e < Kin * MLP_H) {
+        float acc = 0.f;
+        for (int g = 0; g < G; g++)
+            acc += wpart[((size_t)L * G + g) * MLP_H * MLP_H + e];
+        grad[offW + e] += acc;
+    } else if (e < Kin * MLP_H + MLP_H) {
+        const int n = e - Kin * MLP_H;
+        float acc = 0.f;
+        for (int g = 0; g < G; g++)
+            acc += bpart[((size_t)L * G + g) * MLP_H + n];
+        grad[offB + n] += acc;
+    }
 }
 
 __global__ void k_mlp_adam(float *theta, float *m1, float *m2, const float *g, int n, float lr,
@@ -548,7 +840,7 @@ template <int MODE> static int launch_forward(MlpFwdArgs &a, cudaStream_t s) {
 }
 
 static int repack(Mlp &m, cudaStream_t s) {
-    k_mlp_pack<<<(MLP_PACK + 255) / 256, 256, 0, s>>>(m.theta.p, m.pack.p);
+    k_mlp_pack<<<(MLP_PACK + MLP_PACKN + 255) / 256, 256, 0, s>>>(m.theta.p, m.pack.p, m.packn.p);
     MP_CHECK_LAUNCH();
     return MP_OK;
 }
@@ -558,7 +850,9 @@ int mlp_create(Mlp **out, uint64_t seed) {
     int rc;
     if ((rc = m->theta.alloc(MLP_NPARAM)) || (rc = m->m1.alloc(MLP_NPARAM)) ||
         (rc = m->m2.alloc(MLP_NPARAM)) || (rc = m->grad.alloc(MLP_NPARAM)) ||
-        (rc = m->pack.alloc(MLP_PACK)) || (rc = m->err.alloc(1))) {
+        (rc = m->pack.alloc(MLP_PACK)) || (rc = m->packn.alloc(MLP_PACKN)) ||
+        (rc = m->wpart.alloc((size_t)3 * MLP_WSPLIT * (MLP_H * MLP_H + MLP_H))) ||
+        (rc = m->err.alloc(1))) {
         delete m;
         return rc;
     }
@@ -594,8 +888,11 @@ static int mlp_check_err(Mlp &m, cudaStream_t s) {
     int e = 0;
     MP_CUDA(cudaMemcpyAsync(&e, m.err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     MP_CUDA(cudaStreamSynchronize(s));
-    if (e)
+    if (e) {
+        MP_CUDA(cudaMemsetAsync(m.err.p, 0, sizeof(int), s));
+        MP_CUDA(cudaStreamSynchronize(s));
         return fail(MP_TIMEOUT, "tensor-core MLP: an mbarrier wait ran out");
+    }
     return MP_OK;
 }
 
@@ -615,6 +912,7 @@ int mlp_predict_fields(Mlp &m, const MlpFields &F, double *x, double *corr, cons
     a.X = m.fx.p;
     a.y = m.fy.p;
     a.err = m.err.p;
+    a.spin = m.spin;
     MP_TRY(launch_forward<MLP_MODE_ROWS>(a, s));
     k_mlp_combine<<<g, 256, 0, s>>>(F, m.fy.p, x, corr, step);
     MP_CHECK_LAUNCH();
@@ -662,6 +960,8 @@ static int ensure_cap(Mlp &m, int B) {
     return MP_OK;
 }
 
+static int bw_smem(size_t bytes) { return (int)bytes + 1024; }
+
 // forward + backward of one batch: grad = dL/dtheta (accumulated from zero), loss to lossbuf
 static int batch_grad(Mlp &m, const uint16_t *X, const float *t, const int *idx, int B,
                       cudaStream_t s) {
@@ -677,27 +977,45 @@ static int batch_grad(Mlp &m, const uint16_t *X, const float *t, const int *idx,
     a.h2 = m.h2.p;
     a.h3 = m.h3.p;
     a.err = m.err.p;
+    a.spin = m.spin;
     MP_TRY(launch_forward<MLP_MODE_TRAIN>(a, s));
     MP_CUDA(cudaMemsetAsync(m.grad.p, 0, sizeof(float) * MLP_NPARAM, s));
     MP_CUDA(cudaMemsetAsync(m.lossbuf.p, 0, sizeof(float), s));
     k_mlp_out_grad<<<B, MLP_H, 0, s>>>(B, m.y.p, t, idx, m.h3.p, m.theta.p, m.d3.p, m.grad.p,
                                       m.lossbuf.p);
     MP_CHECK_LAUNCH();
-    // layer 3: a = h2, d = d3
-    k_mlp_wgrad<<<MLP_H + 1, MLP_H, 0, s>>>(B, MLP_H, m.h2.p, nullptr, m.d3.p,
-                                            m.grad.p + MLP_OFF_W3, m.grad.p + MLP_OFF_B3);
+    // input gradients of layers 3 and 2 on the tensor cores
+    const int ds = bw_smem(sizeof(MlpDgradSmem));
+    MP_CUDA(cudaFuncSetAttribute(k_mlp_dgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, ds));
+    const unsigned tiles = (unsigned)((B + MLP_TILE - 1) / MLP_TILE);
+    k_mlp_dgrad_tc<<<tiles, 128, ds, s>>>(B, m.d3.p, m.packn.p + MLP_H * MLP_H, m.h2.p, m.d2.p,
+                                          m.err.p, m.spin);
     MP_CHECK_LAUNCH();
-    k_mlp_dgrad<<<B, MLP_H, 0, s>>>(B, m.theta.p, MLP_OFF_W3, m.d3.p, m.h2.p, m.d2.p);
+    k_mlp_dgrad_tc<<<tiles, 128, ds, s>>>(B, m.d2.p, m.packn.p, m.h1.p, m.d1.p, m.err.p, m.spin);
     MP_CHECK_LAUNCH();
-    // layer 2: a = h1, d = d2
-    k_mlp_wgrad<<<MLP_H + 1, MLP_H, 0, s>>>(B, MLP_H, m.h1.p, nullptr, m.d2.p,
-                                            m.grad.p + MLP_OFF_W2, m.grad.p + MLP_OFF_B2);
+    // weight gradients of the three layers in one launch, the batch split across CTAs
+    const int ws = bw_smem(sizeof(MlpWgradSmem));
+    MP_CUDA(cudaFuncSetAttribute(k_mlp_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, ws));
+    const int nch = (B + MLP_WCHUNK - 1) / MLP_WCHUNK;
+    const int G = std::min(nch, MLP_WSPLIT);
+    MlpWgradArgs w{};
+    w.B = B;
+    w.X = X;
+    w.h1 = m.h1.p;
+    w.h2 = m.h2.p;
+    w.idx = idx;
+    w.d1 = m.d1.p;
+    w.d2 = m.d2.p;
+    w.d3 = m.d3.p;
+    w.wpart = m.wpart.p;
+    w.bpart = m.wpart.p + (size_t)3 * MLP_WSPLIT * MLP_H * MLP_H;
+    w.err = m.err.p;
+    w.spin = m.spin;
+    k_mlp_wgrad_tc<<<dim3((unsigned)G, 3), 128, ws, s>>>(w);
     MP_CHECK_LAUNCH();
-    k_mlp_dgrad<<<B, MLP_H, 0, s>>>(B, m.theta.p, MLP_OFF_W2, m.d2.p, m.h1.p, m.d1.p);
-    MP_CHECK_LAUNCH();
-    // layer 1: a = features
-    k_mlp_wgrad<<<MLP_IN + 1, MLP_H, 0, s>>>(B, MLP_IN, X, idx, m.d1.p, m.grad.p + MLP_OFF_W1,
-                                             m.grad.p + MLP_OFF_B1);
+    // the partial arrays are indexed with the launch's G
+    k_mlp_wgrad_reduce<<<dim3((MLP_H * MLP_H + MLP_H + 255) / 256, 3), 256, 0, s>>>(
+        G, w.wpart, w.bpart, m.grad.p);
     MP_CHECK_LAUNCH();
     return MP_OK;
 }
@@ -810,6 +1128,7 @@ extern "C" int mp_mlp_forward(mp_mlp h, const float *X, int n, float *y) {
     a.X = xb.p;
     a.y = yd.p;
     a.err = h->m->err.p;
+    a.spin = h->m->spin;
     MP_TRY(launch_forward<MLP_MODE_ROWS>(a, 0));
     MP_CUDA(cudaMemcpy(y, yd.p, sizeof(float) * n, cudaMemcpyDefault));
     return mlp_check_err(*h->m, 0);
@@ -843,6 +1162,13 @@ extern "C" int mp_mlp_train(mp_mlp h, const float *X, const float *t, int n, int
     MP_TRY(to_bf16_rows(X, (size_t)n * MLP_IN, xb, 0));
     MP_TRY(stage_in(t, (size_t)n, tt, &dt, 0));
     return mlp_train(*h->m, xb.p, dt, n, epochs, batch, lr, seed, loss, 0);
+}
+
+extern "C" int mp_mlp_set_spin_limit(mp_mlp h, long long polls) {
+    if (!h || polls < 0)
+        return fail(MP_BAD_ARG, "mp_mlp_set_spin_limit: a handle and a limit >= 0");
+    h->m->spin = polls;
+    return MP_OK;
 }
 
 extern "C" int mp_mlp_destroy(mp_mlp h) {

@@ -51,6 +51,20 @@ bool is_device_ptr(const void *p) {
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+bool is_current_device_ptr(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (a.type == cudaMemoryTypeManaged)
+        return true;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return false;
+    return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
 }  // namespace mp
 
 using namespace mp;

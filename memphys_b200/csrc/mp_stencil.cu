@@ -23,7 +23,10 @@
 // partial pivoting.  To reproduce those numbers the estimator needs the LU
 // factors, so this kernel factorises A in shared memory (one warp per system,
 // row swaps as in the reference, first max |a| wins) and runs the estimator.
+#include <algorithm>
 #include <cmath>
+#include <memory>
+#include <vector>
 #include "mp_common.cuh"
 
 namespace mp {
@@ -213,39 +216,199 @@ __device__ void load_scaled_points(const StencilJob &J, int id, int n, double *s
 }
 
 // -------------------------------------------------------------- weights
-// Shared memory per group: points (MAX_S*3) + scales (6) + pivot row (W)
-// + argmax slots (2*G) + matrix staging (S*(LD)).
-template <int G, int W> struct GJShape {
+// One thread per matrix row of a group of G warps (S <= 32 G); GROUPS groups
+// per CTA work on independent systems.  Shared memory per group: points, scales
+// (+ scaled probe), the monomials of every node, the pivot row, the cross-warp
+// pivot candidates.
+template <int G, int W, int GROUPS> struct GJShape {
     static constexpr int NT = 32 * G;
-    static constexpr int GROUPS = (G == 1) ? 4 : 1;  // independent groups per CTA
     static constexpr int CTA = NT * GROUPS;
     static constexpr int SMAX = W - 3;               // rows available (R >= 3)
-    static constexpr int LD = (W % 2) ? W : W + 1;   // odd leading dim: conflict-free row loads
     static constexpr int PTS = SMAX * MAX_DIM;
-    static constexpr int DOUBLES = PTS + 3 * MAX_DIM + W + 2 * G + SMAX * LD;
+    // two pivot-row buffers (alternating steps) of W + 2 doubles each: element e of
+    // the pivot row sits at [e + 1], so elements 1, 2 / 3, 4 / ... are 16-byte pairs
+    static constexpr int PROW = (W + 3) / 2 * 2;
+    static constexpr int DOUBLES_RAW = PTS + 3 * MAX_DIM + SMAX * MAX_M + 2 * PROW + 4 * G + 4 * NT;
+    static constexpr int DOUBLES = (DOUBLES_RAW + 1) / 2 * 2;
+    // CTAs per SM the register allocation must allow (one-warp systems: 16 warps per
+    // SM, two-warp systems: 10; the three-warp rows need their 255 registers)
+    static constexpr int WARPS_TARGET = G == 1 ? 16 : (G == 2 ? 10 : 1);
+    static constexpr int MINB = (WARPS_TARGET + G * GROUPS - 1) / (G * GROUPS);
+    // steps per chunk of the elimination: within a chunk the update runs over the
+    // chunk's first live width, so the unrolled code stays ~W^2 / (2 CH) long
+    static constexpr int CH = W <= 56 ? 4 : (W <= 84 ? 8 : 16);
+    static constexpr int NCH = (SMAX + CH - 1) / CH;
 };
 
-template <int G, int W>
-__global__ void __launch_bounds__(GJShape<G, W>::CTA)
+// The row of a thread: entries j < W of [A | B] for row r (coefficient_computations
+// .cpp:70-106 for A, :108-292 for B, :430-454 in interpolation mode), assembled in
+// registers: node-node entries from the scaled points, polynomial entries from the
+// group's monomial table, the right-hand sides from aug_entry.
+template <int W>
+__device__ __forceinline__ void assemble_row(double (&a)[W], int r, int n, int m, int S, int R,
+                                             int dim, int phs, const double *sp, const double *sc,
+                                             const double *pm, const double *xp, double *rhs) {
+    // this row's right-hand sides, through shared memory (a register copy would stay
+    // live across the whole unrolled row)
+    const bool node = r < n;
+    for (int c = 0; c < R; c++)
+        rhs[c] = r < S ? aug_entry(r, S + c, n, m, dim, phs, sp, sc, xp) : 0.0;
+    double xr[MAX_DIM] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < MAX_DIM; d++)
+        if (node && d < dim)
+            xr[d] = sp[r * dim + d];
+    const int p = r - n;  // polynomial row index (r >= n)
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+        double v = 0.0;
+        if (r < S) {
+            if (j < n) {
+                if (node) {
+                    double r2 = 0.0;
+#pragma unroll
+                    for (int d = 0; d < MAX_DIM; d++)
+                        if (d < dim) {
+                            const double t = xr[d] - sp[j * dim + d];
+                            r2 = fma(t, t, r2);
+                        }
+                    v = (j == r) ? 0.0 : rpow_odd(r2, phs);
+                } else {
+                    v = pm[j * MAX_M + p];
+                }
+            } else if (j < S) {
+                v = node ? pm[r * MAX_M + (j - n)] : 0.0;
+            } else if (j < S + R) {
+                v = rhs[j - S];
+            }
+        }
+        a[j] = v;
+    }
+}
+
+// one elimination step with the live width bounded by WC: rows drop their column
+// k (a[0]) and shift left; the pivot row itself is zeroed out of the update (l = 0).
+// pb holds pivot-row element e at pb[e + 1] (16-byte pairs from element 1 on).
+template <int W, int WC>
+__device__ __forceinline__ void gj_update(double (&a)[W], const double *pb, double l) {
+#pragma unroll
+    for (int j = 0; j < WC - 1; j += 2) {
+        const double2 q = *reinterpret_cast<const double2 *>(pb + j + 2);
+        a[j] = fma(-l, q.x, a[j + 1]);
+        if (j + 1 < WC - 1)
+            a[j + 1] = fma(-l, q.y, a[j + 2]);
+    }
+    a[WC - 1] = 0.0;
+}
+
+// the pivot row's live entries into pb (element e at pb[e + 1])
+template <int W, int WC>
+__device__ __forceinline__ void gj_publish(const double (&a)[W], double *pb) {
+    pb[1] = a[0];
+#pragma unroll
+    for (int e = 1; e < WC; e += 2)
+        *reinterpret_cast<double2 *>(pb + e + 1) = make_double2(a[e], e + 1 < WC ? a[e + 1] : 0.0);
+}
+
+// per-thread elimination state
+struct GjRow {
+    bool eligible, singular;
+    int my_step;
+    double my_diag;
+};
+
+// chunk C of the elimination (steps C*CH .. C*CH + CH - 1): the live width of every
+// row is at most WC = W - C*CH there, so the update and the pivot-row publication
+// run over WC registers (a compile-time bound, registers stay statically indexed)
+template <int G, int W, int GROUPS, int C, class Sync>
+__device__ __forceinline__ void gj_chunks(double (&a)[W], GjRow &st, int S, int tid, int lane,
+                                          int warp_in_grp, double *prow, double *amax, Sync sync) {
+    using Sh = GJShape<G, W, GROUPS>;
+    if constexpr (C < Sh::NCH) {
+        if (C * Sh::CH >= S)
+            return;
+        constexpr int WC = W - C * Sh::CH;
+        const int kend = min(S, (C + 1) * Sh::CH);
+        for (int k = C * Sh::CH; k < kend; k++) {
+            // buffers alternate between steps, so no barrier is needed between one
+            // step's reads of the pivot row and the next step's publication
+            double *pb = prow + (k & 1) * Sh::PROW, *am = amax + (k & 1) * 2 * G;
+            // ---- pivot: largest |a[0]| among rows not yet used, lowest row on ties
+            // (|a| >= 0 orders as its bit pattern: high words first, then low words)
+            const unsigned long long key =
+                st.eligible ? (unsigned long long)__double_as_longlong(fabs(a[0])) : 0ull;
+            const unsigned khi = (unsigned)(key >> 32), klo = (unsigned)key;
+            const unsigned mhi = __reduce_max_sync(0xffffffffu, khi);
+            const unsigned mlo = __reduce_max_sync(0xffffffffu, khi == mhi ? klo : 0u);
+            const unsigned ball =
+                __ballot_sync(0xffffffffu, st.eligible && khi == mhi && klo == mlo);
+            const double wmx =
+                __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+            int p;
+            double mx;
+            if (G == 1) {
+                p = __ffs(ball) - 1;
+                mx = wmx;
+            } else {
+                if (lane == 0) {
+                    am[warp_in_grp] = wmx;
+                    am[G + warp_in_grp] = ball ? (double)(warp_in_grp * 32 + __ffs(ball) - 1) : -1.0;
+                }
+                sync();
+                mx = -1.0;
+                p = -1;
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    const double v = am[g];
+                    const int pg = (int)am[G + g];
+                    if (pg >= 0 && v > mx) {
+                        mx = v;
+                        p = pg;
+                    }
+                }
+            }
+            if (tid == p) {
+                gj_publish<W, WC>(a, pb);
+                st.eligible = false;
+                st.my_step = k;
+                st.my_diag = a[0];
+            }
+            sync();
+            const double piv = pb[1];
+            if (!(mx > 0.0))
+                st.singular = true;
+            const double l = (tid == p) ? 0.0 : a[0] / piv;
+            gj_update<W, WC>(a, pb, l);
+        }
+        gj_chunks<G, W, GROUPS, C + 1>(a, st, S, tid, lane, warp_in_grp, prow, amax, sync);
+    }
+}
+
+template <int G, int W, int GROUPS>
+__global__ void __launch_bounds__(GJShape<G, W, GROUPS>::CTA, GJShape<G, W, GROUPS>::MINB)
     stencil_gj_kernel(StencilJob J) {
-    using Sh = GJShape<G, W>;
-    extern __shared__ double smem_raw[];
+    using Sh = GJShape<G, W, GROUPS>;
+    extern __shared__ __align__(16) double smem_raw[];
+    static_assert((Sh::PTS + 3 * MAX_DIM + Sh::SMAX * MAX_M) % 2 == 0,
+                  "pivot rows must start on a 16-byte boundary");
     const int grp = threadIdx.x / Sh::NT, tid = threadIdx.x % Sh::NT;
     const int lane = threadIdx.x & 31, warp_in_grp = tid >> 5;
     double *base = smem_raw + grp * Sh::DOUBLES;
     // sc: scales, minima, scaled probe (interpolation mode)
-    double *sp = base, *sc = sp + Sh::PTS, *prow = sc + 3 * MAX_DIM;
-    double *amax = prow + W;
-    double *mat = amax + 2 * G;
+    double *sp = base, *sc = sp + Sh::PTS, *pm = sc + 3 * MAX_DIM;
+    double *prow = pm + Sh::SMAX * MAX_M, *amax = prow + 2 * Sh::PROW;
+    double *rhs = amax + 4 * G + 4 * tid;
     auto sync = [&]() {
         if (G == 1)
             __syncwarp();
-        else
+        else if (GROUPS == 1)
             __syncthreads();
+        else
+            asm volatile("bar.sync %0, %1;\n" ::"r"(1 + grp), "r"(Sh::NT) : "memory");
     };
     const int dim = J.dim, m = J.m, R = J.probe ? 1 : dim + 1;
     double *xp = J.probe ? sc + 2 * MAX_DIM : nullptr;
-    __shared__ int s_item[Sh::GROUPS];
+    __shared__ int s_item[GROUPS];
     for (;;) {
         if (tid == 0)
             s_item[grp] = (int)atomicAdd(J.queue, 1u);
@@ -255,73 +418,25 @@ __global__ void __launch_bounds__(GJShape<G, W>::CTA)
         if (t >= J.count)
             break;
         const int id = sys_id(J, t);
-        const int n = sys_n(J, id), S = n + m, SR = S + R;
+        const int n = sys_n(J, id), S = n + m;
         load_scaled_points(J, id, n, sp, sc, tid, Sh::NT, sync);
         if (xp) {  // the probe shifted and scaled with its stencil (:23-30)
             if (tid < dim)
                 xp[tid] = (J.probe[(size_t)id * dim + tid] - sc[MAX_DIM + tid]) / sc[tid];
-            sync();
         }
-        for (int q = tid; q < S * SR; q += Sh::NT) {
-            int r = q / SR, j = q - r * SR;
-            mat[r * Sh::LD + j] = aug_entry(r, j, n, m, dim, J.phs, sp, sc, xp);
+        // monomials of every node (the P block and its transpose)
+        for (int q = tid; q < n * m; q += Sh::NT) {
+            const int i = q / m, pp = q - i * m;
+            pm[i * MAX_M + pp] = monomial(sp + i * dim, pp, dim);
         }
         sync();
         double a[W];
-        const bool live = tid < S;
-#pragma unroll
-        for (int j = 0; j < W; j++)
-            a[j] = (live && j < SR) ? mat[tid * Sh::LD + j] : 0.0;
-        bool eligible = live;
-        int my_step = -1;
-        double my_diag = 1.0;
-        bool singular = false;
-        for (int k = 0; k < S; k++) {
-            // ---- pivot: largest |a[0]| among rows not yet used, lowest row on ties
-            double cand = eligible ? fabs(a[0]) : -1.0;
-            double mx = cand;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-                mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-            unsigned ball = __ballot_sync(0xffffffffu, cand == mx);
-            int p;
-            if (G == 1) {
-                p = __ffs(ball) - 1;
-            } else {
-                if (lane == 0) {
-                    amax[warp_in_grp] = mx;
-                    amax[G + warp_in_grp] = (double)(warp_in_grp * 32 + __ffs(ball) - 1);
-                }
-                __syncthreads();
-                double best = amax[0];
-                p = (int)amax[G];
-#pragma unroll
-                for (int g = 1; g < G; g++)
-                    if (amax[g] > best) {
-                        best = amax[g];
-                        p = (int)amax[G + g];
-                    }
-                mx = best;
-            }
-            if (tid == p) {
-#pragma unroll
-                for (int j = 0; j < W; j++)
-                    prow[j] = a[j];
-                eligible = false;
-                my_step = k;
-                my_diag = a[0];
-            }
-            sync();
-            const double piv = prow[0];
-            if (!(mx > 0.0))
-                singular = true;
-            const double l = (tid == p) ? 0.0 : a[0] / piv;
-#pragma unroll
-            for (int j = 0; j < W - 1; j++)
-                a[j] = fma(-l, prow[j + 1], a[j + 1]);
-            a[W - 1] = 0.0;
-            sync();
-        }
+        assemble_row<W>(a, tid, n, m, S, R, dim, J.phs, sp, sc, pm, xp, rhs);
+        GjRow st{tid < S, false, -1, 1.0};
+        gj_chunks<G, W, GROUPS, 0>(a, st, S, tid, lane, warp_in_grp, prow, amax, sync);
+        const int my_step = st.my_step;
+        const double my_diag = st.my_diag;
+        const bool singular = st.singular;
         // ---- results: thread that pivoted at step k holds solution row k
         if (my_step >= 0 && my_step < n) {
             const double inv = 1.0 / my_diag;
@@ -590,16 +705,17 @@ static int upload_exponents(int dim, int poly_deg, int *m_out) {
     return MP_OK;
 }
 
-template <int G, int W> static int launch_gj(StencilJob J, cudaStream_t s) {
-    using Sh = GJShape<G, W>;
-    size_t smem = (size_t)Sh::DOUBLES * Sh::GROUPS * sizeof(double);
-    auto k = stencil_gj_kernel<G, W>;
+template <int G, int W, int GROUPS> static int launch_gj(StencilJob J, cudaStream_t s) {
+    using Sh = GJShape<G, W, GROUPS>;
+    size_t smem = (size_t)Sh::DOUBLES * GROUPS * sizeof(double);
+    auto k = stencil_gj_kernel<G, W, GROUPS>;
     MP_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     MP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, Sh::CTA, smem));
     if (per_sm < 1)
-        return fail(MP_CUDA_ERROR, "stencil kernel G=%d W=%d does not fit on an SM", G, W);
-    int groups_needed = (J.count + Sh::GROUPS - 1) / Sh::GROUPS;
+        return fail(MP_CUDA_ERROR, "stencil kernel G=%d W=%d x%d does not fit on an SM", G, W,
+                    GROUPS);
+    int groups_needed = (J.count + GROUPS - 1) / GROUPS;
     int grid = sm_count() * per_sm;
     if (grid > groups_needed)
         grid = groups_needed;
@@ -611,24 +727,105 @@ template <int G, int W> static int launch_gj(StencilJob J, cudaStream_t s) {
     return MP_OK;
 }
 
-// Size classes: G = ceil(S/32) warps (one row per thread) and a register
-// row of width W = 32G + 4 >= S + dim + 1.
+// Size classes: a register row of width W >= S + dim + 1 (the narrowest that
+// fits: the elimination's work grows with W) and G = ceil(S / 32) warps, one row per
+// thread.
+constexpr int GJ_CLASSES = 7;
+static const int gj_width[GJ_CLASSES] = {36, 44, 56, 68, 76, 84, 100};
+static const int gj_warps[GJ_CLASSES] = {1, 2, 2, 2, 3, 3, 3};
+
 static int gj_class(int S, int R) {
-    for (int c = 0; c < 3; c++) {
-        const int G = c + 1;
-        if (S <= 32 * G && S + R <= 32 * G + 4)
+    for (int c = 0; c < GJ_CLASSES; c++)
+        if (S <= 32 * gj_warps[c] && S + R <= gj_width[c])
             return c;
-    }
     return -1;
 }
 
-static int launch_class(int cls, const StencilJob &J, cudaStream_t s) {
-    switch (cls) {
-    case 0: return launch_gj<1, 36>(J, s);
-    case 1: return launch_gj<2, 68>(J, s);
-    case 2: return launch_gj<3, 100>(J, s);
+// CTA shapes of a class: systems (groups of G warps) per CTA
+constexpr int GJ_SHAPES = 4;
+static const int gj_groups[GJ_CLASSES][GJ_SHAPES] = {{1, 2, 4, 8}, {1, 2, 0, 0}, {1, 2, 0, 0},
+                                                     {1, 2, 0, 0}, {1, 2, 0, 0}, {1, 2, 0, 0},
+                                                     {1, 2, 0, 0}};
+
+static int launch_shape(int cls, int shape, const StencilJob &J, cudaStream_t s) {
+    switch (cls * GJ_SHAPES + shape) {
+    case 0: return launch_gj<1, 36, 1>(J, s);
+    case 1: return launch_gj<1, 36, 2>(J, s);
+    case 2: return launch_gj<1, 36, 4>(J, s);
+    case 3: return launch_gj<1, 36, 8>(J, s);
+    case 4: return launch_gj<2, 44, 1>(J, s);
+    case 5: return launch_gj<2, 44, 2>(J, s);
+    case 8: return launch_gj<2, 56, 1>(J, s);
+    case 9: return launch_gj<2, 56, 2>(J, s);
+    case 12: return launch_gj<2, 68, 1>(J, s);
+    case 13: return launch_gj<2, 68, 2>(J, s);
+    case 16: return launch_gj<3, 76, 1>(J, s);
+    case 17: return launch_gj<3, 76, 2>(J, s);
+    case 20: return launch_gj<3, 84, 1>(J, s);
+    case 21: return launch_gj<3, 84, 2>(J, s);
+    case 24: return launch_gj<3, 100, 1>(J, s);
+    case 25: return launch_gj<3, 100, 2>(J, s);
     }
-    return fail(MP_BAD_ARG, "stencil size class %d", cls);
+    return fail(MP_BAD_ARG, "stencil size class %d shape %d", cls, shape);
+}
+
+// The CTA shape of each (class, dimension), chosen by the autotuner on the first
+// batched call that has enough systems of the class (-1: not tuned yet; the
+// default then is 4 systems per CTA for one-warp systems, one otherwise).
+static int g_gj_shape[GJ_CLASSES][2] = {{-1, -1}, {-1, -1}, {-1, -1}, {-1, -1},
+                                        {-1, -1}, {-1, -1}, {-1, -1}};
+
+static int class_shape_of(int cls, int dim) {
+    const int t = g_gj_shape[cls][dim - 2];
+    return t >= 0 ? t : (cls == 0 ? 2 : 0);
+}
+
+static int launch_class(int cls, const StencilJob &J, cudaStream_t s) {
+    return launch_shape(cls, class_shape_of(cls, J.dim), J, s);
+}
+
+// Time every CTA shape of a class on a sample of its systems (the first
+// `sample` of the class list; the sample's outputs are written, as the full run
+// writes them again) with CUDA events, median of three, and keep the fastest.
+static int gj_autotune(int cls, StencilJob J, int sample, cudaStream_t s) {
+    if (g_gj_shape[cls][J.dim - 2] >= 0)
+        return MP_OK;
+    J.count = std::min(J.count, sample);
+    cudaEvent_t e0, e1;
+    MP_CUDA(cudaEventCreate(&e0));
+    MP_CUDA(cudaEventCreate(&e1));
+    int best = -1;
+    float best_us = 0.f;
+    for (int sh = 0; sh < GJ_SHAPES; sh++) {
+        if (!gj_groups[cls][sh])
+            continue;
+        float t[3];
+        int rc = MP_OK;
+        for (int rep = 0; rep < 4 && rc == MP_OK; rep++) {
+            cudaEventRecord(e0, s);
+            rc = launch_shape(cls, sh, J, s);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0)
+                t[rep - 1] = ms * 1e3f;
+        }
+        if (rc != MP_OK) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return rc;
+        }
+        std::sort(t, t + 3);
+        if (best < 0 || t[1] < best_us) {
+            best = sh;
+            best_us = t[1];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    g_gj_shape[cls][J.dim - 2] = best;
+    return MP_OK;
 }
 
 static int launch_cond(StencilJob J, int s_max, cudaStream_t s) {
@@ -792,6 +989,174 @@ extern "C" int mp_stencil_weights(const double *xyz, int nv, int dim, const int 
     return st_;
 }
 
+// A batch of uneven systems, classified once: the systems of each size class as a
+// device list, a side stream per class forked from and joined to the caller's
+// stream, the queue and singular counters.  Runs launch only.
+struct mp_stencil_plan_s {
+    int nsys = 0, dim = 0, m = 0, poly_deg = 0, s_max = 0;
+    int64_t npts = 0;
+    int count[GJ_CLASSES] = {};
+    dbuf<int> list[GJ_CLASSES];
+    dbuf<unsigned int> words;  // per class: queue (4 words apart), singular count
+    cudaStream_t side[GJ_CLASSES] = {};
+    cudaEvent_t fork = nullptr, join[GJ_CLASSES] = {};
+    const int *sizes = nullptr;
+    const int64_t *offsets = nullptr;
+    dbuf<int> own_sizes;
+    dbuf<int64_t> own_offsets;
+    ~mp_stencil_plan_s() {
+        for (int c = 0; c < GJ_CLASSES; c++) {
+            if (side[c])
+                cudaStreamDestroy(side[c]);
+            if (join[c])
+                cudaEventDestroy(join[c]);
+        }
+        if (fork)
+            cudaEventDestroy(fork);
+    }
+};
+
+extern "C" int mp_stencil_plan_create(int nsys, const int *sizes, const int64_t *offsets, int dim,
+                                      int poly_deg, mp_stencil_plan *out) {
+    if (!out || nsys <= 0 || !sizes || !offsets || (dim != 2 && dim != 3))
+        return fail(MP_BAD_ARG, "mp_stencil_plan_create: bad arguments");
+    int m = mp_num_poly_terms(dim, poly_deg);
+    if (m <= 0 || m > MAX_M)
+        return fail(MP_BAD_ARG, "poly_deg %d in %dD gives %d monomials (max %d)", poly_deg, dim, m,
+                    MAX_M);
+    const int R = dim + 1;
+    std::vector<int> hs(nsys);
+    std::vector<int64_t> ho(nsys);
+    MP_CUDA(cudaMemcpy(hs.data(), sizes, sizeof(int) * nsys, cudaMemcpyDefault));
+    MP_CUDA(cudaMemcpy(ho.data(), offsets, sizeof(int64_t) * nsys, cudaMemcpyDefault));
+    std::unique_ptr<mp_stencil_plan_s> P(new mp_stencil_plan_s);
+    P->nsys = nsys;
+    P->dim = dim;
+    P->m = m;
+    P->poly_deg = poly_deg;
+    std::vector<int> lists[GJ_CLASSES];
+    for (int i = 0; i < nsys; i++) {
+        if (hs[i] < 2)
+            return fail(MP_BAD_ARG, "system %d has %d nodes", i, hs[i]);
+        const int c = gj_class(hs[i] + m, R);
+        if (c < 0)
+            return fail(MP_BAD_ARG, "system %d: %d nodes + %d monomials exceeds %d", i, hs[i], m,
+                        MAX_S);
+        lists[c].push_back(i);
+        P->npts = std::max<int64_t>(P->npts, ho[i] + hs[i]);
+        P->s_max = std::max(P->s_max, hs[i] + m);
+    }
+    if (is_device_ptr(sizes) && is_device_ptr(offsets)) {
+        P->sizes = sizes;
+        P->offsets = offsets;
+    } else {
+        MP_TRY(P->own_sizes.alloc(nsys));
+        MP_TRY(P->own_offsets.alloc(nsys));
+        MP_CUDA(cudaMemcpy(P->own_sizes.p, hs.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice));
+        MP_CUDA(cudaMemcpy(P->own_offsets.p, ho.data(), sizeof(int64_t) * nsys,
+                           cudaMemcpyHostToDevice));
+        P->sizes = P->own_sizes.p;
+        P->offsets = P->own_offsets.p;
+    }
+    MP_TRY(P->words.alloc(4 * GJ_CLASSES));
+    MP_CUDA(cudaMemset(P->words.p, 0, sizeof(unsigned int) * 4 * GJ_CLASSES));
+    MP_CUDA(cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming));
+    for (int c = 0; c < GJ_CLASSES; c++) {
+        P->count[c] = (int)lists[c].size();
+        if (lists[c].empty())
+            continue;
+        MP_TRY(P->list[c].alloc(lists[c].size()));
+        MP_CUDA(cudaMemcpy(P->list[c].p, lists[c].data(), sizeof(int) * lists[c].size(),
+                           cudaMemcpyHostToDevice));
+        MP_CUDA(cudaStreamCreateWithFlags(&P->side[c], cudaStreamNonBlocking));
+        MP_CUDA(cudaEventCreateWithFlags(&P->join[c], cudaEventDisableTiming));
+    }
+    *out = P.release();
+    return MP_OK;
+}
+
+// the jobs of the plan's classes for one run
+static StencilJob plan_job(mp_stencil_plan P, int c, const double *pts, int phs, double *w,
+                           double *cond) {
+    StencilJob J{};
+    J.queue = P->words.p + 4 * c;
+    J.singular = (int *)(P->words.p + 4 * c + 1);
+    J.pts = pts;
+    J.offsets = P->offsets;
+    J.sizes = P->sizes;
+    J.list = P->list[c].p;
+    J.count = P->count[c];
+    J.dim = P->dim;
+    J.m = P->m;
+    J.phs = phs;
+    J.wb = w;
+    J.cond = cond;
+    return J;
+}
+
+extern "C" int mp_stencil_plan_run(mp_stencil_plan P, const double *pts, int phs_deg, double *w,
+                                   double *cond, mp_stream s) {
+    if (!P || !pts || !w)
+        return fail(MP_BAD_ARG, "mp_stencil_plan_run: null argument");
+    if (phs_deg != 3 && phs_deg != 5 && phs_deg != 7 && phs_deg != 9 && phs_deg != 11)
+        return fail(MP_BAD_ARG, "phs_deg should be 3, 5, 7, 9 or 11; got %d", phs_deg);
+    if (!is_device_ptr(pts) || !is_device_ptr(w) || (cond && !is_device_ptr(cond)))
+        return fail(MP_BAD_ARG, "mp_stencil_plan_run takes device arrays (mp_stencil_weights_"
+                                "batched stages host arrays)");
+    int m = 0;
+    MP_TRY(upload_exponents(P->dim, P->poly_deg, &m));
+    cudaStream_t st = S(s);
+    // classes not tuned yet are tuned first, on a sample of their own systems
+    for (int c = 0; c < GJ_CLASSES; c++)
+        if (P->count[c] >= 8 * sm_count() && g_gj_shape[c][P->dim - 2] < 0)
+            MP_TRY(gj_autotune(c, plan_job(P, c, pts, phs_deg, w, nullptr), 32 * sm_count(), st));
+    MP_CUDA(cudaMemsetAsync(P->words.p, 0, sizeof(unsigned int) * 4 * GJ_CLASSES, st));
+    MP_CUDA(cudaEventRecord(P->fork, st));
+    for (int c = 0; c < GJ_CLASSES; c++) {
+        if (!P->count[c])
+            continue;
+        cudaStream_t ss = P->side[c];
+        MP_CUDA(cudaStreamWaitEvent(ss, P->fork, 0));
+        const StencilJob J = plan_job(P, c, pts, phs_deg, w, cond);
+        MP_TRY(launch_class(c, J, ss));
+        if (cond)
+            MP_TRY(launch_cond(J, P->s_max, ss));
+        MP_CUDA(cudaEventRecord(P->join[c], ss));
+        MP_CUDA(cudaStreamWaitEvent(st, P->join[c], 0));
+    }
+    return MP_OK;
+}
+
+extern "C" int mp_stencil_plan_singular(mp_stencil_plan P, int *count, mp_stream s) {
+    if (!P || !count)
+        return fail(MP_BAD_ARG, "mp_stencil_plan_singular: null argument");
+    unsigned int words[4 * GJ_CLASSES];
+    MP_CUDA(cudaMemcpyAsync(words, P->words.p, sizeof(words), cudaMemcpyDeviceToHost, S(s)));
+    MP_CUDA(cudaStreamSynchronize(S(s)));
+    int n = 0;
+    for (int c = 0; c < GJ_CLASSES; c++)
+        n += (int)words[4 * c + 1];
+    *count = n;
+    return MP_OK;
+}
+
+extern "C" int mp_stencil_plan_info(mp_stencil_plan P, int *class_count, int *class_shape) {
+    if (!P)
+        return fail(MP_BAD_ARG, "mp_stencil_plan_info: null plan");
+    for (int c = 0; c < GJ_CLASSES; c++) {
+        if (class_count)
+            class_count[c] = P->count[c];
+        if (class_shape)
+            class_shape[c] = gj_groups[c][class_shape_of(c, P->dim)];
+    }
+    return MP_OK;
+}
+
+extern "C" int mp_stencil_plan_destroy(mp_stencil_plan P) {
+    delete P;
+    return MP_OK;
+}
+
 extern "C" int mp_stencil_weights_batched(int nsys, const int *sizes, const int64_t *offsets,
                                           const double *pts, int dim, int phs_deg, int poly_deg,
                                           double *w, double *cond, mp_stream s) {
@@ -802,116 +1167,32 @@ extern "C" int mp_stencil_weights_batched(int nsys, const int *sizes, const int6
         return fail(MP_BAD_ARG, "mp_stencil_weights_batched: bad arguments");
     if (phs_deg != 3 && phs_deg != 5 && phs_deg != 7 && phs_deg != 9 && phs_deg != 11)
         return fail(MP_BAD_ARG, "phs_deg should be 3, 5, 7, 9 or 11; got %d", phs_deg);
-    int m = 0;
-    MP_TRY(upload_exponents(dim, poly_deg, &m));
+    mp_stencil_plan P = nullptr;
+    MP_TRY(mp_stencil_plan_create(nsys, sizes, offsets, dim, poly_deg, &P));
+    std::unique_ptr<mp_stencil_plan_s> hold(P);
     const int R = dim + 1;
-    // size classes are chosen on the host
-    std::vector<int> hs(nsys);
-    std::vector<int64_t> ho(nsys);
-    MP_CUDA(cudaMemcpy(hs.data(), sizes, sizeof(int) * nsys, cudaMemcpyDefault));
-    MP_CUDA(cudaMemcpy(ho.data(), offsets, sizeof(int64_t) * nsys, cudaMemcpyDefault));
-    int64_t npts = 0;
-    int s_max = 0;
-    std::vector<int> lists[3];
-    for (int i = 0; i < nsys; i++) {
-        if (hs[i] < 2)
-            return fail(MP_BAD_ARG, "system %d has %d nodes", i, hs[i]);
-        int c = gj_class(hs[i] + m, R);
-        if (c < 0)
-            return fail(MP_BAD_ARG, "system %d: %d nodes + %d monomials exceeds %d", i, hs[i], m,
-                        MAX_S);
-        lists[c].push_back(i);
-        if (ho[i] + hs[i] > npts)
-            npts = ho[i] + hs[i];
-        if (hs[i] + m > s_max)
-            s_max = hs[i] + m;
-    }
-    dbuf<int> dsizes, dlist[3];
-    dbuf<int64_t> doff;
     dbuf<double> dpts, dw, dcond;
-    const int *psz = nullptr;
-    const int64_t *pof = nullptr;
     const double *ppts = nullptr;
-    MP_TRY(stage_in(sizes, nsys, dsizes, &psz, st));
-    MP_TRY(stage_in(offsets, nsys, doff, &pof, st));
-    MP_TRY(stage_in(pts, (size_t)npts * dim, dpts, &ppts, st));
+    MP_TRY(stage_in(pts, (size_t)P->npts * dim, dpts, &ppts, st));
     double *pw = w, *pc = cond;
     if (!is_device_ptr(w)) {
-        MP_TRY(dw.alloc((size_t)npts * R));
+        MP_TRY(dw.alloc((size_t)P->npts * R));
         pw = dw.p;
     }
     if (cond && !is_device_ptr(cond)) {
         MP_TRY(dcond.alloc(nsys));
         pc = dcond.p;
     }
-    // one persistent launch per size class, the classes run concurrently
-    cudaEvent_t ev_fork, ev_join[3];
-    cudaStream_t side[3];
-    MP_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-    MP_CUDA(cudaEventRecord(ev_fork, st));
-    StencilScratch scr[3];
-    int bad_total = 0;
-    int rc = MP_OK;
-    int nside = 0;
-    for (int c = 0; c < 3 && rc == MP_OK; c++) {
-        if (lists[c].empty())
-            continue;
-        MP_TRY(dlist[c].alloc(lists[c].size()));
-        MP_CUDA(cudaMemcpyAsync(dlist[c].p, lists[c].data(), sizeof(int) * lists[c].size(),
-                                cudaMemcpyHostToDevice, st));
-    }
-    MP_CUDA(cudaEventRecord(ev_fork, st));
-    for (int c = 0; c < 3; c++) {
-        if (lists[c].empty())
-            continue;
-        MP_CUDA(cudaStreamCreateWithFlags(&side[nside], cudaStreamNonBlocking));
-        MP_CUDA(cudaEventCreateWithFlags(&ev_join[nside], cudaEventDisableTiming));
-        cudaStream_t ss = side[nside];
-        MP_CUDA(cudaStreamWaitEvent(ss, ev_fork, 0));
-        StencilJob J{};
-        MP_TRY(scr[c].get(&J.queue, &J.singular));
-        MP_CUDA(cudaMemsetAsync(J.singular, 0, sizeof(int), ss));
-        J.pts = ppts;
-        J.offsets = pof;
-        J.sizes = psz;
-        J.list = dlist[c].p;
-        J.count = (int)lists[c].size();
-        J.dim = dim;
-        J.m = m;
-        J.phs = phs_deg;
-        J.wb = pw;
-        J.cond = pc;
-        rc = launch_class(c, J, ss);
-        if (rc == MP_OK && cond) {
-            StencilJob Jc = J;
-            rc = launch_cond(Jc, s_max, ss);
-        }
-        MP_CUDA(cudaEventRecord(ev_join[nside], ss));
-        MP_CUDA(cudaStreamWaitEvent(st, ev_join[nside], 0));
-        nside++;
-    }
-    for (int c = 0; c < 3; c++) {
-        if (lists[c].empty() || !scr[c].words.p)
-            continue;
-        int bad = 0;
-        MP_CUDA(cudaMemcpyAsync(&bad, scr[c].words.p + 4, sizeof(int), cudaMemcpyDeviceToHost, st));
-        MP_CUDA(cudaStreamSynchronize(st));
-        bad_total += bad;
-    }
+    MP_TRY(mp_stencil_plan_run(P, ppts, phs_deg, pw, pc, s));
+    int bad = 0;
+    MP_TRY(mp_stencil_plan_singular(P, &bad, s));
     if (dw.p)
-        MP_CUDA(cudaMemcpyAsync(w, dw.p, sizeof(double) * npts * R, cudaMemcpyDeviceToHost, st));
+        MP_CUDA(cudaMemcpyAsync(w, dw.p, sizeof(double) * P->npts * R, cudaMemcpyDeviceToHost, st));
     if (dcond.p)
         MP_CUDA(cudaMemcpyAsync(cond, dcond.p, sizeof(double) * nsys, cudaMemcpyDeviceToHost, st));
     MP_CUDA(cudaStreamSynchronize(st));
-    for (int i = 0; i < nside; i++) {
-        cudaStreamDestroy(side[i]);
-        cudaEventDestroy(ev_join[i]);
-    }
-    cudaEventDestroy(ev_fork);
-    if (rc != MP_OK)
-        return rc;
-    if (bad_total)
-        return fail(MP_SINGULAR_STENCIL, "%d stencil systems had a zero pivot", bad_total);
+    if (bad)
+        return fail(MP_SINGULAR_STENCIL, "%d stencil systems had a zero pivot", bad);
     return MP_OK;
 }
 

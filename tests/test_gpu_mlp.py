@@ -1,5 +1,6 @@
-"""GPU: the tensor-core network (tcgen05) against the numpy oracle, training,
-and what the learned initial guess gains in the pressure solve."""
+"""GPU: the tensor-core network (tcgen05 forward and backward) against the numpy
+oracle, training, the bounded completion waits, and what the learned initial guess
+gains in the pressure solve."""
 import numpy as np
 import pytest
 
@@ -35,6 +36,30 @@ def test_gradient_matches_oracle(net):
         a, b = g[o:o + n], go[o:o + n]
         assert np.linalg.norm(a - b) <= 1e-3 * np.linalg.norm(b) + 1e-7, name
         o += n
+
+
+def test_wait_limit_reports_timeout_and_recovers(mp_lib):
+    """Every tensor-core completion wait is bounded.  With a limit of 0 polls the
+    forward and the backward kernels give up at once and the call returns MP_TIMEOUT;
+    each kernel still waits (bounded) for the MMA it committed before it releases
+    tensor memory, so the same handle afterwards computes the oracle's values."""
+    rng = np.random.default_rng(6)
+    X = rng.normal(size=(300, 64)).astype(np.float32)
+    t = rng.normal(size=300).astype(np.float32)
+    m = meshless.MLP(seed=9)
+    L = capi.lib()
+    capi.check(L.mp_mlp_set_spin_limit(m.handle, 0))
+    for call in (lambda: m.forward(X), lambda: m.gradient(X, t)):
+        with pytest.raises(capi.MemphysError) as e:
+            call()
+        assert e.value.status == capi.MP_TIMEOUT
+    capi.check(L.mp_mlp_set_spin_limit(m.handle, 1 << 22))
+    yo, _ = omlp.forward(m.params(), X)
+    assert np.abs(m.forward(X) - yo).max() <= 1e-3 * max(1.0, np.abs(yo).max())
+    loss, g = m.gradient(X, t)
+    lo, go = omlp.loss_grad(m.params(), X, t)
+    assert loss == pytest.approx(lo, rel=1e-4)
+    assert np.linalg.norm(g - go) <= 1e-3 * np.linalg.norm(go)
 
 
 def test_training_reduces_loss(mp_lib):

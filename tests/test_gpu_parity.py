@@ -158,6 +158,52 @@ def test_batched_uneven_sizes_one_call(mp_lib):
         assert np.abs(a - b).max() <= 1e-8 * np.abs(b).max()
 
 
+def test_stencil_plan_runs_match_oracle(mp_lib):
+    """The plan form of the batched weights: classify once, run asynchronously twice
+    (the first run also tunes the CTA shape of every class with enough systems), on
+    device arrays; every system against the oracle's LAPACK-checked restatement."""
+    import ctypes as C
+    rng = np.random.default_rng(12)
+    sizes = rng.choice([20, 30, 40, 60], size=6000).astype(np.int32)
+    off = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    pts = []
+    for n in sizes:
+        d = rng.normal(size=(n, 2))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        d *= rng.uniform(0, 1, size=(n, 1)) ** 0.5
+        d[0] = 0
+        pts.append(d * rng.uniform(1e-3, 1e-2))
+    pts = np.ascontiguousarray(np.concatenate(pts))
+    L = capi.lib()
+    dsz, doff = capi.DeviceArray.from_host(sizes), capi.DeviceArray.from_host(off)
+    dpts, dw = capi.DeviceArray.from_host(pts), capi.DeviceArray((3 * int(sizes.sum()),))
+    plan = C.c_void_p()
+    capi.check(L.mp_stencil_plan_create(len(sizes), ptr(dsz), ptr(doff), 2, 3, C.byref(plan)))
+    try:
+        counts, shapes = (C.c_int * 7)(), (C.c_int * 7)()
+        capi.check(L.mp_stencil_plan_info(plan, counts, shapes))
+        # register widths 36 / 44 / 56 / 76 for n = 20 / 30 / 40 / 60 (m = 10, 3 rhs)
+        assert list(counts) == [int((sizes == 20).sum()), int((sizes == 30).sum()),
+                                int((sizes == 40).sum()), 0, int((sizes == 60).sum()), 0, 0]
+        ref, _, bad = oracle.batched_weights(sizes, off, pts, 2)
+        assert bad == 0
+        for _ in range(2):
+            dw.zero()
+            capi.check(L.mp_stencil_plan_run(plan, ptr(dpts), 3, ptr(dw), None, None))
+            nbad = C.c_int()
+            capi.check(L.mp_stencil_plan_singular(plan, C.byref(nbad), None))
+            assert nbad.value == 0
+            w = dw.to_host()
+            for n, o in zip(sizes, off):
+                a, b = w[3 * o:3 * (o + n)], ref[3 * o:3 * (o + n)]
+                assert np.abs(a - b).max() <= 1e-8 * np.abs(b).max()
+        capi.check(L.mp_stencil_plan_info(plan, counts, shapes))
+        print("systems per CTA after tuning:", list(shapes))
+        assert shapes[0] in (1, 2, 4, 8) and all(shapes[c] in (1, 2) for c in (1, 2, 4))
+    finally:
+        L.mp_stencil_plan_destroy(plan)
+
+
 @pytest.fixture(scope="module")
 def cav(mp_lib):
     cl = clouds.cavity_2d(48, seed=9)

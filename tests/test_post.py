@@ -72,6 +72,16 @@ class _CpuCloud:
         return self.ops[which]
 
 
+
+def test_max_l1_error_nan_and_empty_parts():
+    """general_functions.cpp:940-1032: `max_err < fabs(d)` skips NaN in the maximum, the
+    mean carries it, and a part without entries divides 0 by 0."""
+    a = np.array([0.0, 1.0, np.nan, 4.0])
+    m, l1 = post.calc_max_l1_error(a, np.zeros(4))
+    assert m == 4.0 and np.isnan(l1)
+    mb, lb, mi, li = post.calc_max_l1_error(np.ones(3), np.zeros(3), np.zeros(3, bool))
+    assert mb == 0.0 and np.isnan(lb) and mi == 1.0 and li == 1.0
+
 def test_error_and_residual_tables(tmp_path):
     import scipy.sparse as sp
     from memphys_b200 import capi

@@ -61,3 +61,28 @@ def test_noalloc_refuses_oversized_cloud_and_host_pointers(mp_lib):
     dn = capi.DeviceArray((cl.nv, 12), np.int32)
     capi.check(knn_noalloc(dx, db, dn, cl, 12), "mp_knn_stencils_noalloc")
     assert np.array_equal(dn.to_host(), knn_alloc(cl, 12))
+
+
+def test_noalloc_runs_with_the_device_memory_held(mp_lib):
+    """With all but a sliver of the device's free memory held by another allocation,
+    the no-allocation entry point still runs (a hidden cudaMalloc would fail there) and
+    leaves the free memory as it found it."""
+    import torch
+    cl = clouds.cavity_2d(96, seed=11)
+    ref = knn_alloc(cl, 20)
+    dx = capi.DeviceArray.from_host(np.ascontiguousarray(cl.xyz, np.float64))
+    db = capi.DeviceArray.from_host(np.ascontiguousarray(cl.boundary, np.uint8))
+    dn = capi.DeviceArray((cl.nv, 20), np.int32)
+    capi.check(knn_noalloc(dx, db, dn, cl, 20), "mp_knn_stencils_noalloc")  # kernels loaded
+    free0, _ = torch.cuda.mem_get_info()
+    hog = capi.DeviceArray((free0 - (48 << 20),), np.uint8)  # leave 48 MiB
+    try:
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 < (64 << 20)
+        for _ in range(2):
+            dn.zero()
+            capi.check(knn_noalloc(dx, db, dn, cl, 20), "mp_knn_stencils_noalloc")
+            assert np.array_equal(dn.to_host(), ref)
+        assert torch.cuda.mem_get_info()[0] == free1
+    finally:
+        hog.free()
