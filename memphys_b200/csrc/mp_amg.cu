@@ -835,10 +835,22 @@ template <class T> struct V2a;
 template <> struct V2a<double> { using type = double2; };
 template <> struct V2a<float> { using type = float2; };
 
+// Operator loads.  EVF (evict first): the finest level's operators and transfers
+// stream through L2 once per use (273 MB at 1M nodes, twice the L2), so their lines
+// go first and leave the coarse levels resident; a coarse level's operator is read
+// four times in a row inside one cycle (two smoothing steps and the residual on each
+// side) and is loaded with the default policy so that its repeats hit in L2.
+template <bool EVF, class P> __device__ __forceinline__ P ldop(const P *p) {
+    if constexpr (EVF)
+        return __ldcs(p);
+    else
+        return __ldg(p);
+}
+
 // Two rows of (M u): T is the vector type, V the stored value type.  With DIFF
 // the first entry of each row is the self entry holding the row sum, and the
 // others multiply (u_j - u_i): a = s_i u_i + sum_k a_ik (u_k - u_i).
-template <class T, class V, bool DIFF>
+template <class T, class V, bool DIFF, bool EVF>
 __device__ __forceinline__ void spmv_pair(const EllView<V> &A, int w, int lane,
                                           const T *__restrict__ x, T &a0, T &a1) {
     using V2 = typename V2a<V>::type;
@@ -857,14 +869,14 @@ __device__ __forceinline__ void spmv_pair(const EllView<V> &A, int w, int lane,
                 const int i0 = w * SLICE + 2 * lane;
                 s0 = i0 < A.nrows ? __ldg(x + i0) : T(0);
                 s1 = i0 + 1 < A.nrows ? __ldg(x + i0 + 1) : T(0);
-                const int4 e = __ldcs(P);
+                const int4 e = ldop<EVF>(P);
                 a0 = (T)__int_as_float(e.y) * s0;
                 a1 = (T)__int_as_float(e.w) * s1;
                 k0 = 1;
             }
 #pragma unroll 4
             for (int k = k0; k < K; k++) {
-                const int4 e = __ldcs(P + (size_t)k * (SLICE / 2));
+                const int4 e = ldop<EVF>(P + (size_t)k * (SLICE / 2));
                 const T g0 = __ldg(x + e.x), g1 = __ldg(x + e.z);
                 a0 = fma((T)__int_as_float(e.y), DIFF ? g0 - s0 : g0, a0);
                 a1 = fma((T)__int_as_float(e.w), DIFF ? g1 - s1 : g1, a1);
@@ -876,7 +888,7 @@ __device__ __forceinline__ void spmv_pair(const EllView<V> &A, int w, int lane,
         const int i0 = w * SLICE + 2 * lane;
         s0 = i0 < A.nrows ? __ldg(x + i0) : T(0);
         s1 = i0 + 1 < A.nrows ? __ldg(x + i0 + 1) : T(0);
-        const V2 v = __ldcs(reinterpret_cast<const V2 *>(A.vals + base));
+        const V2 v = ldop<EVF>(reinterpret_cast<const V2 *>(A.vals + base));
         a0 = (T)v.x * s0;
         a1 = (T)v.y * s1;
         k0 = 1;
@@ -884,8 +896,8 @@ __device__ __forceinline__ void spmv_pair(const EllView<V> &A, int w, int lane,
 #pragma unroll 4
     for (int k = k0; k < K; k++) {
         const size_t o = base + (size_t)k * SLICE;
-        const int2 c = __ldcs(reinterpret_cast<const int2 *>(A.cols + o));
-        const V2 v = __ldcs(reinterpret_cast<const V2 *>(A.vals + o));
+        const int2 c = ldop<EVF>(reinterpret_cast<const int2 *>(A.cols + o));
+        const V2 v = ldop<EVF>(reinterpret_cast<const V2 *>(A.vals + o));
         const T x0 = __ldg(x + c.x), x1 = __ldg(x + c.y);
         a0 = fma((T)v.x, DIFF ? x0 - s0 : x0, a0);
         a1 = fma((T)v.y, DIFF ? x1 - s1 : x1, a1);
@@ -895,7 +907,7 @@ __device__ __forceinline__ void spmv_pair(const EllView<V> &A, int w, int lane,
 __device__ __forceinline__ int gwarp_a() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
 
 // Epilogue kinds of the fused level kernels
-enum { EP_CHEB_PRE = 0, EP_RESID, EP_PLAIN, EP_PROLONG, EP_CHEB_POST1, EP_CHEB_POST2 };
+enum { EP_CHEB_PRE = 0, EP_RESID, EP_PLAIN, EP_PROLONG, EP_CHEB_POST1, EP_CHEB_POST2, EP_RESTRICT };
 
 struct ChebC {
     double inv_theta, theta, c1, c2, c3, c4;
@@ -915,6 +927,9 @@ template <class V> struct CsrView {
 //   EP_PROLONG   : x = x + M u                              (M = P, u = coarse x)
 //   EP_CHEB_POST1: d = dinv (b - M x) / theta               (u = x)
 //   EP_CHEB_POST2: x = x + (1 + c3) d + c4 (theta d - dinv M d)   (u = d)
+//   EP_RESTRICT  : y = M u, d = dinv y / theta               (M = R; y, d, dinv and
+//                  theta of the coarser level: the first step of its pre-smoother
+//                  from a zero guess, written with its right-hand side)
 // No kernel writes the vector it gathers.
 template <class T, int EP>
 __device__ __forceinline__ void level_epilogue(int i, T a, const T *b, const T *dinv, T *d, T *x,
@@ -929,6 +944,9 @@ __device__ __forceinline__ void level_epilogue(int i, T a, const T *b, const T *
         x[i] = x[i] + a;
     } else if (EP == EP_CHEB_POST1) {
         d[i] = dinv[i] * (b[i] - a) * (T)c.inv_theta;
+    } else if (EP == EP_RESTRICT) {
+        y[i] = a;
+        d[i] = dinv[i] * a * (T)c.inv_theta;
     } else {
         const T di = d[i];
         x[i] = x[i] + (T)(1.0 + c.c3) * di + (T)c.c4 * ((T)c.theta * di - dinv[i] * a);
@@ -939,7 +957,7 @@ __device__ __forceinline__ void level_epilogue(int i, T a, const T *b, const T *
 // (8 blocks of 256 per SM): these kernels wait on memory, and occupancy is what
 // keeps enough loads in flight (at 48 registers the FP32 form ran at 53 % warps
 // active and 60 % of DRAM bandwidth)
-template <class T, class V, bool DIFF, int EP>
+template <class T, class V, bool DIFF, bool EVF, int EP>
 __global__ void __launch_bounds__(256, 8)
     k_level(EllView<V> M, const T *__restrict__ u, const T *__restrict__ b,
             const T *__restrict__ dinv, T *d, T *x, T *y, ChebC c, const int *done) {
@@ -951,7 +969,7 @@ __global__ void __launch_bounds__(256, 8)
     if (w >= (M.nrows + SLICE - 1) / SLICE)
         return;
     T a[2];
-    spmv_pair<T, V, DIFF>(M, w, lane, u, a[0], a[1]);
+    spmv_pair<T, V, DIFF, EVF>(M, w, lane, u, a[0], a[1]);
     const int i0 = w * SLICE + 2 * lane;
 #pragma unroll
     for (int q = 0; q < 2; q++)
@@ -961,7 +979,7 @@ __global__ void __launch_bounds__(256, 8)
 
 // CSR: G lanes per row, partial sums combined with shuffles inside the group
 // (DIFF: the row's first entry is its self entry, see spmv_pair)
-template <class T, class V, int G, bool DIFF, int EP>
+template <class T, class V, int G, bool DIFF, bool EVF, int EP>
 __global__ void __launch_bounds__(256)
     k_level_csr(CsrView<V> M, const T *__restrict__ u, const T *__restrict__ b,
                 const T *__restrict__ dinv, T *d, T *x, T *y, ChebC c, const int *done) {
@@ -978,15 +996,15 @@ __global__ void __launch_bounds__(256)
         if (M.pk) {  // (column, FP32 value) pairs: one 8-byte load per entry
 #pragma unroll 4
             for (int t = b0 + li; t < e; t += G) {
-                const int2 q = __ldcs(M.pk + t);
+                const int2 q = ldop<EVF>(M.pk + t);
                 const T ut = __ldg(u + q.x);
                 acc = fma((T)__int_as_float(q.y), (DIFF && t != b0) ? ut - ui : ut, acc);
             }
         } else {
 #pragma unroll 4
             for (int t = b0 + li; t < e; t += G) {
-                const T ut = __ldg(u + __ldcs(M.ci + t));
-                acc = fma((T)__ldcs(M.v + t), (DIFF && t != b0) ? ut - ui : ut, acc);
+                const T ut = __ldg(u + ldop<EVF>(M.ci + t));
+                acc = fma((T)ldop<EVF>(M.v + t), (DIFF && t != b0) ? ut - ui : ut, acc);
             }
         }
     }
@@ -1091,7 +1109,7 @@ template <> struct LvlOps<float, true> : LvlOps<float, false> {
 static unsigned sblocks(int n) { return (unsigned)(((n + SLICE - 1) / SLICE + 7) / 8); }
 
 // launch one fused level operation with the operator's tuned schedule
-template <class T, class V, bool DIFF, int EP>
+template <class T, class V, bool DIFF, int EP, bool EVF = false>
 static int level_op(int mode, const EllView<V> &E, const CsrView<V> &Cv, const T *u, const T *b,
                     const T *dinv, T *d, T *x, T *y, const ChebC &c, const int *done,
                     cudaStream_t s) {
@@ -1099,11 +1117,11 @@ static int level_op(int mode, const EllView<V> &E, const CsrView<V> &Cv, const T
     const dim3 blk(256);
     cudaError_t e;
     switch (mode) {
-    case 0: e = launch_pdl(k_level<T, V, DIFF, EP>, dim3(sblocks(n)), blk, s, E, u, b, dinv, d, x, y, c, done); break;
-    case 1: e = launch_pdl(k_level_csr<T, V, 4, DIFF, EP>, dim3((unsigned)((n * 4 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
-    case 2: e = launch_pdl(k_level_csr<T, V, 8, DIFF, EP>, dim3((unsigned)((n * 8 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
-    case 3: e = launch_pdl(k_level_csr<T, V, 16, DIFF, EP>, dim3((unsigned)((n * 16 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
-    default: e = launch_pdl(k_level_csr<T, V, 32, DIFF, EP>, dim3((unsigned)(((size_t)n * 32 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
+    case 0: e = launch_pdl(k_level<T, V, DIFF, EVF, EP>, dim3(sblocks(n)), blk, s, E, u, b, dinv, d, x, y, c, done); break;
+    case 1: e = launch_pdl(k_level_csr<T, V, 4, DIFF, EVF, EP>, dim3((unsigned)((n * 4 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
+    case 2: e = launch_pdl(k_level_csr<T, V, 8, DIFF, EVF, EP>, dim3((unsigned)((n * 8 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
+    case 3: e = launch_pdl(k_level_csr<T, V, 16, DIFF, EVF, EP>, dim3((unsigned)((n * 16 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
+    default: e = launch_pdl(k_level_csr<T, V, 32, DIFF, EVF, EP>, dim3((unsigned)(((size_t)n * 32 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
     }
     if (e != cudaSuccess)
         return fail(MP_CUDA_ERROR, "multigrid launch: %s", cudaGetErrorString(e));
@@ -1111,9 +1129,24 @@ static int level_op(int mode, const EllView<V> &E, const CsrView<V> &Cv, const T
     return MP_OK;
 }
 
-// V(1,1) cycle from level l: T vectors, V stored values, DIFF level operators
+// level_op with the load policy of level l (evict first on the finest level)
+template <class T, class V, bool DIFF, int EP>
+static int level_op_at(size_t l, int mode, const EllView<V> &E, const CsrView<V> &Cv, const T *u,
+                       const T *b, const T *dinv, T *d, T *x, T *y, const ChebC &c,
+                       const int *done, cudaStream_t s) {
+    if (l == 0)
+        return level_op<T, V, DIFF, EP, true>(mode, E, Cv, u, b, dinv, d, x, y, c, done, s);
+    return level_op<T, V, DIFF, EP, false>(mode, E, Cv, u, b, dinv, d, x, y, c, done, s);
+}
+
+// V(1,1) cycle from level l: T vectors, V stored values, DIFF level operators.
+// head_ready: d = dinv b / theta, the first step of the pre-smoother from a zero
+// guess, was written by whoever wrote b (the coarser levels' by the restriction
+// epilogue; level 0's by the Krylov update that produced the preconditioner input,
+// see amg_head), otherwise a kernel forms it here.
 template <class T, class V, bool DIFF>
-static int vcycle(const Amg &a, size_t l, const T *b, T *x, const int *done, cudaStream_t s) {
+static int vcycle(const Amg &a, size_t l, const T *b, T *x, const int *done, bool head_ready,
+                  cudaStream_t s) {
     using LV = LvlVec<T>;
     using LO = LvlOps<V, DIFF>;
     AmgLevel &L = *a.L[l];
@@ -1132,43 +1165,73 @@ static int vcycle(const Amg &a, size_t l, const T *b, T *x, const int *done, cud
     const CsrView<V> Ac = LO::Ac(L), Pc = LO::Pc(L), Rc = LO::Rc(L);
     const T *dinv = LV::dinv(L);
     T *d = LV::d(L), *r = LV::r(L);
-    const unsigned vb = (unsigned)std::min((L.n + 255) / 256, sm_count() * 8);
     const int mA = l == 0 ? 0 : L.sA.mode;
-    const cudaError_t e = launch_pdl(k_cheb_start<T>, dim3(vb), dim3(256), s, L.n, b, dinv, d,
-                                     (T)c.inv_theta, done);
-    if (e != cudaSuccess)
-        return fail(MP_CUDA_ERROR, "multigrid launch: %s", cudaGetErrorString(e));
-    MP_CHECK_LAUNCH();
-    MP_TRY((level_op<T, V, DIFF, EP_CHEB_PRE>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
-    for (int k = 1; k < a.sweeps; k++) {  // further pre-smoothing from the current x
-        MP_TRY((level_op<T, V, DIFF, EP_CHEB_POST1>(mA, A, Ac, x, b, dinv, d, x, nullptr, c, done, s)));
-        MP_TRY((level_op<T, V, DIFF, EP_CHEB_POST2>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
+    if (!head_ready) {
+        const unsigned vb = (unsigned)std::min((L.n + 255) / 256, sm_count() * 8);
+        const cudaError_t e = launch_pdl(k_cheb_start<T>, dim3(vb), dim3(256), s, L.n, b, dinv, d,
+                                         (T)c.inv_theta, done);
+        if (e != cudaSuccess)
+            return fail(MP_CUDA_ERROR, "multigrid launch: %s", cudaGetErrorString(e));
+        MP_CHECK_LAUNCH();
     }
-    MP_TRY((level_op<T, V, DIFF, EP_RESID>(mA, A, Ac, x, b, dinv, d, x, r, c, done, s)));
-    MP_TRY((level_op<T, V, false, EP_PLAIN>(L.sR.mode, LO::R(L), Rc, r, nullptr, nullptr, nullptr,
-                                            nullptr, LV::b(N), c, done, s)));
-    MP_TRY((vcycle<T, V, DIFF>(a, l + 1, LV::b(N), LV::x(N), done, s)));
-    MP_TRY((level_op<T, V, false, EP_PROLONG>(L.sP.mode, LO::P(L), Pc, LV::x(N), nullptr, nullptr,
-                                              nullptr, x, nullptr, c, done, s)));
+    MP_TRY((level_op_at<T, V, DIFF, EP_CHEB_PRE>(l, mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
+    for (int k = 1; k < a.sweeps; k++) {  // further pre-smoothing from the current x
+        MP_TRY((level_op_at<T, V, DIFF, EP_CHEB_POST1>(l, mA, A, Ac, x, b, dinv, d, x, nullptr, c, done, s)));
+        MP_TRY((level_op_at<T, V, DIFF, EP_CHEB_POST2>(l, mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
+    }
+    MP_TRY((level_op_at<T, V, DIFF, EP_RESID>(l, mA, A, Ac, x, b, dinv, d, x, r, c, done, s)));
+    // restriction; unless the next level is the coarsest (a direct solve), it also
+    // starts that level's pre-smoother
+    const bool next_smooths = l + 2 < a.L.size();
+    if (next_smooths) {
+        const ChebC cn = cheb_consts(N.lmax, a.cheb_ratio);
+        MP_TRY((level_op_at<T, V, false, EP_RESTRICT>(l, L.sR.mode, LO::R(L), Rc, r, nullptr,
+                                                      LV::dinv(N), LV::d(N), nullptr, LV::b(N),
+                                                      cn, done, s)));
+    } else {
+        MP_TRY((level_op_at<T, V, false, EP_PLAIN>(l, L.sR.mode, LO::R(L), Rc, r, nullptr, nullptr,
+                                                   nullptr, nullptr, LV::b(N), c, done, s)));
+    }
+    MP_TRY((vcycle<T, V, DIFF>(a, l + 1, LV::b(N), LV::x(N), done, next_smooths, s)));
+    MP_TRY((level_op_at<T, V, false, EP_PROLONG>(l, L.sP.mode, LO::P(L), Pc, LV::x(N), nullptr,
+                                                 nullptr, nullptr, x, nullptr, c, done, s)));
     for (int k = 0; k < a.sweeps; k++) {
-        MP_TRY((level_op<T, V, DIFF, EP_CHEB_POST1>(mA, A, Ac, x, b, dinv, d, x, nullptr, c, done, s)));
-        MP_TRY((level_op<T, V, DIFF, EP_CHEB_POST2>(mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
+        MP_TRY((level_op_at<T, V, DIFF, EP_CHEB_POST1>(l, mA, A, Ac, x, b, dinv, d, x, nullptr, c, done, s)));
+        MP_TRY((level_op_at<T, V, DIFF, EP_CHEB_POST2>(l, mA, A, Ac, d, b, dinv, d, x, nullptr, c, done, s)));
     }
     return MP_OK;
 }
 
 template <class T>
-int amg_apply(const Amg &a, const T *in, T *out, const int *done, cudaStream_t s) {
+int amg_apply(const Amg &a, const T *in, T *out, const int *done, cudaStream_t s,
+              bool head_ready) {
+    if (a.L.size() < 2)
+        head_ready = false;
     if constexpr (std::is_same<T, double>::value) {
         if (a.store == AMG_MG32)
-            return vcycle<double, float, true>(a, 0, in, out, done, s);
-        return vcycle<double, double, false>(a, 0, in, out, done, s);
+            return vcycle<double, float, true>(a, 0, in, out, done, head_ready, s);
+        return vcycle<double, double, false>(a, 0, in, out, done, head_ready, s);
     } else {
-        return vcycle<float, float, true>(a, 0, in, out, done, s);
+        return vcycle<float, float, true>(a, 0, in, out, done, head_ready, s);
     }
 }
-template int amg_apply<double>(const Amg &, const double *, double *, const int *, cudaStream_t);
-template int amg_apply<float>(const Amg &, const float *, float *, const int *, cudaStream_t);
+template int amg_apply<double>(const Amg &, const double *, double *, const int *, cudaStream_t,
+                               bool);
+template int amg_apply<float>(const Amg &, const float *, float *, const int *, cudaStream_t,
+                              bool);
+
+template <class T> AmgHead<T> amg_head(const Amg &a) {
+    AmgHead<T> h{};
+    if (a.L.size() < 2)
+        return h;
+    const AmgLevel &L = *a.L[0];
+    h.d = LvlVec<T>::d(const_cast<AmgLevel &>(L));
+    h.dinv = LvlVec<T>::dinv(L);
+    h.inv_theta = (T)cheb_consts(L.lmax, a.cheb_ratio).inv_theta;
+    return h;
+}
+template AmgHead<double> amg_head<double>(const Amg &);
+template AmgHead<float> amg_head<float>(const Amg &);
 
 // ------------------------------------------------------- field filter
 __global__ void k_filter_scale(int n, double *s) {
@@ -1201,7 +1264,7 @@ int amg_filter_setup(const Amg &a, double *scale1, cudaStream_t s) {
     MP_CHECK_LAUNCH();
     const ChebC c{};
     const CsrView<double> Rc{L.Rc.n, L.Rc.rp.p, L.Rc.ci.p, L.Rc.v64.p};
-    MP_TRY((level_op<double, double, false, EP_PLAIN>(L.sR.mode, L.R.view64(), Rc, ones.p, nullptr,
+    MP_TRY((level_op<double, double, false, EP_PLAIN, true>(L.sR.mode, L.R.view64(), Rc, ones.p, nullptr,
                                                       nullptr, nullptr, nullptr, scale1, c,
                                                       a.zero_flag.p, s)));
     const int n1 = a.L[1]->n;
@@ -1219,13 +1282,13 @@ int amg_filter(const Amg &a, const double *c, double *work1, const double *scale
     const ChebC k{};
     const CsrView<double> Rc{L.Rc.n, L.Rc.rp.p, L.Rc.ci.p, L.Rc.v64.p};
     const CsrView<double> Pc{L.Pc.n, L.Pc.rp.p, L.Pc.ci.p, L.Pc.v64.p};
-    MP_TRY((level_op<double, double, false, EP_PLAIN>(L.sR.mode, L.R.view64(), Rc, c, nullptr,
+    MP_TRY((level_op<double, double, false, EP_PLAIN, true>(L.sR.mode, L.R.view64(), Rc, c, nullptr,
                                                       nullptr, nullptr, nullptr, work1, k,
                                                       a.zero_flag.p, s)));
     const int n1 = a.L[1]->n;
     k_scale_vec<<<(n1 + 255) / 256, 256, 0, s>>>(n1, scale1, work1);
     MP_CHECK_LAUNCH();
-    MP_TRY((level_op<double, double, false, EP_PLAIN>(L.sP.mode, L.P.view64(), Pc, work1, nullptr,
+    MP_TRY((level_op<double, double, false, EP_PLAIN, true>(L.sP.mode, L.P.view64(), Pc, work1, nullptr,
                                                       nullptr, nullptr, nullptr, out, k,
                                                       a.zero_flag.p, s)));
     return MP_OK;
@@ -1240,7 +1303,7 @@ int amg_filter(const Amg &a, const double *c, double *work1, const double *scale
 // traffic evicts a coarse operator between its uses; an operator timed warm
 // from L2 ranks the schedules differently.  The median of five launches decides.
 template <class T, class V, bool DIFF>
-static int tune_one(const EllView<V> &E, const CsrView<V> &Cv, int ncols, bool allow_sell,
+static int tune_one(size_t l, const EllView<V> &E, const CsrView<V> &Cv, int ncols, bool allow_sell,
                     OpSched &out, const int *zero, dbuf<char> &flush, cudaStream_t s) {
     const int n = Cv.nrows;
     if (!n) {
@@ -1264,7 +1327,7 @@ static int tune_one(const EllView<V> &E, const CsrView<V> &Cv, int ncols, bool a
         for (int rep = 0; rep < REPS && rc == MP_OK; rep++) {
             cudaMemsetAsync(flush.p, rep & 0xff, flush.n, s);
             cudaEventRecord(e0, s);
-            rc = level_op<T, V, DIFF, EP_PLAIN>(mode, E, Cv, u.p, nullptr, nullptr, nullptr,
+            rc = level_op_at<T, V, DIFF, EP_PLAIN>(l, mode, E, Cv, u.p, nullptr, nullptr, nullptr,
                                                 nullptr, y.p, c, zero, s);
             cudaEventRecord(e1, s);
             cudaEventSynchronize(e1);
@@ -1324,9 +1387,9 @@ template <class T, class V, bool DIFF> static int tune_levels(Amg &a, cudaStream
         if (!flush.p)
             MP_TRY(flush.alloc((size_t)192 << 20));
         if (l > 0)
-            MP_TRY((tune_one<T, V, DIFF>(LO::A(L), LO::Ac(L), L.n, true, L.sA, z, flush, s)));
-        MP_TRY((tune_one<T, V, false>(LT::P(L), LT::Pc(L), a.L[l + 1]->n, true, L.sP, z, flush, s)));
-        MP_TRY((tune_one<T, V, false>(LT::R(L), LT::Rc(L), L.n, true, L.sR, z, flush, s)));
+            MP_TRY((tune_one<T, V, DIFF>(l, LO::A(L), LO::Ac(L), L.n, true, L.sA, z, flush, s)));
+        MP_TRY((tune_one<T, V, false>(l, LT::P(L), LT::Pc(L), a.L[l + 1]->n, true, L.sP, z, flush, s)));
+        MP_TRY((tune_one<T, V, false>(l, LT::R(L), LT::Rc(L), L.n, true, L.sR, z, flush, s)));
         g_tuned[key] = TuneVal{L.sA, L.sP, L.sR};
     }
     return MP_OK;

@@ -103,7 +103,22 @@ void amg_destroy(Amg *a);
 // the inverse on the first n0 entries alone maps every vector to zero mean and the
 // preconditioned system would lose its border row.  FP64 vectors use
 // the FP32 difference-form operators when the hierarchy was built with AMG_MG32.
+// head_ready: the caller has already written the level-0 head (see AmgHead) for
+// `in`; ignored for a one-level hierarchy.
 template <class T>
-int amg_apply(const Amg &a, const T *in, T *out, const int *done, cudaStream_t s);
+int amg_apply(const Amg &a, const T *in, T *out, const int *done, cudaStream_t s,
+              bool head_ready = false);
+
+// The first step of the finest level's pre-smoother from a zero guess,
+// d[i] = dinv[i] * in[i] * inv_theta, which the kernel that writes the
+// preconditioner's input can write alongside it (amg_apply with head_ready = true
+// then skips that pass).  d == nullptr for a one-level hierarchy (the cycle is
+// then a direct solve).
+template <class T> struct AmgHead {
+    T *d;
+    const T *dinv;
+    T inv_theta;
+};
+template <class T> AmgHead<T> amg_head(const Amg &a);
 
 }  // namespace mp

@@ -268,11 +268,12 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
     }
 }
 
-// p = r + beta (p - omega v); y = M^-1 p for the fused preconditioners
+// p = r + beta (p - omega v); y = M^-1 p for the fused preconditioners; for the
+// multigrid (H.d set) also the head of its cycle, H.d = H.dinv p / theta
 template <class T, int PK>
 __global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_update_p(int nv, int bordered, const T *r, T *p, const T *v, T *y, const T *dinv,
-               const BicgScalars *S) {
+               const BicgScalars *S, AmgHead<T> H) {
     if (S->done)
         return;
     const double beta = (S->rho / S->rho_old) * (S->alpha / S->omega);
@@ -283,6 +284,8 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
         p[i] = pi;
         if (PK == PK_JACOBI)
             y[i] = dinv[i] * pi;
+        if (PK == PK_EXTERNAL && H.d)
+            H.d[i] = H.dinv[i] * pi * H.inv_theta;
     }
     if (bordered && blockIdx.x == 0 && threadIdx.x == 0) {
         const T pi = r[nv] + bt * (p[nv] - om * v[nv]);
@@ -339,7 +342,7 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
 template <class T, int PK>
 __global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_update_s(int nv, int bordered, const T *r, const T *v, T *s, T *z, const T *dinv, T *x,
-               const T *y, BicgScalars *S, RedBuf R, cudaGraphConditionalHandle h) {
+               const T *y, BicgScalars *S, RedBuf R, cudaGraphConditionalHandle h, AmgHead<T> H) {
     KRYLOV_SMEM
     if (S->done)
         return;
@@ -351,6 +354,8 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
         s[i] = si;
         if (PK == PK_JACOBI)
             z[i] = dinv[i] * si;
+        if (PK == PK_EXTERNAL && H.d)
+            H.d[i] = H.dinv[i] * si * H.inv_theta;
         x[i] = x[i] + al * y[i];
         acc[0] += (double)si * si;
     }
@@ -650,31 +655,34 @@ static int issue_iteration(const PpeSystem &P, const EllView<T> &A, const T *din
     const int nv = P.nv, nsys = P.nsys, bd = P.bordered;
     T *yy = pk == PK_NONE ? p : y;
     T *zz = pk == PK_NONE ? s_ : z;
+    // the multigrid's first smoothing pass is fused into the updates that write its input
+    const AmgHead<T> H = pk == PK_EXTERNAL ? amg_head<T>(*P.amg) : AmgHead<T>{};
+    const bool head = H.d != nullptr;
     k_restart<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, x, b, r, r0, S, R);
     MP_CHECK_LAUNCH();
     if (pk == PK_JACOBI)
-        k_update_p<T, PK_JACOBI><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S);
+        k_update_p<T, PK_JACOBI><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S, H);
     else if (pk == PK_NONE)
-        k_update_p<T, PK_NONE><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S);
+        k_update_p<T, PK_NONE><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S, H);
     else
-        k_update_p<T, PK_EXTERNAL><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S);
+        k_update_p<T, PK_EXTERNAL><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S, H);
     MP_CHECK_LAUNCH();
     if (pk == PK_EXTERNAL)
-        MP_TRY(amg_apply<T>(*P.amg, p, yy, &S->done, st));
+        MP_TRY(amg_apply<T>(*P.amg, p, yy, &S->done, st, head));
     k_spmv_alpha<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, yy, v, r0, S, R);
     MP_CHECK_LAUNCH();
     if (pk == PK_JACOBI)
         k_update_s<T, PK_JACOBI><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, x, yy,
-                                                                S, R, h);
+                                                                S, R, h, H);
     else if (pk == PK_NONE)
         k_update_s<T, PK_NONE><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, x, yy, S,
-                                                              R, h);
+                                                              R, h, H);
     else
         k_update_s<T, PK_EXTERNAL><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, x,
-                                                                  yy, S, R, h);
+                                                                  yy, S, R, h, H);
     MP_CHECK_LAUNCH();
     if (pk == PK_EXTERNAL)
-        MP_TRY(amg_apply<T>(*P.amg, s_, zz, &S->done, st));
+        MP_TRY(amg_apply<T>(*P.amg, s_, zz, &S->done, st, head));
     k_spmv_omega<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, zz, t, s_, S, R);
     MP_CHECK_LAUNCH();
     k_update_xr<T><<<vec_blocks(nsys), KT, 0, st>>>(nsys, x, zz, s_, t, r, r0, S, R, h);
