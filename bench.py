@@ -96,6 +96,8 @@ def parse():
     ap.add_argument("--no-cube", action="store_true",
                     help="skip the 3D mixed-precision cube (2,195,456 nodes)")
     ap.add_argument("--cube-n", type=int, default=128)
+    ap.add_argument("--integrator-steps", type=int, default=3,
+                    help="timed steps of each other time integrator at the headline size (0: skip)")
     ap.add_argument("--cube-spinup", type=int, default=10)
     ap.add_argument("--no-channel", action="store_true",
                     help="skip the learned-guess channel (1,004,010 nodes)")
@@ -104,9 +106,11 @@ def parse():
     ap.add_argument("--channel-samples", type=int, default=4096)
     ap.add_argument("--inner-tol", type=float, default=1e-3,
                     help="mixed precision: relative reduction of each FP32 refinement solve")
-    ap.add_argument("--profile", default=None, choices=["steps", "spmv", "stencil"],
+    ap.add_argument("--profile", default=None,
+                    choices=["steps", "spmv", "stencil", "cloud", "sis", "fsf", "train"],
                     help="set up, warm up, then run `--steps` steps (SpMV launches, stencil-weight "
-                         "computations) inside a profiler capture range and exit (for ncu "
+                         "computations, cloud builds, semi-implicit or Fourier-z steps, training "
+                         "epochs) inside a profiler capture range and exit (for ncu "
                          "--profile-from-start off)")
     ap.add_argument("--variant", default="plain",
                     choices=["plain", "mg32", "extrapolated_mg32", "projected_mg32",
@@ -152,30 +156,56 @@ def max_over_ranks(pg, v: float) -> float:
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region.
+
+    The sampler starts before the region and the region starts only once its first
+    sample is written; the samples counted are those written between the region's
+    start and end (every 50 ms).  A region shorter than the interval keeps the first
+    sample after it and says so (`after_region`)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    INTERVAL_MS = 50
 
     def __init__(self, index: int):
         self.index = index
         self.p = None
         self.path = os.path.join(tempfile.gettempdir(), f"memphys_clocks_{os.getpid()}_{index}.csv")
+        self.n0 = self.n1 = 0
+        self.after = False
+
+    def _lines(self):
+        try:
+            with open(self.path) as f:
+                return [ln for ln in f if ln.count(",") >= 8]
+        except OSError:
+            return []
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits",
+                                       "-lms", str(self.INTERVAL_MS)],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
+            t_end = time.time() + 5.0
+            while not self._lines() and time.time() < t_end and self.p.poll() is None:
+                time.sleep(0.01)
+            self.n0 = len(self._lines())
         except Exception:
             self.p = None
         return self
 
     def __exit__(self, *exc):
         if self.p is not None:
+            self.n1 = len(self._lines())
+            if self.n1 <= self.n0:  # region shorter than the interval: the next sample
+                t_end = time.time() + 1.0
+                while len(self._lines()) <= self.n0 and time.time() < t_end:
+                    time.sleep(0.005)
+                self.n1 = min(len(self._lines()), self.n0 + 1)
+                self.after = True
             self.p.send_signal(signal.SIGTERM)
             try:
                 self.p.wait(timeout=5)
@@ -185,21 +215,25 @@ class Clocks:
         return False
 
     def summary(self):
-        if self.p is None or not os.path.exists(self.path):
+        if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        rows = []
-        for ln in open(self.path):
-            parts = [x.strip() for x in ln.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
+        rows = [[x.strip() for x in ln.split(",")] for ln in self._lines()[self.n0:self.n1]]
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+        out = {"sm_mhz": float(np.median(sm)) if sm else None,
+               "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows),
+               "interval_ms": self.INTERVAL_MS}
+        if self.after:
+            out["after_region"] = True
+        return out
 
 
 def measured_peak():
@@ -250,7 +284,7 @@ def run_ours(args, ws, rank, local, pg):
     ns = fs.system_size
     p0 = np.zeros(ns)
     if args.profile:
-        return profile_range(args, cl, cld, make, fs, vel0, p0, stream)
+        return profile_range(args, cl, cld, make, fs, vel0, p0, stream, pts, prm)
     import ctypes as C
 
     # headline: plain FP64 from rest, `--warmup` untimed steps, `--steps` timed steps
@@ -435,6 +469,8 @@ def run_ours(args, ws, rank, local, pg):
         legs.append(("cube3d_mixed", lambda: cube_mixed(args, stream)))
     if ws == 1 and not args.no_channel:
         legs.append(("channel_learned", lambda: channel_learned(args, stream)))
+    if ws == 1 and args.integrator_steps > 0:
+        legs.append(("integrators", lambda: integrators(args, cl, cld, prm, pts)))
     for name, run in legs:
         try:
             out[name] = run()
@@ -473,6 +509,100 @@ def steps_timed(f, stream, first, warmup, steps):
         for _ in range(steps):
             f.step(1, stream.handle)
     return tm.ms / steps, f.log(first + warmup, steps)
+
+
+def integrators(args, cl, cld, prm, pts):
+    """The other time integrators on the headline's 1,004,000-node cavity and dt, each
+    end to end through its entry point with host arrays in and out (CUDA events on the
+    default stream, which those calls use; every call ends synchronised).
+
+    SEMI_IMPLICIT_SPLIT_SOLVER as the reference's own driver sets it up
+    (eccentric_couette_flow_batch_ml.cpp:61-72: 5 outer iterations, iterative
+    tolerance 1e-4): Jacobi-BiCGSTAB velocity solves and the multigrid pressure
+    correction, to 1e-8, from rest.  IMPLICIT_SCALAR_TRANSPORT_SOLVER: one heated-lid
+    scalar step per call in the resulting velocity (the driver's closing call, :93-94).
+    FRACTIONAL_STEP_FOURIER: the cavity extruded over 2 nw + 1 = 5 planes of period 1,
+    5,020,000 unknowns per field."""
+    from memphys_b200 import capi, meshless
+    nv = cl.nv
+    K = max(1, args.integrator_steps)
+    out = {"nodes": nv, "dt": prm.dt}
+    state = {}
+
+    def semi_implicit():
+        t0 = time.time()
+        sis = meshless.SEMI_IMPLICIT_SPLIT_SOLVER(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                                  cl.p_dirichlet, 5, 1e-4, 10000)
+        t_setup = time.time() - t0
+        ns = sis.system_size
+        u, v, p = cl.vel_bc[0].copy(), cl.vel_bc[1].copy(), np.zeros(ns)
+        logs = []
+        un, vn, pn = np.zeros(nv), np.zeros(nv), np.zeros(ns)
+        sis.single_timestep_2d(un, vn, pn, u, v, p, 0)  # BDF1 step, untimed
+        u, v, p = un.copy(), vn.copy(), pn.copy()
+        with capi.Timer(None) as tm:
+            for k in range(K):
+                logs.append(sis.single_timestep_2d(un, vn, pn, u, v, p, 1 + k))
+                u, v, p = un.copy(), vn.copy(), pn.copy()
+        state["vel"] = (u, v)
+        return {"ms_per_step": round(tm.ms / K, 3), "steps": K,
+                "outer_iters_per_step": float(np.mean([l[0] for l in logs])),
+                "last_l1_change": logs[-1][1], "setup_s": round(t_setup, 2),
+                "config": "n_outer_iter 5, iterative_tolerance 1e-4, solves to 1e-8, "
+                          "BDF2 steps after one BDF1 step from rest"}
+
+    def scalar_transport():
+        # a transient step: the unsteady coefficient is 1 / dt (the reference multiplies
+        # it by the BDF factor only), convection 1, diffusion 0.01; the velocity is the
+        # semi-implicit run's (the lid's where that run failed)
+        u, v = state.get("vel", (cl.vel_bc[0], cl.vel_bc[1]))
+        ist = meshless.IMPLICIT_SCALAR_TRANSPORT_SOLVER(pts, cld, prm, cl.boundary, 10000,
+                                                        1.0 / prm.dt, 1.0, -0.01)
+        phi = np.where(cl.boundary & (cl.vel_bc[0] != 0), 1.0, 0.0)
+        phn = np.zeros(nv)
+        ist.single_timestep_2d(phn, phi, u, v, 0)
+        phi = phn.copy()
+        its = []
+        with capi.Timer(None) as tm:
+            for k in range(K):
+                n_it, rr = ist.single_timestep_2d(phn, phi, u, v, 1 + k)
+                its.append(n_it)
+                phi = phn.copy()
+        return {"ms_per_step": round(tm.ms / K, 3), "steps": K,
+                "iters_per_step": float(np.mean(its)), "last_relres": rr}
+
+    def fourier_z():
+        nw, N = 2, 5
+        t0 = time.time()
+        fsf = meshless.FRACTIONAL_STEP_FOURIER(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                               cl.u_dirichlet, cl.p_dirichlet, 1.0, nw, 2)
+        t_setup = time.time() - t0
+        z = np.arange(N) / N
+        x, y = cl.xyz[:, 0], cl.xyz[:, 1]
+        g = [np.repeat(cl.vel_bc[0][:, None], N, 1), np.zeros((nv, N)),
+             np.where(cl.boundary[:, None], 0.0,
+                      0.05 * (np.sin(np.pi * x) * np.sin(np.pi * y))[:, None]
+                      * np.cos(2 * np.pi * z)[None, :]), np.zeros((nv, N))]
+        o = [np.zeros((nv, N)) for _ in range(4)]
+        fsf.single_timestep(*o, *g, 0)
+        g = [a.copy() for a in o]
+        with capi.Timer(None) as tm:
+            for k in range(K):
+                fsf.single_timestep(*o, *g, 1 + k)
+                g = [a.copy() for a in o]
+        return {"ms_per_step": round(tm.ms / K, 3), "steps": K, "planes": N,
+                "unknowns_per_field": nv * N, "setup_s": round(t_setup, 2),
+                "w_max": float(np.abs(g[2]).max())}
+
+    for name, fn in (("semi_implicit", semi_implicit), ("scalar_transport", scalar_transport),
+                     ("fourier_z", fourier_z)):
+        try:
+            out[name] = fn()
+        except capi.MemphysError as e:
+            out[name] = {"error": str(e)[:300]}
+            if capi.lib().mp_stream_sync(None) != capi.MP_OK:
+                raise
+    return out
 
 
 def cube_mixed(args, stream):
@@ -657,12 +787,64 @@ def batched_stencils(nsys: int, stream):
     return res
 
 
-def profile_range(args, cl, cld, make, fs, vel0, p0, stream):
+def profile_range(args, cl, cld, make, fs, vel0, p0, stream, pts, prm):
     """Warm-up outside, `--steps` steps (SpMV launches, weight computations) inside the
     capture range."""
     from memphys_b200 import capi, meshless
     L = capi.lib()
     nv = cld.nv
+
+    def in_range(run):
+        for _ in range(args.warmup):
+            run(False)
+        L.mp_stream_sync(None)
+        stream.sync()
+        capi.check(L.mp_profiler(1))
+        for k in range(args.steps):
+            run(True)
+        L.mp_stream_sync(None)
+        stream.sync()
+        capi.check(L.mp_profiler(0))
+
+    if args.profile == "cloud":
+        # kNN stencils, PHS-RBF-FD weights and condition numbers of the whole cloud
+        in_range(lambda timed: meshless.CLOUD(pts, prm, compute_cond=True))
+        return {"profile": "cloud", "builds": args.steps, "nodes": nv}
+    if args.profile == "sis":
+        sis = meshless.SEMI_IMPLICIT_SPLIT_SOLVER(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                                  cl.p_dirichlet, 5, 1e-4, 10000)
+        st = {"u": cl.vel_bc[0].copy(), "v": cl.vel_bc[1].copy(), "p": np.zeros(sis.system_size),
+              "it": 0}
+
+        def sis_step(timed):
+            un, vn, pn = np.zeros(nv), np.zeros(nv), np.zeros(sis.system_size)
+            sis.single_timestep_2d(un, vn, pn, st["u"], st["v"], st["p"], st["it"])
+            st.update(u=un, v=vn, p=pn, it=st["it"] + 1)
+        in_range(sis_step)
+        return {"profile": "sis", "steps": args.steps, "nodes": nv}
+    if args.profile == "fsf":
+        N = 5
+        fsf = meshless.FRACTIONAL_STEP_FOURIER(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                               cl.u_dirichlet, cl.p_dirichlet, 1.0, 2, 2)
+        st = {"g": [np.repeat(cl.vel_bc[0][:, None], N, 1)] + [np.zeros((nv, N))] * 3, "it": 0}
+
+        def fsf_step(timed):
+            o = [np.zeros((nv, N)) for _ in range(4)]
+            fsf.single_timestep(*o, *st["g"], st["it"])
+            st.update(g=o, it=st["it"] + 1)
+        in_range(fsf_step)
+        return {"profile": "fsf", "steps": args.steps, "nodes": nv, "planes": N}
+    if args.profile == "train":
+        # samples from a short spin-up, then training epochs in the range
+        net = meshless.MLP(seed=7)
+        meshless.attach_mlp(fs, net, sample_nodes=min(args.samples, nv),
+                            capacity_steps=max(args.spinup, 3))
+        fs.set_state(vel0, p0, 0)
+        fs.step(max(args.spinup, 3), stream.handle)
+        stream.sync()
+        in_range(lambda timed: meshless.train_mlp(fs, epochs=1, batch=1024, lr=1e-3))
+        return {"profile": "train", "epochs": args.steps,
+                "samples": min(args.samples, nv) * max(args.spinup - 2, 1)}
     if args.profile == "steps":
         if args.variant != "plain":
             fs = make(precision=capi.MP_MG32)
