@@ -378,8 +378,13 @@ int mp_sis_create(mp_cloud c, const uint8_t *boundary, const double *normal,
                   const mp_solver_cfg *p_solver, mp_sis *out);
 /* nv + 1 when the pressure is full Neumann (bordered), else nv */
 int mp_sis_system_size(mp_sis s, int *nsys);
-/* solves launched as CUDA graphs (1, default) or kernel by kernel (0) */
+/* solves launched as CUDA graphs (1, default) or kernel by kernel (0); with graphs
+ * the whole outer loop of a step is one graph launch, its stopping test on the device */
 int mp_sis_set_graph(mp_sis s, int use_graph);
+/* SEMI_IMPLICIT_SPLIT_SOLVER::iterative_tolerance (class.hpp:444, a public member the
+ * reference's driver resets before every step, eccentric_couette_flow_batch_ml.cpp:71-73):
+ * the L1-change tolerance of the following steps */
+int mp_sis_set_tolerance(mp_sis s, double iterative_tolerance);
 /* single_timestep_2d (:376-421): vel_old = {u_old, v_old} (nv each), p_old
  * (system size) -> vel_new, p_new; it = timestep index (BDF1 at 0); the solver
  * keeps u_old, v_old of the call for the next BDF2 step.  Host or device

@@ -35,7 +35,8 @@ EXPORTS = [
     "mp_stream_sync", "mp_timer_start", "mp_timer_stop", "mp_profiler", "mp_launch_count", "mp_num_poly_terms",
     "mp_cloud_size", "mp_poly_exponents", "mp_knn_stencils", "mp_knn_stencils_noalloc",
     "mp_interp_matrix", "mp_knn_probe", "mp_order_rcm", "mp_order_morton", "mp_permute_stencils", "mp_permute_rows",
-    "mp_sis_create", "mp_sis_system_size", "mp_sis_set_graph", "mp_sis_single_timestep",
+    "mp_sis_create", "mp_sis_system_size", "mp_sis_set_graph", "mp_sis_set_tolerance",
+    "mp_sis_single_timestep",
     "mp_sis_destroy", "mp_ist_create", "mp_ist_set_graph", "mp_ist_single_timestep",
     "mp_ist_destroy", "mp_fsf_create", "mp_fsf_set_graph", "mp_fsf_single_timestep",
     "mp_fsf_destroy",
@@ -109,6 +110,7 @@ def lib() -> C.CDLL:
             "mp_permute_rows": [vp, vp, i, i, vp, vp],
             "mp_sis_create": [vp, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(vp)],
             "mp_sis_system_size": [vp, C.POINTER(i)], "mp_sis_set_graph": [vp, i],
+            "mp_sis_set_tolerance": [vp, C.c_double],
             "mp_sis_single_timestep": [vp, vp, vp, vp, vp, i, C.POINTER(i), C.POINTER(d),
                                        C.POINTER(d), vp],
             "mp_sis_destroy": [vp],

@@ -285,47 +285,37 @@ __global__ void k_hist_rotate(int nsys, const double *pcur, double *ph1, double 
 // Fischer's projection of successive right-hand sides: with D_j the last m <= 8
 // pressure increments and W_j = A D_j (= b_j - b_{j-1}: each p^{j+1} solved A p = b_j to the
 // tolerance), the guess p^n + sum_j c_j D_j minimises ||(b_n - b_{n-1}) - sum_j
-// c_j W_j|| = ||b_n - A(p^n + sum c_j D_j)|| up to the tolerance.  One pass forms
-// the right-hand side and the Gram matrix of the W_j (normalised, with a small
-// ridge: successive increments are nearly parallel), the last block solves it.
+// c_j W_j|| = ||b_n - A(p^n + sum c_j D_j)|| up to the tolerance.  The Gram matrix
+// G_jl = W_j . W_l of the ring's images is kept on the device: a pushed pair adds
+// its row (k_proj_push), so a step's solve forms only the m right-hand-side products
+// W_j . (b_n - b_{n-1}) and its last block solves the normalised system (with a
+// small ridge: successive increments are nearly parallel).
 constexpr int PROJ_MAX = 8;
-constexpr int PROJ_SUMS = PROJ_MAX + PROJ_MAX * (PROJ_MAX + 1) / 2;
 
 __global__ void __launch_bounds__(256)
-    k_proj_solve(int nsys, const double *b, const double *bprev, const double *W, int *state,
-                 double *coef, double *partials, unsigned *ticket) {
-    __shared__ double red[32 * PROJ_SUMS];
+    k_proj_solve(int nsys, const double *b, const double *bprev, const double *W,
+                 const double *Gm, int *state, double *coef, double *partials, unsigned *ticket) {
+    __shared__ double red[32 * PROJ_MAX];
     const int cnt = state[0];
-    double acc[PROJ_SUMS];
+    double acc[PROJ_MAX];
 #pragma unroll
-    for (int q = 0; q < PROJ_SUMS; q++)
+    for (int q = 0; q < PROJ_MAX; q++)
         acc[q] = 0.0;
     if (cnt > 0) {
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += gridDim.x * blockDim.x) {
             const double r = b[i] - bprev[i];
-            double w[PROJ_MAX];
 #pragma unroll
             for (int j = 0; j < PROJ_MAX; j++)
-                w[j] = j < cnt ? W[(size_t)j * nsys + i] : 0.0;
-            int q = PROJ_MAX;
-#pragma unroll
-            for (int j = 0; j < PROJ_MAX; j++) {
-                acc[j] += w[j] * r;
-#pragma unroll
-                for (int l = j; l < PROJ_MAX; l++)
-                    acc[q++] += w[j] * w[l];
-            }
+                if (j < cnt)
+                    acc[j] = fma(W[(size_t)j * nsys + i], r, acc[j]);
         }
     }
-    if (grid_reduce<PROJ_SUMS>(acc, partials, ticket, red) && threadIdx.x == 0) {
+    if (grid_reduce<PROJ_MAX>(acc, partials, ticket, red) && threadIdx.x == 0) {
         double G[PROJ_MAX][PROJ_MAX], h[PROJ_MAX], c[PROJ_MAX], sc[PROJ_MAX];
-        int q = PROJ_MAX;
-        for (int j = 0; j < PROJ_MAX; j++)
-            for (int l = j; l < PROJ_MAX; l++) {
-                G[j][l] = G[l][j] = acc[q];
-                q++;
-            }
         const int m = cnt > 0 ? cnt : 0;
+        for (int j = 0; j < m; j++)
+            for (int l = 0; l < m; l++)
+                G[j][l] = Gm[j * PROJ_MAX + l];
         bool ok = m > 0;
         for (int j = 0; j < m; j++) {
             sc[j] = G[j][j] > 0 ? 1.0 / sqrt(G[j][j]) : 0.0;
@@ -394,19 +384,37 @@ __global__ void k_proj_apply(int nsys, double *x, const double *D, const double 
     }
 }
 
-// after the solve: the new increment and its image into the ring slot at the head
-// (the first step after a restart only records the right-hand side)
-__global__ void k_proj_push(int nsys, const double *x, const double *pcur, const double *b,
-                            double *bprev, double *D, double *W, const int *state) {
+// after the solve: the new increment and its image into the ring slot at the head,
+// and that image's row of the Gram matrix against every slot holding a pair (slots
+// fill from 0, so while the ring is filling they are 0..head); the first step after
+// a restart only records the right-hand side
+__global__ void __launch_bounds__(256)
+    k_proj_push(int nsys, const double *x, const double *pcur, const double *b, double *bprev,
+                double *D, double *W, const int *state, int m, double *Gm, double *partials,
+                unsigned *ticket) {
+    __shared__ double red[32 * PROJ_MAX];
     const int cnt = state[0], head = state[1];
+    const int nval = cnt < 0 ? 0 : min(cnt + 1, m);
+    double acc[PROJ_MAX];
+#pragma unroll
+    for (int q = 0; q < PROJ_MAX; q++)
+        acc[q] = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += gridDim.x * blockDim.x) {
         const double bi = b[i];
         if (cnt >= 0) {
+            const double w = bi - bprev[i];
             D[(size_t)head * nsys + i] = x[i] - pcur[i];
-            W[(size_t)head * nsys + i] = bi - bprev[i];
+            W[(size_t)head * nsys + i] = w;
+#pragma unroll
+            for (int j = 0; j < PROJ_MAX; j++)
+                if (j < nval)
+                    acc[j] = fma(w, j == head ? w : W[(size_t)j * nsys + i], acc[j]);
         }
         bprev[i] = bi;
     }
+    if (cnt >= 0 && grid_reduce<PROJ_MAX>(acc, partials, ticket, red) && threadIdx.x == 0)
+        for (int j = 0; j < nval; j++)
+            Gm[head * PROJ_MAX + j] = Gm[j * PROJ_MAX + head] = acc[j];
 }
 
 // the ring holds m pairs
@@ -466,7 +474,7 @@ struct mp_fs1_s {
     // W_j = A D_j = b_j - b_{j-1}, the previous right-hand side, and on the device the
     // number of valid columns (-1: no previous right-hand side yet), the ring head and
     // the coefficients of the last guess
-    dbuf<double> pD, pW, pbprev, pcoef, ppart;
+    dbuf<double> pD, pW, pbprev, pcoef, ppart, pG;
     int proj_m = 0;    // ring length (pairs kept)
     dbuf<int> pstate;  // [0] valid columns, [1] ring head
     dbuf<unsigned> pticket;
@@ -535,8 +543,8 @@ static int fs1_issue_pre(mp_fs1_s *f, int cur, cudaStream_t s) {
         MP_CHECK_LAUNCH();
         if (uses_projection(f->guess)) {
             const unsigned g = (unsigned)std::min((ns + 255) / 256, sm_count() * 4);
-            k_proj_solve<<<g, 256, 0, s>>>(ns, f->P.W.b64.p, f->pbprev.p, f->pW.p, f->pstate.p,
-                                           f->pcoef.p, f->ppart.p, f->pticket.p);
+            k_proj_solve<<<g, 256, 0, s>>>(ns, f->P.W.b64.p, f->pbprev.p, f->pW.p, f->pG.p,
+                                           f->pstate.p, f->pcoef.p, f->ppart.p, f->pticket.p);
             MP_CHECK_LAUNCH();
             k_proj_apply<<<g, 256, 0, s>>>(ns, f->P.W.x.p, f->pD.p, f->pcoef.p, f->pstate.p);
             MP_CHECK_LAUNCH();
@@ -601,7 +609,8 @@ static int fs1_issue_post(mp_fs1_s *f, int cur, cudaStream_t s) {
         const int ns = f->P.sys.nsys;
         const unsigned g = (unsigned)std::min((ns + 255) / 256, sm_count() * 4);
         k_proj_push<<<g, 256, 0, s>>>(ns, f->P.W.x.p, f->pcur.p, f->P.W.b64.p, f->pbprev.p,
-                                      f->pD.p, f->pW.p, f->pstate.p);
+                                      f->pD.p, f->pW.p, f->pstate.p, f->proj_m, f->pG.p,
+                                      f->ppart.p, f->pticket.p);
         MP_CHECK_LAUNCH();
         k_proj_advance<<<1, 1, 0, s>>>(f->pstate.p, f->proj_m);
         MP_CHECK_LAUNCH();
@@ -664,7 +673,9 @@ static int proj_reserve(mp_fs1 f) {
         MP_TRY(f->pW.alloc(ns * m));
         MP_TRY(f->pbprev.alloc(ns));
         MP_TRY(f->pcoef.alloc(PROJ_MAX));
-        MP_TRY(f->ppart.alloc((size_t)PROJ_SUMS * sm_count() * 4 + 64));
+        MP_TRY(f->ppart.alloc((size_t)PROJ_MAX * sm_count() * 4 + 64));
+        MP_TRY(f->pG.alloc(PROJ_MAX * PROJ_MAX));
+        MP_CUDA(cudaMemset(f->pG.p, 0, sizeof(double) * PROJ_MAX * PROJ_MAX));
         MP_TRY(f->pticket.alloc(1));
         MP_TRY(f->pstate.alloc(2));
         MP_CUDA(cudaMemset(f->pticket.p, 0, sizeof(unsigned)));

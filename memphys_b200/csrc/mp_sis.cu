@@ -196,19 +196,89 @@ __global__ void k_sis_err(int nv, const double *u, const double *ui, const doubl
             part[4 * (size_t)blockIdx.x + q] = s[q][0];
 }
 
-// the blocks' partials in block order: [l1 error, max error] (:401-404)
-__global__ void k_sis_err_final(int nb, const double *part, int nv, double *out) {
-    if (blockIdx.x | threadIdx.x)
-        return;
-    double su = 0, sv = 0, mu = 0, mv = 0;
-    for (int b = 0; b < nb; b++) {
-        su += part[4 * (size_t)b];
-        sv += part[4 * (size_t)b + 1];
-        mu = fmax(mu, part[4 * (size_t)b + 2]);
-        mv = fmax(mv, part[4 * (size_t)b + 3]);
+// Outer-iteration state on the device: the count, the L1 and max changes of the
+// last iteration, and the first failed solve (0 none, 1 u, 2 v, 3 pressure) with
+// its status, iterations and relative residual.
+struct SisCtl {
+    int outer, status, failed, iters;
+    double relres, err[2];
+    double itol;  // the stopping tolerance of the L1 change, written by the host per step
+};
+
+// status of a finished solve, as Ppe::read_stats reports it
+__device__ int solve_status(const BicgScalars *S, double tol, double *relres) {
+    const double rr = S->b64_sq > 0 ? sqrt(S->rr_true / S->b64_sq) : 0.0;
+    int st = S->status;
+    if (st == MP_OK && rr > tol && S->b64_sq > 0 && !(S->rr_true <= S->abs_tol2))
+        st = MP_NOT_CONVERGED;
+    if (st == MP_OK && !isfinite(rr))
+        st = MP_NAN_DETECTED;
+    *relres = rr;
+    return st;
+}
+
+__global__ void k_sis_outer_init(SisCtl *ctl, cudaGraphConditionalHandle h) {
+    ctl->outer = 0;
+    ctl->status = MP_OK;
+    ctl->failed = 0;
+    ctl->iters = 0;
+    ctl->relres = 0;
+    ctl->err[0] = ctl->err[1] = 0;
+    if (h)
+        cudaGraphSetConditional(h, 1u);
+}
+
+// End of an outer iteration: the blocks' partials to [l1 error, max error]
+// (:401-404), the three solves' statuses, and whether another iteration runs
+// (:405-418: the L1 change is above the tolerance, fewer than n_outer iterations
+// ran, and every solve succeeded).  One block of 256 threads.
+__global__ void __launch_bounds__(256)
+    k_sis_outer_end(int nb, const double *part, int nv, SisCtl *ctl, const BicgScalars *Su,
+                    const BicgScalars *Sv, const BicgScalars *Sp, double tol_u, double tol_v,
+                    double tol_p, int n_outer, cudaGraphConditionalHandle h) {
+    __shared__ double sh[4][256];
+    double a[4] = {0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        a[0] += part[4 * (size_t)b];
+        a[1] += part[4 * (size_t)b + 1];
+        a[2] = fmax(a[2], part[4 * (size_t)b + 2]);
+        a[3] = fmax(a[3], part[4 * (size_t)b + 3]);
     }
-    out[0] = su / (2.0 * nv) + sv / (2.0 * nv);
-    out[1] = mu / 2.0 + mv / 2.0;
+    for (int q = 0; q < 4; q++)
+        sh[q][threadIdx.x] = a[q];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w /= 2) {
+        if ((int)threadIdx.x < w) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+            sh[2][threadIdx.x] = fmax(sh[2][threadIdx.x], sh[2][threadIdx.x + w]);
+            sh[3][threadIdx.x] = fmax(sh[3][threadIdx.x], sh[3][threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x)
+        return;
+    const double l1 = sh[0][0] / (2.0 * nv) + sh[1][0] / (2.0 * nv);
+    ctl->err[0] = l1;
+    ctl->err[1] = sh[2][0] / 2.0 + sh[3][0] / 2.0;
+    ctl->outer += 1;
+    const BicgScalars *S[3] = {Su, Sv, Sp};
+    const double tol[3] = {tol_u, tol_v, tol_p};
+    for (int q = 0; q < 3 && ctl->status == MP_OK; q++) {
+        double rr;
+        const int st = solve_status(S[q], tol[q], &rr);
+        if (st != MP_OK) {
+            ctl->status = st;
+            ctl->failed = q + 1;
+            ctl->iters = S[q]->it;
+            ctl->relres = rr;
+        }
+    }
+    if (ctl->status == MP_OK && !isfinite(l1))
+        ctl->status = MP_NAN_DETECTED;
+    const bool more = ctl->status == MP_OK && l1 > ctl->itol && ctl->outer < n_outer;
+    if (h)
+        cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
 // IMPLICIT_SCALAR_TRANSPORT_SOLVER::modify_matrix (implicit_scalar_transport_solver.cpp:87-109):
@@ -257,20 +327,12 @@ struct mp_sis_s {
     dbuf<uint8_t> udir, vdir, pdir;
     dbuf<double> normal;
     Ppe U, V, P;
-    dbuf<double> uo, vo, uoo, voo, pn, uit, vit, part, err;
+    dbuf<double> uo, vo, uoo, voo, pn, uit, vit, part;
+    dbuf<SisCtl> ctl;
     int err_blocks = 0;
     bool use_graph = true;
+    GraphExec graph[2];  // the outer loop of a BDF1 and of a BDF2 step
 };
-
-static int sis_solve(Ppe &S, bool graph, cudaStream_t st, const char *what) {
-    MP_TRY(S.solve_resident(st, graph));
-    SolveStats ss;
-    MP_TRY(S.read_stats(st, &ss));
-    if (ss.status != MP_OK)
-        return fail(ss.status, "semi-implicit %s solve: status %d after %d iterations, relres %g",
-                    what, ss.status, ss.iters, ss.relres);
-    return MP_OK;
-}
 
 extern "C" int mp_sis_create(mp_cloud c, const uint8_t *boundary, const double *normal,
                              const uint8_t *u_dir, const uint8_t *v_dir, const uint8_t *p_dir,
@@ -341,7 +403,7 @@ extern "C" int mp_sis_create(mp_cloud c, const uint8_t *boundary, const double *
     for (dbuf<double> *d : {&s->uoo, &s->voo})
         MP_CUDA(cudaMemset(d->p, 0, sizeof(double) * nv));
     s->err_blocks = std::min((nv + 255) / 256, sm_count() * 4);
-    if ((rc = s->part.alloc((size_t)4 * s->err_blocks)) != MP_OK || (rc = s->err.alloc(2)) != MP_OK)
+    if ((rc = s->part.alloc((size_t)4 * s->err_blocks)) != MP_OK || (rc = s->ctl.alloc(1)) != MP_OK)
         return bail(rc);
     // boundary stencils holding other boundary nodes make the boundary pressure
     // rows depend on each other: run them in index order then
@@ -362,6 +424,13 @@ extern "C" int mp_sis_create(mp_cloud c, const uint8_t *boundary, const double *
     return MP_OK;
 }
 
+extern "C" int mp_sis_set_tolerance(mp_sis s, double iterative_tolerance) {
+    if (!s || !(iterative_tolerance >= 0))
+        return fail(MP_BAD_ARG, "mp_sis_set_tolerance: a solver and a tolerance >= 0 needed");
+    s->itol = iterative_tolerance;
+    return MP_OK;
+}
+
 extern "C" int mp_sis_system_size(mp_sis s, int *nsys) {
     if (!s || !nsys)
         return fail(MP_BAD_ARG, "mp_sis_system_size: null argument");
@@ -376,6 +445,103 @@ extern "C" int mp_sis_set_graph(mp_sis s, int use_graph) {
     return MP_OK;
 }
 
+// One outer iteration in three kernel sequences around the solves (each issued
+// eagerly or captured): before the velocity solves, between them and the
+// pressure-correction solve, and after it (ending with the stopping test).
+static int sis_issue_head(mp_sis_s *s, int bdf1, cudaStream_t st) {
+    const int nv = s->nv, K = s->K;
+    const size_t vb = sizeof(double) * nv;
+    CloudView cv = cloud_view(s->c);
+    const SisConst c{nv, K, s->rho, s->mu, s->dt};
+    const double a1 = bdf1 ? 1.0 : 1.5;
+    double *un = s->U.W.x.p, *vn = s->V.W.x.p;
+    const size_t tot = (size_t)ell_padded_rows(nv) * K;
+    const unsigned eb = (unsigned)((tot + 255) / 256), rb = (unsigned)((nv + 255) / 256);
+    MP_CUDA(cudaMemcpyAsync(s->uit.p, un, vb, cudaMemcpyDeviceToDevice, st));
+    MP_CUDA(cudaMemcpyAsync(s->vit.p, vn, vb, cudaMemcpyDeviceToDevice, st));
+    k_sis_values<<<eb, 256, 0, st>>>(c, cv.cols, cv.w[0], cv.w[1], cv.w[3], cv.bflag, un, vn,
+                                     a1 * s->rho / s->dt, s->U.sys.A.v64.p, s->V.sys.A.v64.p);
+    MP_CHECK_LAUNCH();
+    MP_TRY(s->U.refresh_diag(st));
+    MP_TRY(s->V.refresh_diag(st));
+    k_sis_vel_source<<<rb, 256, 0, st>>>(c, cv.cols, cv.w[0], cv.w[1], cv.bflag, s->udir.p,
+                                         s->vdir.p, s->pn.p, s->uo.p, s->vo.p, s->uoo.p, s->voo.p,
+                                         bdf1, s->U.W.b64.p, s->V.W.b64.p);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+static int sis_issue_mid(mp_sis_s *s, int bdf1, cudaStream_t st) {
+    const int ns = s->nsys;
+    CloudView cv = cloud_view(s->c);
+    const SisConst c{s->nv, s->K, s->rho, s->mu, s->dt};
+    const double a1 = bdf1 ? 1.0 : 1.5;
+    k_sis_p_source<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(
+        c, cv.cols, cv.w[0], cv.w[1], cv.bflag, s->U.W.x.p, s->V.W.x.p, a1 * s->rho / s->dt, ns,
+        s->P.W.b64.p);
+    MP_CHECK_LAUNCH();
+    MP_CUDA(cudaMemsetAsync(s->P.W.x.p, 0, sizeof(double) * ns, st));
+    return MP_OK;
+}
+
+static int sis_issue_tail(mp_sis_s *s, int bdf1, cudaGraphConditionalHandle h, cudaStream_t st) {
+    const int nv = s->nv, ns = s->nsys;
+    CloudView cv = cloud_view(s->c);
+    const SisConst c{nv, s->K, s->rho, s->mu, s->dt};
+    const double a1 = bdf1 ? 1.0 : 1.5;
+    double *un = s->U.W.x.p, *vn = s->V.W.x.p, *pp = s->P.W.x.p;
+    const unsigned rb = (unsigned)((nv + 255) / 256);
+    k_sis_add<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(ns, s->pn.p, pp);
+    MP_CHECK_LAUNCH();
+    k_sis_p_boundary<<<s->serial_pb ? 1 : rb, s->serial_pb ? 1 : 256, 0, st>>>(
+        c, cv.cols, cv.w[0], cv.w[1], cv.w[3], cv.bflag, s->pdir.p, s->normal.p, un, vn, s->uo.p,
+        s->vo.p, s->uoo.p, s->voo.p, bdf1, s->serial_pb, s->pn.p);
+    MP_CHECK_LAUNCH();
+    k_sis_vel_corr<<<rb, 256, 0, st>>>(c, cv.cols, cv.w[0], cv.w[1], cv.bflag, pp,
+                                       s->dt / (a1 * s->rho), un, vn);
+    MP_CHECK_LAUNCH();
+    k_sis_err<<<s->err_blocks, 256, 0, st>>>(nv, un, s->uit.p, vn, s->vit.p, s->part.p);
+    MP_CHECK_LAUNCH();
+    k_sis_outer_end<<<1, 256, 0, st>>>(s->err_blocks, s->part.p, nv, s->ctl.p, s->U.W.scal.p,
+                                       s->V.W.scal.p, s->P.W.scal.p, s->U.cfg.tol, s->V.cfg.tol,
+                                       s->P.cfg.tol, s->n_outer, h);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
+// The whole outer loop as one graph: a while node whose body holds the three
+// solves (each its own nested while loop) and ends with the stopping test, so a
+// step makes no host round trip between its copies in and out.
+static int sis_graph(mp_sis_s *s, int bdf1, GraphExec &G) {
+    if (G.e)
+        return MP_OK;
+    GraphBuilder gb;
+    MP_TRY(gb.init_root(s->P.cap_stream()));
+    cudaGraphConditionalHandle h;
+    int rc = gb.make_handle(&h);
+    if (rc == MP_OK)
+        rc = gb.captured([&](cudaStream_t cs) -> int {
+            k_sis_outer_init<<<1, 1, 0, cs>>>(s->ctl.p, h);
+            MP_CHECK_LAUNCH();
+            return MP_OK;
+        });
+    if (rc == MP_OK)
+        rc = gb.while_loop(h, [&](GraphBuilder &body) {
+            MP_TRY(body.captured([&](cudaStream_t cs) { return sis_issue_head(s, bdf1, cs); }));
+            MP_TRY(s->U.build_solve_graph(body));
+            MP_TRY(s->V.build_solve_graph(body));
+            MP_TRY(body.captured([&](cudaStream_t cs) { return sis_issue_mid(s, bdf1, cs); }));
+            MP_TRY(s->P.build_solve_graph(body));
+            return body.captured([&](cudaStream_t cs) { return sis_issue_tail(s, bdf1, h, cs); });
+        });
+    if (rc != MP_OK) {
+        if (gb.g)
+            cudaGraphDestroy(gb.g);
+        return rc;
+    }
+    return G.instantiate(gb);
+}
+
 extern "C" int mp_sis_single_timestep(mp_sis s, const double *const *vel_old,
                                       const double *p_old, double *const *vel_new,
                                       double *p_new, int it, int *n_outer, double *l1_err,
@@ -384,64 +550,50 @@ extern "C" int mp_sis_single_timestep(mp_sis s, const double *const *vel_old,
         !vel_new[1] || !p_new || it < 0)
         return fail(MP_BAD_ARG, "mp_sis_single_timestep: bad arguments");
     cudaStream_t st = S(stream);
-    const int nv = s->nv, K = s->K, ns = s->nsys;
+    const int nv = s->nv, ns = s->nsys;
     const size_t vb = sizeof(double) * nv;
-    CloudView cv = cloud_view(s->c);
-    const SisConst c{nv, K, s->rho, s->mu, s->dt};
     const int bdf1 = it == 0;
-    const double a1 = bdf1 ? 1.0 : 1.5;
-    double *un = s->U.W.x.p, *vn = s->V.W.x.p, *pp = s->P.W.x.p;
+    double *un = s->U.W.x.p, *vn = s->V.W.x.p;
     // u_new = u_old, v_new = v_old, p_new = p_old (:384)
     MP_CUDA(cudaMemcpyAsync(s->uo.p, vel_old[0], vb, cudaMemcpyDefault, st));
     MP_CUDA(cudaMemcpyAsync(s->vo.p, vel_old[1], vb, cudaMemcpyDefault, st));
     MP_CUDA(cudaMemcpyAsync(s->pn.p, p_old, sizeof(double) * ns, cudaMemcpyDefault, st));
     MP_CUDA(cudaMemcpyAsync(un, s->uo.p, vb, cudaMemcpyDeviceToDevice, st));
     MP_CUDA(cudaMemcpyAsync(vn, s->vo.p, vb, cudaMemcpyDeviceToDevice, st));
-    const size_t tot = (size_t)ell_padded_rows(nv) * K;
-    const unsigned eb = (unsigned)((tot + 255) / 256), rb = (unsigned)((nv + 255) / 256);
-    const unsigned sb = (unsigned)((ns + 255) / 256);
-    double herr[2] = {0, 0};
-    int outer = 0;
-    for (outer = 0; outer < s->n_outer; outer++) {
-        MP_CUDA(cudaMemcpyAsync(s->uit.p, un, vb, cudaMemcpyDeviceToDevice, st));
-        MP_CUDA(cudaMemcpyAsync(s->vit.p, vn, vb, cudaMemcpyDeviceToDevice, st));
-        k_sis_values<<<eb, 256, 0, st>>>(c, cv.cols, cv.w[0], cv.w[1], cv.w[3], cv.bflag, un, vn,
-                                         a1 * s->rho / s->dt, s->U.sys.A.v64.p, s->V.sys.A.v64.p);
-        MP_CHECK_LAUNCH();
-        MP_TRY(s->U.refresh_diag(st));
-        MP_TRY(s->V.refresh_diag(st));
-        k_sis_vel_source<<<rb, 256, 0, st>>>(c, cv.cols, cv.w[0], cv.w[1], cv.bflag, s->udir.p,
-                                             s->vdir.p, s->pn.p, s->uo.p, s->vo.p, s->uoo.p,
-                                             s->voo.p, bdf1, s->U.W.b64.p, s->V.W.b64.p);
-        MP_CHECK_LAUNCH();
-        MP_TRY(sis_solve(s->U, s->use_graph, st, "u"));
-        MP_TRY(sis_solve(s->V, s->use_graph, st, "v"));
-        k_sis_p_source<<<sb, 256, 0, st>>>(c, cv.cols, cv.w[0], cv.w[1], cv.bflag, un, vn,
-                                           a1 * s->rho / s->dt, ns, s->P.W.b64.p);
-        MP_CHECK_LAUNCH();
-        MP_CUDA(cudaMemsetAsync(pp, 0, sizeof(double) * ns, st));
-        MP_TRY(sis_solve(s->P, s->use_graph, st, "pressure-correction"));
-        k_sis_add<<<sb, 256, 0, st>>>(ns, s->pn.p, pp);
-        MP_CHECK_LAUNCH();
-        k_sis_p_boundary<<<s->serial_pb ? 1 : rb, s->serial_pb ? 1 : 256, 0, st>>>(
-            c, cv.cols, cv.w[0], cv.w[1], cv.w[3], cv.bflag, s->pdir.p, s->normal.p, un, vn,
-            s->uo.p, s->vo.p, s->uoo.p, s->voo.p, bdf1, s->serial_pb, s->pn.p);
-        MP_CHECK_LAUNCH();
-        k_sis_vel_corr<<<rb, 256, 0, st>>>(c, cv.cols, cv.w[0], cv.w[1], cv.bflag, pp,
-                                           s->dt / (a1 * s->rho), un, vn);
-        MP_CHECK_LAUNCH();
-        k_sis_err<<<s->err_blocks, 256, 0, st>>>(nv, un, s->uit.p, vn, s->vit.p, s->part.p);
-        MP_CHECK_LAUNCH();
-        k_sis_err_final<<<1, 1, 0, st>>>(s->err_blocks, s->part.p, nv, s->err.p);
-        MP_CHECK_LAUNCH();
-        MP_CUDA(cudaMemcpyAsync(herr, s->err.p, sizeof(herr), cudaMemcpyDeviceToHost, st));
+    SisCtl hc{};
+    // the tolerance may change between steps (the reference's driver sets it from the
+    // steady-state change every step); a pageable source is staged before the call returns
+    MP_CUDA(cudaMemcpyAsync(&s->ctl.p->itol, &s->itol, sizeof(double), cudaMemcpyHostToDevice, st));
+    if (s->use_graph) {
+        GraphExec &G = s->graph[bdf1 ? 0 : 1];
+        MP_TRY(sis_graph(s, bdf1, G));
+        MP_TRY(G.launch(st));
+        MP_CUDA(cudaMemcpyAsync(&hc, s->ctl.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
         MP_CUDA(cudaStreamSynchronize(st));
-        if (!std::isfinite(herr[0]))
-            return fail(MP_NAN_DETECTED, "semi-implicit step %d: NaN in the velocity", it);
-        if (herr[0] <= s->itol) {
-            outer++;
-            break;
+    } else {  // eager: the same sequences, the host reads the state after each iteration
+        k_sis_outer_init<<<1, 1, 0, st>>>(s->ctl.p, 0);
+        MP_CHECK_LAUNCH();
+        for (int outer = 0; outer < s->n_outer; outer++) {
+            MP_TRY(sis_issue_head(s, bdf1, st));
+            MP_TRY(s->U.solve_resident(st, false));
+            MP_TRY(s->V.solve_resident(st, false));
+            MP_TRY(sis_issue_mid(s, bdf1, st));
+            MP_TRY(s->P.solve_resident(st, false));
+            MP_TRY(sis_issue_tail(s, bdf1, 0, st));
+            MP_CUDA(cudaMemcpyAsync(&hc, s->ctl.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
+            MP_CUDA(cudaStreamSynchronize(st));
+            if (hc.status != MP_OK || !(hc.err[0] > s->itol))
+                break;
         }
+    }
+    if (hc.status != MP_OK) {
+        static const char *what[4] = {"velocity", "u", "v", "pressure-correction"};
+        if (hc.failed)
+            return fail(hc.status,
+                        "semi-implicit step %d, outer iteration %d: %s solve status %d after %d "
+                        "iterations, relres %g", it, hc.outer, what[hc.failed], hc.status,
+                        hc.iters, hc.relres);
+        return fail(hc.status, "semi-implicit step %d: NaN in the velocity", it);
     }
     // extras (:206-216): u_old_old = u_old
     MP_CUDA(cudaMemcpyAsync(s->uoo.p, s->uo.p, vb, cudaMemcpyDeviceToDevice, st));
@@ -451,11 +603,11 @@ extern "C" int mp_sis_single_timestep(mp_sis s, const double *const *vel_old,
     MP_CUDA(cudaMemcpyAsync(p_new, s->pn.p, sizeof(double) * ns, cudaMemcpyDefault, st));
     MP_CUDA(cudaStreamSynchronize(st));
     if (n_outer)
-        *n_outer = std::min(outer, s->n_outer);
+        *n_outer = hc.outer;
     if (l1_err)
-        *l1_err = herr[0];
+        *l1_err = hc.err[0];
     if (max_err)
-        *max_err = herr[1];
+        *max_err = hc.err[1];
     return MP_OK;
 }
 

@@ -291,6 +291,8 @@ class SEMI_IMPLICIT_SPLIT_SOLVER {
   public:
     mp_sis handle = nullptr;
     int system_size = 0;
+    // public as in the reference (class.hpp): its driver resets it before every step
+    double iterative_tolerance = 0;
     std::vector<unsigned char> u_d, v_d, p_d;
 
     SEMI_IMPLICIT_SPLIT_SOLVER(POINTS &points, CLOUD &cloud, PARAMETERS &parameters,
@@ -301,6 +303,7 @@ class SEMI_IMPLICIT_SPLIT_SOLVER {
         u_d.assign(u_dirichlet_flag1.begin(), u_dirichlet_flag1.end());
         v_d.assign(v_dirichlet_flag1.begin(), v_dirichlet_flag1.end());
         p_d.assign(p_dirichlet_flag1.begin(), p_dirichlet_flag1.end());
+        iterative_tolerance = iterative_tolerance1;
         mp_sis_cfg cfg{parameters.rho, parameters.mu, parameters.dt, n_outer_iter1,
                        iterative_tolerance1, precond_freq_it1};
         mp_solver_cfg vel = parameters.integrator_cfg(), pres = parameters.integrator_cfg();
@@ -333,6 +336,8 @@ class SEMI_IMPLICIT_SPLIT_SOLVER {
         double *vn[2] = {u_new.data(), v_new.data()};
         int n = 0;
         double l1 = 0, mx = 0;
+        check(mp_sis_set_tolerance(handle, iterative_tolerance),
+              "SEMI_IMPLICIT_SPLIT_SOLVER::iterative_tolerance");
         check(mp_sis_single_timestep(handle, vo, p_old.data(), vn, p_new.data(), it1, &n, &l1, &mx,
                                      nullptr),
               "SEMI_IMPLICIT_SPLIT_SOLVER::single_timestep_2d");

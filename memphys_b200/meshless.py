@@ -461,7 +461,19 @@ class SEMI_IMPLICIT_SPLIT_SOLVER:
         check(capi.lib().mp_sis_system_size(h, C.byref(ns)))
         self.system_size = ns.value
         self.nv = points.nv
+        self._itol = float(iterative_tolerance)
         check(capi.lib().mp_sis_set_graph(h, int(use_graph)))
+
+    @property
+    def iterative_tolerance(self) -> float:
+        """The L1-change tolerance of the outer iteration; the reference's driver resets
+        this public member before every step (eccentric_couette_flow_batch_ml.cpp:71-73)."""
+        return self._itol
+
+    @iterative_tolerance.setter
+    def iterative_tolerance(self, value: float):
+        check(capi.lib().mp_sis_set_tolerance(self.handle, float(value)), "iterative_tolerance")
+        self._itol = float(value)
 
     def single_timestep_2d(self, u_new, v_new, p_new, u_old, v_old, p_old, it,
                            n_outer_iter_log=None, iterative_l1_err_log=None,

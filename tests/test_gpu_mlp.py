@@ -167,3 +167,52 @@ def test_learned_guess_channel_with_obstacle(mp_lib):
         res[guess] = log[2:, 0].mean()
     print("channel: mean iterations zero / learned guess:", res)
     assert res[capi.MP_GUESS_LEARNED] < 0.8 * res[capi.MP_GUESS_ZERO]
+
+
+def test_learned_guess_against_projection(mp_lib):
+    """The learned guess against the method without the network: the projection guess it
+    starts from.  Reduced learned-guess configuration (channel with the cylinder,
+    Re = 200); the network trains on 60 plain-solver steps, then both guesses run 16
+    steps from the same state, restarted, to the same tolerance.
+
+    What the test holds: the learned guess never starts from a larger residual than the
+    projection (its weight minimises the guess's residual and is zero when the network
+    does not help; the margin covers the two runs' histories, which differ by their
+    solves' errors), never needs more than half an iteration per step more, and both
+    reach 1e-8.  The gain itself is printed; on this flow and on the 1M-node ones
+    the network's weight settles near zero and the gain is nil (the recorded negative
+    result of the learned part)."""
+    cl = clouds.channel_2d(0.025, seed=6)
+    prm = meshless.PARAMETERS(solver_type="cuda_bicgstab_amg", solver_tolerance=1e-8, n_iter=4000)
+    prm.rho, prm.mu = 1.0, 0.2 / 200.0
+    pts = meshless.POINTS(cl)
+    cld = meshless.CLOUD(pts, prm, compute_cond=False)
+    prm.dt = 0.1 * meshless.calc_dt(cld, 1.5, 1.0, 0.0, prm.mu / prm.rho, 0.25)
+    fs = meshless.FRACTIONAL_STEP_1(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                    cl.p_dirichlet, 2, w_dirichlet_flag=cl.w_dirichlet)
+    fs.set_state([cl.vel_bc[0], cl.vel_bc[1]], np.zeros(fs.system_size), 0)
+    net = meshless.MLP(seed=11)
+    meshless.attach_mlp(fs, net, sample_nodes=4096, capacity_steps=60)
+    fs.step(60)
+    loss = meshless.train_mlp(fs, epochs=10, batch=1024, lr=1e-3)
+    assert np.isfinite(loss)
+    meshless.attach_mlp(fs, net, sample_nodes=1, capacity_steps=1, collect=False)
+    vel, p = fs.get_state()
+    res = {}
+    for guess in (capi.MP_GUESS_PROJECT, capi.MP_GUESS_LEARNED):
+        meshless.set_guess(fs, guess)
+        # both from the same state as a first step (Euler, then AB2 from its own history;
+        # a later step index would carry the previous run's Adams-Bashforth history) with
+        # the guess history emptied
+        fs.set_state(vel, p, 0)
+        fs.step(16)
+        log = fs.log(0, 16)
+        assert np.all(log[:, 1] <= 1e-8)
+        res[guess] = {"iters": float(log[8:, 0].mean()), "relres0": float(log[8:, 4].mean()),
+                      "weight": float(log[8:, 6].mean())}
+    proj, lrn = res[capi.MP_GUESS_PROJECT], res[capi.MP_GUESS_LEARNED]
+    print("channel, steps 8-15 after a restart: projection", proj, "learned", lrn,
+          "gain in iterations", proj["iters"] - lrn["iters"])
+    # the two runs' histories differ by their solves' errors (1e-8), hence the margin
+    assert lrn["relres0"] <= proj["relres0"] * 1.1
+    assert lrn["iters"] <= proj["iters"] + 0.5

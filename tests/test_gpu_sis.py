@@ -84,6 +84,44 @@ def test_sis_rejects_bad_configuration(mp_lib):
 
 
 @pytest.mark.parametrize("use_graph", [True, False])
+def test_sis_tolerance_changed_between_steps(mp_lib, use_graph):
+    """The reference's driver resets iterative_tolerance before every step from the
+    steady-state change (eccentric_couette_flow_batch_ml.cpp:67-73); the graph holds
+    the outer loop with its stopping test on the device, so the new tolerance must
+    reach it: the outer-iteration counts follow the oracle's step by step."""
+    cl = clouds.cavity_2d(24, seed=3)
+    dt, n_outer = 5e-3, 8
+    # 1e-11: once the outer iteration has converged far, the pressure correction's source
+    # is rounding-sized and the bordered system floors near 2e-12 relative in FP64
+    prm = meshless.PARAMETERS(solver_type="cuda_bicgstab_amg", solver_tolerance=1e-11,
+                              n_iter=5000)
+    prm.rho, prm.mu, prm.dt = 1.0, 0.01, dt
+    pts = meshless.POINTS(cl)
+    cld = meshless.CLOUD(pts, prm, compute_cond=False).fetch()
+    sis = meshless.SEMI_IMPLICIT_SPLIT_SOLVER(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                              cl.p_dirichlet, n_outer, 1e-4, 1,
+                                              use_graph=use_graph)
+    w = {"gx": cld.grad_x_coeff, "gy": cld.grad_y_coeff, "lap": cld.laplacian_coeff}
+    ref = osis.SIS(cl, cld.nb_points_col, w, 1.0, 0.01, dt, cl.u_dirichlet, cl.v_dirichlet,
+                   cl.p_dirichlet, n_outer, 1e-4)
+    u, v, p = cl.vel_bc[0].copy(), cl.vel_bc[1].copy(), np.zeros(sis.system_size)
+    ru, rv, rp_ = u.copy(), v.copy(), p.copy()
+    counts, rcounts = [], []
+    for it, tol in enumerate([1.0, 1e-7, 1e-3, 1e-7]):
+        sis.iterative_tolerance = tol
+        ref.itol = tol
+        un, vn, pn = np.zeros_like(u), np.zeros_like(v), np.zeros_like(p)
+        counts.append(sis.single_timestep_2d(un, vn, pn, u, v, p, it)[0])
+        u, v, p = un, vn, pn
+        ru, rv, rp_, n, _, _ = ref.single_timestep_2d(ru, rv, rp_, it)
+        rcounts.append(n)
+    print("outer iterations GPU / oracle:", counts, rcounts)
+    assert counts == rcounts
+    assert len(set(counts)) > 1  # the tolerances changed the iteration counts
+    assert np.abs(u - ru).max() <= 1e-8 * np.abs(ru).max()
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
 def test_scalar_transport_matches_oracle(mp_lib, use_graph):
     """IMPLICIT_SCALAR_TRANSPORT_SOLVER: a temperature-like scalar in the cavity, hot
     lid (Dirichlet 1), cold bottom (Dirichlet 0), insulated sides (Neumann), carried
