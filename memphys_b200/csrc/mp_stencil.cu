@@ -85,17 +85,25 @@ __device__ __forceinline__ double ipow(double x, int e) {
     return v;
 }
 
-__device__ __forceinline__ double monomial(const double *x, int j, int dim) {
-    double t = ipow(x[0], c_exps[j * dim]);
+// monomial j at x; ex: the exponent table (a shared-memory copy of c_exps: lanes of a
+// warp read different monomials, which constant memory would serialise)
+__device__ __forceinline__ double monomial(const double *x, int j, int dim, const int *ex) {
+    double t = ipow(x[0], ex[j * dim]);
     for (int d = 1; d < dim; d++)
-        t *= ipow(x[d], c_exps[j * dim + d]);
+        t *= ipow(x[d], ex[j * dim + d]);
     return t;
 }
 
+// Layout of a stencil's scale record: per-axis scales, minima, the scaled probe
+// (interpolation mode) and the reciprocal scales
+constexpr int SC_SCALE = 0, SC_MIN = MAX_DIM, SC_PROBE = 2 * MAX_DIM, SC_INV = 3 * MAX_DIM;
+constexpr int SC_DOUBLES = 5 * MAX_DIM;  // odd multiple of MAX_DIM: keeps the GJ layout's pairs aligned
+
 // Entry (r, j) of the augmented system [A | B] for a stencil with n nodes whose
-// scaled coordinates are in sp (n x dim) and per-axis scales in sc.
+// scaled coordinates are in sp (n x dim) and scale record in sc (divisions by the
+// scales are products with their reciprocals).
 __device__ double aug_entry(int r, int j, int n, int m, int dim, int phs, const double *sp,
-                            const double *sc, const double *xp = nullptr) {
+                            const double *sc, const int *ex, const double *xp = nullptr) {
     const int S = n + m;
     if (j < S) {
         if (r < n && j < n) {
@@ -109,9 +117,9 @@ __device__ double aug_entry(int r, int j, int n, int m, int dim, int phs, const 
             return rpow_odd(r2, phs);
         }
         if (r < n)
-            return monomial(sp + r * dim, j - n, dim);
+            return monomial(sp + r * dim, j - n, dim, ex);
         if (j < n)
-            return monomial(sp + j * dim, r - n, dim);
+            return monomial(sp + j * dim, r - n, dim, ex);
         return 0.0;
     }
     if (xp) {  // interpolation: r^phs to the scaled probe, monomials at it (:430-454)
@@ -123,7 +131,7 @@ __device__ double aug_entry(int r, int j, int n, int m, int dim, int phs, const 
             }
             return rpow_odd(r2, phs);
         }
-        return monomial(xp, r - n, dim);
+        return monomial(xp, r - n, dim, ex);
     }
     const int c = j - S;  // rhs column: 0..dim-1 gradient, dim Laplacian
     const double *x0 = sp;  // centre = local node 0
@@ -134,7 +142,7 @@ __device__ double aug_entry(int r, int j, int n, int m, int dim, int phs, const 
             r2 += t * t;
         }
         if (c < dim)  // :124-125
-            return -phs * (sp[r * dim + c] - x0[c]) * rpow_odd(r2, phs - 2) / sc[c];
+            return -phs * (sp[r * dim + c] - x0[c]) * rpow_odd(r2, phs - 2) * sc[SC_INV + c];
         if (!(fabs(r2) > 1e-14))  // :229
             return 0.0;
         double acc = 0.0, rq4 = rpow_odd(r2, phs - 4), rq2 = rpow_odd(r2, phs - 2);
@@ -143,12 +151,12 @@ __device__ double aug_entry(int r, int j, int n, int m, int dim, int phs, const 
             double g = phs * phs * (dk * dk) * rq4;
             g = g - 2.0 * phs * (dk * dk) * rq4;
             g = g + phs * rq2;
-            acc += g / (sc[d] * sc[d]);
+            acc += g * (sc[SC_INV + d] * sc[SC_INV + d]);
         }
         return acc;
     }
     const int p = r - n;
-    const int *e = c_exps + p * dim;
+    const int *e = ex + p * dim;
     if (c < dim) {  // :128-140 and siblings
         if (e[c] <= 0)
             return 0.0;
@@ -156,7 +164,7 @@ __device__ double aug_entry(int r, int j, int n, int m, int dim, int phs, const 
         for (int d = 0; d < dim; d++)
             if (d != c)
                 t *= ipow(x0[d], e[d]);
-        return t / sc[c];
+        return t * sc[SC_INV + c];
     }
     double acc = 0.0;  // :252-289
     for (int k = 0; k < dim; k++) {
@@ -165,7 +173,7 @@ __device__ double aug_entry(int r, int j, int n, int m, int dim, int phs, const 
             for (int d = 0; d < dim; d++)
                 if (d != k)
                     t *= ipow(x0[d], e[d]);
-            acc += t / (sc[k] * sc[k]);
+            acc += t * (sc[SC_INV + k] * sc[SC_INV + k]);
         }
     }
     return acc;
@@ -203,14 +211,15 @@ __device__ void load_scaled_points(const StencilJob &J, int id, int n, double *s
         }
         if (tid == 0)
             for (int d = 0; d < dim; d++) {
-                sc[d] = hi[d] - lo[d];
-                sc[MAX_DIM + d] = lo[d];
+                sc[SC_SCALE + d] = hi[d] - lo[d];
+                sc[SC_MIN + d] = lo[d];
+                sc[SC_INV + d] = 1.0 / (hi[d] - lo[d]);
             }
     }
     sync();
     for (int k = tid; k < n * dim; k += nt) {
         int d = k % dim;
-        sp[k] = (sp[k] - sc[MAX_DIM + d]) / sc[d];
+        sp[k] = (sp[k] - sc[SC_MIN + d]) * sc[SC_INV + d];
     }
     sync();
 }
@@ -226,9 +235,10 @@ template <int G, int W, int GROUPS> struct GJShape {
     static constexpr int SMAX = W - 3;               // rows available (R >= 3)
     static constexpr int PTS = SMAX * MAX_DIM;
     // two pivot-row buffers (alternating steps) of W + 2 doubles each: element e of
-    // the pivot row sits at [e + 1], so elements 1, 2 / 3, 4 / ... are 16-byte pairs
+    // the pivot row sits at [e + 1], so elements 1, 2 / 3, 4 / ... are 16-byte pairs;
+    // [0] holds the reciprocal of the pivot
     static constexpr int PROW = (W + 3) / 2 * 2;
-    static constexpr int DOUBLES_RAW = PTS + 3 * MAX_DIM + SMAX * MAX_M + 2 * PROW + 4 * G + 4 * NT;
+    static constexpr int DOUBLES_RAW = PTS + SC_DOUBLES + SMAX * MAX_M + 2 * PROW + 4 * G + 4 * NT;
     static constexpr int DOUBLES = (DOUBLES_RAW + 1) / 2 * 2;
     // CTAs per SM the register allocation must allow (one-warp systems: 16 warps per
     // SM, two-warp systems: 10; the three-warp rows need their 255 registers)
@@ -247,12 +257,13 @@ template <int G, int W, int GROUPS> struct GJShape {
 template <int W>
 __device__ __forceinline__ void assemble_row(double (&a)[W], int r, int n, int m, int S, int R,
                                              int dim, int phs, const double *sp, const double *sc,
-                                             const double *pm, const double *xp, double *rhs) {
+                                             const double *pm, const double *xp,
+                                             const int *ex, double *rhs) {
     // this row's right-hand sides, through shared memory (a register copy would stay
     // live across the whole unrolled row)
     const bool node = r < n;
     for (int c = 0; c < R; c++)
-        rhs[c] = r < S ? aug_entry(r, S + c, n, m, dim, phs, sp, sc, xp) : 0.0;
+        rhs[c] = r < S ? aug_entry(r, S + c, n, m, dim, phs, sp, sc, ex, xp) : 0.0;
     double xr[MAX_DIM] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int d = 0; d < MAX_DIM; d++)
@@ -288,7 +299,8 @@ __device__ __forceinline__ void assemble_row(double (&a)[W], int r, int n, int m
 
 // one elimination step with the live width bounded by WC: rows drop their column
 // k (a[0]) and shift left; the pivot row itself is zeroed out of the update (l = 0).
-// pb holds pivot-row element e at pb[e + 1] (16-byte pairs from element 1 on).
+// pb holds pivot-row element e at pb[e + 1] (16-byte pairs from element 1 on) and the
+// pivot's reciprocal at pb[0].
 template <int W, int WC>
 __device__ __forceinline__ void gj_update(double (&a)[W], const double *pb, double l) {
 #pragma unroll
@@ -368,16 +380,16 @@ __device__ __forceinline__ void gj_chunks(double (&a)[W], GjRow &st, int S, int 
                 }
             }
             if (tid == p) {
+                pb[0] = 1.0 / a[0];  // the multiplier's reciprocal: one division per step
                 gj_publish<W, WC>(a, pb);
                 st.eligible = false;
                 st.my_step = k;
                 st.my_diag = a[0];
             }
             sync();
-            const double piv = pb[1];
             if (!(mx > 0.0))
                 st.singular = true;
-            const double l = (tid == p) ? 0.0 : a[0] / piv;
+            const double l = (tid == p) ? 0.0 : a[0] * pb[0];
             gj_update<W, WC>(a, pb, l);
         }
         gj_chunks<G, W, GROUPS, C + 1>(a, st, S, tid, lane, warp_in_grp, prow, amax, sync);
@@ -389,13 +401,13 @@ __global__ void __launch_bounds__(GJShape<G, W, GROUPS>::CTA, GJShape<G, W, GROU
     stencil_gj_kernel(StencilJob J) {
     using Sh = GJShape<G, W, GROUPS>;
     extern __shared__ __align__(16) double smem_raw[];
-    static_assert((Sh::PTS + 3 * MAX_DIM + Sh::SMAX * MAX_M) % 2 == 0,
+    static_assert((Sh::PTS + SC_DOUBLES + Sh::SMAX * MAX_M) % 2 == 0,
                   "pivot rows must start on a 16-byte boundary");
     const int grp = threadIdx.x / Sh::NT, tid = threadIdx.x % Sh::NT;
     const int lane = threadIdx.x & 31, warp_in_grp = tid >> 5;
     double *base = smem_raw + grp * Sh::DOUBLES;
     // sc: scales, minima, scaled probe (interpolation mode)
-    double *sp = base, *sc = sp + Sh::PTS, *pm = sc + 3 * MAX_DIM;
+    double *sp = base, *sc = sp + Sh::PTS, *pm = sc + SC_DOUBLES;
     double *prow = pm + Sh::SMAX * MAX_M, *amax = prow + 2 * Sh::PROW;
     double *rhs = amax + 4 * G + 4 * tid;
     auto sync = [&]() {
@@ -407,8 +419,12 @@ __global__ void __launch_bounds__(GJShape<G, W, GROUPS>::CTA, GJShape<G, W, GROU
             asm volatile("bar.sync %0, %1;\n" ::"r"(1 + grp), "r"(Sh::NT) : "memory");
     };
     const int dim = J.dim, m = J.m, R = J.probe ? 1 : dim + 1;
-    double *xp = J.probe ? sc + 2 * MAX_DIM : nullptr;
+    double *xp = J.probe ? sc + SC_PROBE : nullptr;
     __shared__ int s_item[GROUPS];
+    __shared__ int s_ex[MAX_M * MAX_DIM];
+    for (int q = threadIdx.x; q < MAX_M * MAX_DIM; q += blockDim.x)
+        s_ex[q] = c_exps[q];
+    __syncthreads();
     for (;;) {
         if (tid == 0)
             s_item[grp] = (int)atomicAdd(J.queue, 1u);
@@ -422,16 +438,17 @@ __global__ void __launch_bounds__(GJShape<G, W, GROUPS>::CTA, GJShape<G, W, GROU
         load_scaled_points(J, id, n, sp, sc, tid, Sh::NT, sync);
         if (xp) {  // the probe shifted and scaled with its stencil (:23-30)
             if (tid < dim)
-                xp[tid] = (J.probe[(size_t)id * dim + tid] - sc[MAX_DIM + tid]) / sc[tid];
+                xp[tid] = (J.probe[(size_t)id * dim + tid] - sc[SC_MIN + tid]) * sc[SC_INV + tid];
         }
-        // monomials of every node (the P block and its transpose)
+        // monomials of every node (the P block and its transpose); consecutive lanes
+        // take consecutive nodes of one monomial
         for (int q = tid; q < n * m; q += Sh::NT) {
-            const int i = q / m, pp = q - i * m;
-            pm[i * MAX_M + pp] = monomial(sp + i * dim, pp, dim);
+            const int pp = q / n, i = q - pp * n;
+            pm[i * MAX_M + pp] = monomial(sp + i * dim, pp, dim, s_ex);
         }
         sync();
         double a[W];
-        assemble_row<W>(a, tid, n, m, S, R, dim, J.phs, sp, sc, pm, xp, rhs);
+        assemble_row<W>(a, tid, n, m, S, R, dim, J.phs, sp, sc, pm, xp, s_ex, rhs);
         GjRow st{tid < S, false, -1, 1.0};
         gj_chunks<G, W, GROUPS, 0>(a, st, S, tid, lane, warp_in_grp, prow, amax, sync);
         const int my_step = st.my_step;
@@ -470,7 +487,7 @@ __global__ void __launch_bounds__(GJShape<G, W, GROUPS>::CTA, GJShape<G, W, GROU
 // One warp per system; A (S x S, leading dim LDA odd) in dynamic shared memory.
 struct CondSmem {
     int lda, s_max;
-    __host__ __device__ int doubles() const { return MAX_S * MAX_DIM + 2 * MAX_DIM + s_max * lda + 4 * s_max; }
+    __host__ __device__ int doubles() const { return MAX_S * MAX_DIM + SC_DOUBLES + s_max * lda + 4 * s_max; }
 };
 
 __device__ __forceinline__ double warp_max(double v) {
@@ -541,7 +558,7 @@ __device__ double norm1_warp(const double *v, int s, int lane) {
 
 __global__ void __launch_bounds__(32) stencil_cond_kernel(StencilJob J, CondSmem L) {
     extern __shared__ double sm[];
-    double *sp = sm, *sc = sp + MAX_S * MAX_DIM, *A = sc + 2 * MAX_DIM;
+    double *sp = sm, *sc = sp + MAX_S * MAX_DIM, *A = sc + SC_DOUBLES;
     double *v = A + L.s_max * L.lda, *t = v + L.s_max, *sg = t + L.s_max;
     int *perm = (int *)(sg + L.s_max);
     const int lane = threadIdx.x;
@@ -559,7 +576,7 @@ __global__ void __launch_bounds__(32) stencil_cond_kernel(StencilJob J, CondSmem
         load_scaled_points(J, id, n, sp, sc, lane, 32, sync);
         for (int q = lane; q < s * s; q += 32) {
             int r = q / s, j = q - r * s;
-            A[r * lda + j] = aug_entry(r, j, n, m, dim, J.phs, sp, sc);
+            A[r * lda + j] = aug_entry(r, j, n, m, dim, J.phs, sp, sc, c_exps);
         }
         for (int i = lane; i < s; i += 32)
             perm[i] = i;
