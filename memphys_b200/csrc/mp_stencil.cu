@@ -226,20 +226,31 @@ __device__ void load_scaled_points(const StencilJob &J, int id, int n, double *s
 
 // -------------------------------------------------------------- weights
 // One thread per matrix row of a group of G warps (S <= 32 G); GROUPS groups
-// per CTA work on independent systems.  Shared memory per group: points, scales
-// (+ scaled probe), the monomials of every node, the pivot row, the cross-warp
-// pivot candidates.
+// per CTA work on independent systems.  Shared memory per group (each region an
+// even number of doubles, so the pivot rows start on 16-byte boundaries): points,
+// the scale record, the monomials of every node, the node-pair table, the pivot
+// rows, the cross-warp pivot candidates, each thread's right-hand sides.
+constexpr int even2(int x) { return (x + 1) / 2 * 2; }
 template <int G, int W, int GROUPS> struct GJShape {
     static constexpr int NT = 32 * G;
     static constexpr int CTA = NT * GROUPS;
-    static constexpr int SMAX = W - 3;               // rows available (R >= 3)
-    static constexpr int PTS = SMAX * MAX_DIM;
+    static constexpr int SMAX = W - 3;               // rows of a weights system (R >= 3)
+    // nodes of any system of the class: S + R <= W and S <= 32 G with R >= 1, m >= 1
+    static constexpr int NMAX = (NT < W - 1 ? NT : W - 1) - 1;
+    static constexpr int NP = NMAX > SMAX ? NMAX : SMAX;  // point and monomial rows
     // two pivot-row buffers (alternating steps) of W + 2 doubles each: element e of
     // the pivot row sits at [e + 1], so elements 1, 2 / 3, 4 / ... are 16-byte pairs;
     // [0] holds the reciprocal of the pivot
     static constexpr int PROW = (W + 3) / 2 * 2;
-    static constexpr int DOUBLES_RAW = PTS + SC_DOUBLES + SMAX * MAX_M + 2 * PROW + 4 * G + 4 * NT;
-    static constexpr int DOUBLES = (DOUBLES_RAW + 1) / 2 * 2;
+    // the pair table r_ij^phs, packed upper triangle of up to NMAX nodes
+    static constexpr int TRI = NMAX * (NMAX - 1) / 2;
+    static constexpr int OFF_SC = even2(NP * MAX_DIM);
+    static constexpr int OFF_PM = OFF_SC + even2(SC_DOUBLES);
+    static constexpr int OFF_TRI = OFF_PM + even2(NP * MAX_M);
+    static constexpr int OFF_PROW = OFF_TRI + even2(TRI);
+    static constexpr int OFF_AMAX = OFF_PROW + 2 * PROW;
+    static constexpr int OFF_RHS = OFF_AMAX + 4 * G;
+    static constexpr int DOUBLES = even2(OFF_RHS + 4 * NT);
     // CTAs per SM the register allocation must allow (one-warp systems: 16 warps per
     // SM, two-warp systems: 10; the three-warp rows need their 255 registers)
     static constexpr int WARPS_TARGET = G == 1 ? 16 : (G == 2 ? 10 : 1);
@@ -247,43 +258,107 @@ template <int G, int W, int GROUPS> struct GJShape {
     // steps per chunk of the elimination: within a chunk the update runs over the
     // chunk's first live width, so the unrolled code stays ~W^2 / (2 CH) long
     static constexpr int CH = W <= 56 ? 4 : (W <= 84 ? 8 : 16);
-    static constexpr int NCH = (SMAX + CH - 1) / CH;
+    static constexpr int NCH = (W - 1 + CH - 1) / CH;  // covers every S < W
 };
+
+// Index of the pair (i, j), i < j < n, in the packed upper triangle of an n-node
+// stencil: row i holds j = i + 1 .. n - 1
+__device__ __forceinline__ int tri_index(int i, int j, int n) {
+    return i * n - i * (i + 1) / 2 + (j - i - 1);
+}
+
+// r_ij^phs of every node pair of the stencil, once per pair (the saddle matrix's
+// Phi block is symmetric): the pairs spread evenly over the group's nt threads
+// (consecutive packed indices per step of the loop), so every thread takes about
+// n (n - 1) / (2 nt) of the roots instead of its row's n - 1.
+__device__ __forceinline__ void pair_table(double *tri, int n, int dim, int phs, const double *sp,
+                                           int tid, int nt) {
+    const int np = n * (n - 1) / 2;
+    if (tid >= np)
+        return;
+    int i = 0, j = tid + 1;  // pair number tid
+    while (j >= n) {
+        ++i;
+        j = j - n + i + 1;
+    }
+    for (int q = tid; q < np; q += nt) {
+        double r2 = 0.0;
+        for (int d = 0; d < dim; d++) {
+            const double t = sp[i * dim + d] - sp[j * dim + d];
+            r2 = fma(t, t, r2);
+        }
+        tri[q] = rpow_odd(r2, phs);
+        j += nt;  // pair number q + nt
+        while (j >= n && i < n) {
+            ++i;
+            j = j - n + i + 1;
+        }
+    }
+}
+
+// The right-hand sides of node row r (:108-248): the basis' gradient and Laplacian
+// at the centre node 0, with one root of r^2 for all columns (phs >= 3)
+__device__ __forceinline__ void node_rhs(int r, int dim, int phs, const double *sp,
+                                         const double *sc, double *rhs) {
+    double r2 = 0.0, dk[MAX_DIM];
+    for (int d = 0; d < dim; d++) {
+        dk[d] = sp[r * dim + d] - sp[d];
+        r2 += dk[d] * dk[d];
+    }
+    const double rt = sqrt(r2);
+    // r^(phs - 2) and r^(phs - 4) for odd phs >= 3 from the one root, formed as
+    // rpow_odd forms them (the same products in the same order)
+    double rq2 = rt, rq4 = rt;
+    for (int i = 1; i < phs - 2; i += 2)
+        rq2 *= r2;
+    if (phs == 3)
+        rq4 = 1.0 / rt;
+    else
+        for (int i = 1; i < phs - 4; i += 2)
+            rq4 *= r2;
+    for (int c = 0; c < dim; c++)  // :124-125
+        rhs[c] = -phs * dk[c] * rq2 * sc[SC_INV + c];
+    double acc = 0.0;
+    if (fabs(r2) > 1e-14) {  // :229
+        for (int d = 0; d < dim; d++) {  // :231-248
+            double g = phs * phs * (dk[d] * dk[d]) * rq4;
+            g = g - 2.0 * phs * (dk[d] * dk[d]) * rq4;
+            g = g + phs * rq2;
+            acc += g * (sc[SC_INV + d] * sc[SC_INV + d]);
+        }
+    }
+    rhs[dim] = acc;
+}
 
 // The row of a thread: entries j < W of [A | B] for row r (coefficient_computations
 // .cpp:70-106 for A, :108-292 for B, :430-454 in interpolation mode), assembled in
-// registers: node-node entries from the scaled points, polynomial entries from the
-// group's monomial table, the right-hand sides from aug_entry.
+// registers: node-node entries from the group's pair table, polynomial entries from
+// its monomial table, the right-hand sides from their formulas.
 template <int W>
 __device__ __forceinline__ void assemble_row(double (&a)[W], int r, int n, int m, int S, int R,
                                              int dim, int phs, const double *sp, const double *sc,
-                                             const double *pm, const double *xp,
-                                             const int *ex, double *rhs) {
+                                             const double *pm, const double *tri,
+                                             const double *xp, const int *ex, double *rhs) {
     // this row's right-hand sides, through shared memory (a register copy would stay
     // live across the whole unrolled row)
     const bool node = r < n;
-    for (int c = 0; c < R; c++)
-        rhs[c] = r < S ? aug_entry(r, S + c, n, m, dim, phs, sp, sc, ex, xp) : 0.0;
-    double xr[MAX_DIM] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int d = 0; d < MAX_DIM; d++)
-        if (node && d < dim)
-            xr[d] = sp[r * dim + d];
+    if (node && !xp && phs >= 3)
+        node_rhs(r, dim, phs, sp, sc, rhs);
+    else
+        for (int c = 0; c < R; c++)
+            rhs[c] = r < S ? aug_entry(r, S + c, n, m, dim, phs, sp, sc, ex, xp) : 0.0;
     const int p = r - n;  // polynomial row index (r >= n)
+    // pair (r, j) in the packed table: tri_index(r, j, n) = tr + j above the diagonal,
+    // tri_index(j, r, n) = j n - (j (j + 3) / 2 + 1) + r below it
+    const int tr = r * n - r * (r + 1) / 2 - r - 1;
 #pragma unroll
     for (int j = 0; j < W; j++) {
         double v = 0.0;
         if (r < S) {
             if (j < n) {
                 if (node) {
-                    double r2 = 0.0;
-#pragma unroll
-                    for (int d = 0; d < MAX_DIM; d++)
-                        if (d < dim) {
-                            const double t = xr[d] - sp[j * dim + d];
-                            r2 = fma(t, t, r2);
-                        }
-                    v = (j == r) ? 0.0 : rpow_odd(r2, phs);
+                    const int q = j > r ? tr + j : j * n - (j * (j + 3) / 2 + 1) + r;
+                    v = j == r ? 0.0 : tri[q];
                 } else {
                     v = pm[j * MAX_M + p];
                 }
@@ -401,15 +476,14 @@ __global__ void __launch_bounds__(GJShape<G, W, GROUPS>::CTA, GJShape<G, W, GROU
     stencil_gj_kernel(StencilJob J) {
     using Sh = GJShape<G, W, GROUPS>;
     extern __shared__ __align__(16) double smem_raw[];
-    static_assert((Sh::PTS + SC_DOUBLES + Sh::SMAX * MAX_M) % 2 == 0,
-                  "pivot rows must start on a 16-byte boundary");
+    static_assert(Sh::OFF_PROW % 2 == 0, "pivot rows must start on a 16-byte boundary");
     const int grp = threadIdx.x / Sh::NT, tid = threadIdx.x % Sh::NT;
     const int lane = threadIdx.x & 31, warp_in_grp = tid >> 5;
     double *base = smem_raw + grp * Sh::DOUBLES;
     // sc: scales, minima, scaled probe (interpolation mode)
-    double *sp = base, *sc = sp + Sh::PTS, *pm = sc + SC_DOUBLES;
-    double *prow = pm + Sh::SMAX * MAX_M, *amax = prow + 2 * Sh::PROW;
-    double *rhs = amax + 4 * G + 4 * tid;
+    double *sp = base, *sc = base + Sh::OFF_SC, *pm = base + Sh::OFF_PM;
+    double *tri = base + Sh::OFF_TRI, *prow = base + Sh::OFF_PROW, *amax = base + Sh::OFF_AMAX;
+    double *rhs = base + Sh::OFF_RHS + 4 * tid;
     auto sync = [&]() {
         if (G == 1)
             __syncwarp();
@@ -446,9 +520,10 @@ __global__ void __launch_bounds__(GJShape<G, W, GROUPS>::CTA, GJShape<G, W, GROU
             const int pp = q / n, i = q - pp * n;
             pm[i * MAX_M + pp] = monomial(sp + i * dim, pp, dim, s_ex);
         }
+        pair_table(tri, n, dim, J.phs, sp, tid, Sh::NT);
         sync();
         double a[W];
-        assemble_row<W>(a, tid, n, m, S, R, dim, J.phs, sp, sc, pm, xp, s_ex, rhs);
+        assemble_row<W>(a, tid, n, m, S, R, dim, J.phs, sp, sc, pm, tri, xp, s_ex, rhs);
         GjRow st{tid < S, false, -1, 1.0};
         gj_chunks<G, W, GROUPS, 0>(a, st, S, tid, lane, warp_in_grp, prow, amax, sync);
         const int my_step = st.my_step;
