@@ -649,9 +649,44 @@ __global__ void __launch_bounds__(32) stencil_cond_kernel(StencilJob J, CondSmem
         const int id = sys_id(J, tt);
         const int n = sys_n(J, id), s = n + m;
         load_scaled_points(J, id, n, sp, sc, lane, 32, sync);
-        for (int q = lane; q < s * s; q += 32) {
-            int r = q / s, j = q - r * s;
-            A[r * lda + j] = aug_entry(r, j, n, m, dim, J.phs, sp, sc, c_exps);
+        // the saddle matrix (aug_entry's A block): r^phs once per node pair, written
+        // to both triangles; zero diagonal; the monomials, one per lane and step of a
+        // single monomial index (uniform constant-memory reads), to P and P^T; zero
+        // polynomial block
+        {
+            const int np = n * (n - 1) / 2;
+            int i = 0, j = lane + 1;
+            while (j >= n && i < n) {
+                ++i;
+                j = j - n + i + 1;
+            }
+            for (int q = lane; q < np; q += 32) {
+                double r2 = 0.0;
+                for (int d = 0; d < dim; d++) {
+                    const double tq = sp[i * dim + d] - sp[j * dim + d];
+                    r2 += tq * tq;
+                }
+                const double v = rpow_odd(r2, J.phs);
+                A[i * lda + j] = v;
+                A[j * lda + i] = v;
+                j += 32;
+                while (j >= n && i < n) {
+                    ++i;
+                    j = j - n + i + 1;
+                }
+            }
+        }
+        for (int i = lane; i < n; i += 32)
+            A[i * lda + i] = 0.0;
+        for (int q = lane; q < n * m; q += 32) {
+            const int pp = q / n, i = q - pp * n;
+            const double v = monomial(sp + i * dim, pp, dim, c_exps);
+            A[i * lda + n + pp] = v;
+            A[(n + pp) * lda + i] = v;
+        }
+        for (int q = lane; q < m * m; q += 32) {
+            const int a = q / m, b = q - a * m;
+            A[(n + a) * lda + n + b] = 0.0;
         }
         for (int i = lane; i < s; i += 32)
             perm[i] = i;
