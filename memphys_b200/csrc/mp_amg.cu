@@ -893,6 +893,19 @@ __device__ __forceinline__ void spmv_pair(const EllView<V> &A, int w, int lane,
         a1 = (T)v.y * s1;
         k0 = 1;
     }
+    if (!DIFF && A.dslice && A.dslice[w]) {  // 16-bit column deltas (warp-uniform)
+        const int i0 = w * SLICE + 2 * lane;
+#pragma unroll 4
+        for (int k = 0; k < K; k++) {
+            const size_t o = base + (size_t)k * SLICE;
+            const short2 c = ldop<EVF>(reinterpret_cast<const short2 *>(A.dcols + o));
+            const V2 v = ldop<EVF>(reinterpret_cast<const V2 *>(A.vals + o));
+            const T x0 = __ldg(x + i0 + c.x), x1 = __ldg(x + i0 + 1 + c.y);
+            a0 = fma((T)v.x, x0, a0);
+            a1 = fma((T)v.y, x1, a1);
+        }
+        return;
+    }
 #pragma unroll 4
     for (int k = k0; k < K; k++) {
         const size_t o = base + (size_t)k * SLICE;

@@ -75,6 +75,52 @@ int ell_make_fp32(Ell &E, cudaStream_t s) {
     return MP_OK;
 }
 
+// one warp per slice: does every column - row of the slice fit 16 bits?  If so the
+// deltas are written and the slice's flag set
+__global__ void k_ell_deltas(int nrows, int K, const int *cols, short *d, unsigned char *flag,
+                             unsigned *count) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int nsl = (nrows + SLICE - 1) / SLICE;
+    if (w >= nsl)
+        return;
+    const size_t base = (size_t)w * K * SLICE;
+    bool fits = true;
+    for (int t = lane; t < K * SLICE; t += 32) {
+        const int row = w * SLICE + (t % SLICE);
+        const int dl = cols[base + t] - row;
+        fits = fits && dl >= -32768 && dl <= 32767;
+    }
+    fits = __all_sync(0xffffffffu, fits);
+    if (fits)
+        for (int t = lane; t < K * SLICE; t += 32)
+            d[base + t] = (short)(cols[base + t] - (w * SLICE + (t % SLICE)));
+    if (lane == 0) {
+        flag[w] = fits ? 1 : 0;
+        if (fits)
+            atomicAdd(count, 1u);
+    }
+}
+
+int ell_make_deltas(Ell &E, cudaStream_t s, double *frac) {
+    if (E.soff.p || !E.cols.p)
+        return fail(MP_BAD_ARG, "ell_make_deltas: uniform-width operators only");
+    const int nsl = (E.nrows + SLICE - 1) / SLICE;
+    MP_TRY(E.dcols.alloc(E.cols.n));
+    MP_TRY(E.dslice.alloc(nsl));
+    dbuf<unsigned> cnt;
+    MP_TRY(cnt.alloc(1));
+    MP_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned), s));
+    k_ell_deltas<<<(unsigned)((nsl + 7) / 8), 256, 0, s>>>(E.nrows, E.K, E.cols.p, E.dcols.p,
+                                                           E.dslice.p, cnt.p);
+    MP_CHECK_LAUNCH();
+    unsigned h = 0;
+    MP_CUDA(cudaMemcpyAsync(&h, cnt.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    MP_CUDA(cudaStreamSynchronize(s));
+    if (frac)
+        *frac = nsl ? (double)h / nsl : 0.0;
+    return MP_OK;
+}
+
 // y = alpha*A x + beta*y, one warp per 64-row slice, two rows per lane
 template <class T>
 __global__ void __launch_bounds__(256)

@@ -34,6 +34,11 @@ template <class T> struct EllView {
     // FP32 operators may also carry (column, value bits) pairs in the same sliced
     // order: one 16-byte load then fetches both entries of a lane's two rows
     const int2 *pk = nullptr;
+    // FP64 operators may also carry 16-bit column deltas (column - row) in the same
+    // sliced order, used in the slices whose flag dslice[s] is set (every delta of the
+    // slice fits): 2 bytes instead of 4 per entry on the index stream
+    const short *dcols = nullptr;
+    const unsigned char *dslice = nullptr;
 };
 
 // start offset and width of slice w
@@ -56,8 +61,12 @@ struct Ell {
     dbuf<double> v64;
     dbuf<float> v32;
     dbuf<int> soff;
+    dbuf<short> dcols;             // 16-bit column deltas (ell_make_deltas)
+    dbuf<unsigned char> dslice;    // per slice: 1 when its deltas are used
     size_t entries() const { return v64.p ? v64.n : (v32.p ? v32.n : cols.n); }
-    EllView<double> view64() const { return {nrows, ncols, K, cols.p, v64.p, soff.p}; }
+    EllView<double> view64() const {
+        return {nrows, ncols, K, cols.p, v64.p, soff.p, nullptr, dcols.p, dslice.p};
+    }
     EllView<float> view32() const { return {nrows, ncols, K, cols.p, v32.p, soff.p}; }
 };
 
@@ -66,6 +75,11 @@ int ell_create(Ell &E, int nrows, int ncols, int K, const int *cols, const doubl
                bool fp32, cudaStream_t s);
 // Convert existing FP64 values to an FP32 copy on the device.
 int ell_make_fp32(Ell &E, cudaStream_t s);
+// 16-bit column deltas of a uniform-width operator, per slice where all of them fit
+// (stencils are local in a node-ordered cloud; slices that reach far nodes, such as
+// boundary nodes numbered last, keep their 32-bit columns).  Returns the fraction of
+// slices that use deltas in *frac (nullable).
+int ell_make_deltas(Ell &E, cudaStream_t s, double *frac = nullptr);
 
 // up to 4 value arrays sharing one column structure (mp_op_apply_multi)
 template <class T> struct MultiVals {

@@ -51,6 +51,25 @@ __device__ __forceinline__ void ell_pair(const EllView<T> &A, int w, int lane,
             return;
         }
     }
+    if (A.dslice && A.dslice[w]) {  // 16-bit column deltas (warp-uniform)
+        const int i0 = w * SLICE + 2 * lane;
+        const T *xr0 = x + i0, *xr1 = x + i0 + 1;
+        short2 d = __ldcs(reinterpret_cast<const short2 *>(A.dcols + base));
+        V2 v = __ldcs(reinterpret_cast<const V2 *>(A.vals + base));
+        xs0 = __ldg(xr0 + d.x);
+        xs1 = __ldg(xr1 + d.y);
+        a0 = v.x * xs0;
+        a1 = v.y * xs1;
+#pragma unroll 4
+        for (int k = 1; k < K; k++) {
+            const size_t o = base + (size_t)k * SLICE;
+            d = __ldcs(reinterpret_cast<const short2 *>(A.dcols + o));
+            v = __ldcs(reinterpret_cast<const V2 *>(A.vals + o));
+            a0 = fma(v.x, __ldg(xr0 + d.x), a0);
+            a1 = fma(v.y, __ldg(xr1 + d.y), a1);
+        }
+        return;
+    }
     int2 c = __ldcs(reinterpret_cast<const int2 *>(A.cols + base));
     V2 v = __ldcs(reinterpret_cast<const V2 *>(A.vals + base));
     xs0 = __ldg(x + c.x);
@@ -956,6 +975,9 @@ int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet
         MP_TRY(ell_make_fp32(sys.A, st));
         MP_TRY(ell_diff32(sys.A, sys.d32, sys.dpk, st));
     }
+    // 16-bit column deltas where the stencils are local (the FP64 SpMVs of the Krylov
+    // iteration and of the multigrid's finest level read them)
+    MP_TRY(ell_make_deltas(sys.A, st));
     MP_TRY(sys.dinv.alloc(nv));
     if (mixed)
         MP_TRY(sys.dinv32.alloc(nv));
