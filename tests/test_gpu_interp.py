@@ -48,6 +48,23 @@ def test_interp_matches_oracle_and_reproduces_cubics(mp_lib, make, n, np_):
         assert abs(w[k][cols[k] == j][0] - 1.0) <= 1e-9
 
 
+@pytest.mark.parametrize("n,poly", [(40, 1), (39, 1), (33, 3)])
+def test_interp_largest_systems_of_a_class(mp_lib, n, poly):
+    """Interpolation systems have one right-hand side, so a register-width class holds
+    up to W - 1 rows (here n + m = 42-43 in the 44-wide class), two more than a
+    weights system of the same class: every elimination step and every stencil point
+    must still be there (the oracle solves the same systems with LAPACK)."""
+    cl = clouds.cavity_2d(30, seed=4)
+    rng = np.random.default_rng(11)
+    probe = rng.uniform(0.05, 0.95, size=(200, 2))
+    cols, w = interp(cl.xyz, probe, n, poly=poly)
+    rc, rw = oracle.interp_matrix(cl.xyz, probe, n, poly_deg=poly)
+    assert np.array_equal(cols, rc)
+    scale = np.abs(rw).max(1, keepdims=True)
+    assert np.all(np.abs(w - rw) <= 1e-9 * scale)
+    assert np.abs(w.sum(1) - 1.0).max() <= 1e-9  # constants are reproduced
+
+
 def test_interp_rejects_bad_arguments(mp_lib):
     cl = clouds.cavity_2d(10, seed=1)
     probe = np.array([[0.5, 0.5]])
