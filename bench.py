@@ -586,12 +586,36 @@ def integrators(args, cl, cld, prm, pts):
         o = [np.zeros((nv, N)) for _ in range(4)]
         fsf.single_timestep(*o, *g, 0)
         g = [a.copy() for a in o]
+        # end to end through the Python mirror: host (nv, N) arrays, transposed to the
+        # C ABI's plane-contiguous (Eigen column-major) layout and back on the host
         with capi.Timer(None) as tm:
             for k in range(K):
                 fsf.single_timestep(*o, *g, 1 + k)
                 g = [a.copy() for a in o]
+        e2e_ms = tm.ms / K
+        # device-resident through the C ABI: plane-contiguous device fields, ping-pong
+        import ctypes as C
+        L = capi.lib()
+        stream = capi.Stream()
+        dev = [[capi.DeviceArray.from_host(np.ascontiguousarray(a.T)) for a in g],
+               [capi.DeviceArray((N, nv)) for _ in range(4)]]
+
+        def dstep(k, a, b):
+            vo = (C.c_void_p * 3)(*[dev[a][i].ptr for i in range(3)])
+            vn = (C.c_void_p * 3)(*[dev[b][i].ptr for i in range(3)])
+            capi.check(L.mp_fsf_single_timestep(fsf.handle, vo, C.c_void_p(dev[a][3].ptr), vn,
+                                                C.c_void_p(dev[b][3].ptr), k, stream.handle),
+                       "mp_fsf_single_timestep")
+        dstep(1 + K, 0, 1)
+        with capi.Timer(stream.handle) as tm:
+            for k in range(K):
+                dstep(2 + K + k, (k + 1) % 2, k % 2)
         return {"ms_per_step": round(tm.ms / K, 3), "steps": K, "planes": N,
                 "unknowns_per_field": nv * N, "setup_s": round(t_setup, 2),
+                "ms_per_step_host_arrays": round(e2e_ms, 3),
+                "timing": "device fields through mp_fsf_single_timestep (ms_per_step); host "
+                          "(nv, N) arrays through the Python mirror, which transposes them to "
+                          "the plane-contiguous layout and back (ms_per_step_host_arrays)",
                 "w_max": float(np.abs(g[2]).max())}
 
     for name, fn in (("semi_implicit", semi_implicit), ("scalar_transport", scalar_transport),

@@ -256,17 +256,22 @@ struct mp_fsf_s {
     dbuf<double> phys[4], uphi, vphi, xy, z, ft[4];
     bool started = false;
     bool use_graph = true;
+    // the modes' pressure solves are independent (each mode has its own system,
+    // hierarchy and Krylov vectors): one stream per mode, joined after the solves;
+    // each solve's final scalars are kept (real, imaginary) for the status check
+    std::vector<cudaStream_t> ms;
+    std::vector<cudaEvent_t> mev;
+    cudaEvent_t fork = nullptr;
+    dbuf<BicgScalars> stats;
+    ~mp_fsf_s() {
+        for (cudaStream_t x : ms)
+            cudaStreamDestroy(x);
+        for (cudaEvent_t e : mev)
+            cudaEventDestroy(e);
+        if (fork)
+            cudaEventDestroy(fork);
+    }
 };
-
-static int fsf_solve(Ppe &S, bool graph, cudaStream_t st) {
-    MP_TRY(S.solve_resident(st, graph));
-    SolveStats ss;
-    MP_TRY(S.read_stats(st, &ss));
-    if (ss.status != MP_OK)
-        return fail(ss.status, "Fourier pressure solve: status %d after %d iterations, relres %g",
-                    ss.status, ss.iters, ss.relres);
-    return MP_OK;
-}
 
 extern "C" int mp_fsf_create(mp_cloud c, const uint8_t *boundary, const double *normal,
                              const uint8_t *u_dir, const uint8_t *v_dir, const uint8_t *w_dir,
@@ -334,6 +339,15 @@ extern "C" int mp_fsf_create(mp_cloud c, const uint8_t *boundary, const double *
         MP_CUDA(cudaMemset(p->W.x.p, 0, sizeof(double) * p->sys.nsys));
     }
     f->bordered0 = f->P[0]->sys.bordered;
+    f->ms.resize(M, nullptr);
+    f->mev.resize(M, nullptr);
+    for (int iw = 0; iw < M; iw++) {
+        MP_CUDA(cudaStreamCreateWithFlags(&f->ms[iw], cudaStreamNonBlocking));
+        MP_CUDA(cudaEventCreateWithFlags(&f->mev[iw], cudaEventDisableTiming));
+    }
+    MP_CUDA(cudaEventCreateWithFlags(&f->fork, cudaEventDisableTiming));
+    if ((rc = f->stats.alloc((size_t)2 * M)) != MP_OK)
+        return bail(rc);
     if ((rc = f->cn.alloc((size_t)2 * M)) != MP_OK)
         return bail(rc);
     for (dbuf<uint8_t> *b : {&f->udir, &f->vdir, &f->wdir, &f->pdir})
@@ -462,22 +476,49 @@ extern "C" int mp_fsf_single_timestep(mp_fsf f, const double *const *vel_old, co
     double bmax = 0.0;
     for (double v : cn)
         bmax = std::max(bmax, v);
+    // the modes' solves concurrently, one stream per mode (real then imaginary part of a
+    // mode on its stream: they share its Krylov vectors)
+    MP_CUDA(cudaEventRecord(f->fork, st));
     for (int iw = 0; iw < M; iw++) {
         Ppe &S = *f->P[iw];
-        MP_TRY(S.set_abs_tol(S.cfg.tol * std::sqrt(bmax), st));
+        cudaStream_t ms = f->ms[iw];
+        MP_CUDA(cudaStreamWaitEvent(ms, f->fork, 0));
+        MP_TRY(S.set_abs_tol(S.cfg.tol * std::sqrt(bmax), ms));
         const size_t o = (size_t)iw * nv, vb = sizeof(double) * nv;
         const bool border = S.sys.nsys == nv + 1;
         for (int q = 0; q < (border ? 1 : 2); q++) {  // the bordered mode solves its real part
-            MP_CUDA(cudaMemcpyAsync(S.W.b64.p, f->ps[q].p + o, vb, cudaMemcpyDeviceToDevice, st));
-            MP_CUDA(cudaMemcpyAsync(S.W.x.p, f->f[3][q].p + o, vb, cudaMemcpyDeviceToDevice, st));
+            MP_CUDA(cudaMemcpyAsync(S.W.b64.p, f->ps[q].p + o, vb, cudaMemcpyDeviceToDevice, ms));
+            MP_CUDA(cudaMemcpyAsync(S.W.x.p, f->f[3][q].p + o, vb, cudaMemcpyDeviceToDevice, ms));
             if (border)  // the source's border entry is 0; the multiplier keeps its last value
-                MP_CUDA(cudaMemsetAsync(S.W.b64.p + nv, 0, sizeof(double), st));
-            MP_TRY(fsf_solve(S, f->use_graph, st));
+                MP_CUDA(cudaMemsetAsync(S.W.b64.p + nv, 0, sizeof(double), ms));
+            MP_TRY(S.solve_resident(ms, f->use_graph));
+            MP_CUDA(cudaMemcpyAsync(f->stats.p + 2 * iw + q, S.W.scal.p, sizeof(BicgScalars),
+                                    cudaMemcpyDeviceToDevice, ms));
             // the new pressure coefficients go to ft[q] (mode iw), kept apart from the old
-            MP_CUDA(cudaMemcpyAsync(f->ft[q].p + o, S.W.x.p, vb, cudaMemcpyDeviceToDevice, st));
+            MP_CUDA(cudaMemcpyAsync(f->ft[q].p + o, S.W.x.p, vb, cudaMemcpyDeviceToDevice, ms));
         }
         if (border)  // the first mode's imaginary part stays 0
-            MP_CUDA(cudaMemsetAsync(f->ft[1].p + o, 0, vb, st));
+            MP_CUDA(cudaMemsetAsync(f->ft[1].p + o, 0, vb, ms));
+        MP_CUDA(cudaEventRecord(f->mev[iw], ms));
+        MP_CUDA(cudaStreamWaitEvent(st, f->mev[iw], 0));
+    }
+    {  // every solve's status, as Ppe::read_stats judges it
+        std::vector<BicgScalars> hs((size_t)2 * M);
+        MP_CUDA(cudaMemcpyAsync(hs.data(), f->stats.p, sizeof(BicgScalars) * 2 * M,
+                                cudaMemcpyDeviceToHost, st));
+        MP_CUDA(cudaStreamSynchronize(st));
+        for (int iw = 0; iw < M; iw++) {
+            const Ppe &S = *f->P[iw];
+            for (int q = 0; q < (S.sys.nsys == nv + 1 ? 1 : 2); q++) {
+                SolveStats ss;
+                S.stats_of(hs[2 * iw + q], &ss);
+                if (ss.status != MP_OK)
+                    return fail(ss.status,
+                                "Fourier pressure solve (mode %d, %s part): status %d after %d "
+                                "iterations, relres %g", iw, q ? "imaginary" : "real",
+                                ss.status, ss.iters, ss.relres);
+            }
+        }
     }
     const double *pr = f->ft[0].p, *pi = f->ft[1].p;
     // calc_vel_corr: the new velocity coefficients go to scratch (nv x N >= nv x M)

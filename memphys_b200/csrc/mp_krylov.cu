@@ -891,6 +891,11 @@ int Ppe::read_stats(cudaStream_t st, SolveStats *out) {
     BicgScalars hs;
     MP_CUDA(cudaMemcpyAsync(&hs, W.scal.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
     MP_CUDA(cudaStreamSynchronize(st));
+    stats_of(hs, out);
+    return MP_OK;
+}
+
+void Ppe::stats_of(const BicgScalars &hs, SolveStats *out) const {
     out->iters = cfg.precision != MP_FP32 ? hs.it : hs.total_inner;
     out->outer = hs.outer_it;
     out->abs_res = std::sqrt(hs.rr_true);
@@ -901,7 +906,6 @@ int Ppe::read_stats(cudaStream_t st, SolveStats *out) {
         out->status = MP_NOT_CONVERGED;
     if (hs.status == MP_OK && !std::isfinite(out->relres))
         out->status = MP_NAN_DETECTED;
-    return MP_OK;
 }
 
 int Ppe::set_abs_tol(double atol, cudaStream_t st) {

@@ -77,6 +77,8 @@ struct Ppe {
     // solve with W.b64 as rhs and W.x as initial guess / solution
     int solve_resident(cudaStream_t st, bool use_graph);
     int read_stats(cudaStream_t st, SolveStats *out);
+    // the same judgement of a solve's final scalars already on the host
+    void stats_of(const BicgScalars &hs, SolveStats *out) const;
     cudaStream_t cap_stream();
 };
 
