@@ -1028,6 +1028,85 @@ __global__ void __launch_bounds__(256)
         level_epilogue<T, EP>(row, acc, b, dinv, d, x, y, c);
 }
 
+// sliced ELL with the slice's entries split over the CTA's 8 warps: one 64-row slice
+// per CTA, warp q takes entries k = q, q + 8, ... of both rows of every lane, the
+// partial sums meet in shared memory and warp 0 adds them in warp order and runs the
+// epilogue.  For coarse levels whose slices are few and wide (level 1: 2,007 slices
+// of ~35-50 entries), where one warp per slice leaves the GPU a fifth full and a
+// lane's entries form a long dependent chain.
+template <class T, class V, bool DIFF, bool EVF, int EP>
+__global__ void __launch_bounds__(256)
+    k_level_ks(EllView<V> M, const T *__restrict__ u, const T *__restrict__ b,
+               const T *__restrict__ dinv, T *d, T *x, T *y, ChebC c, const int *done) {
+    using V2 = typename V2a<V>::type;
+    __shared__ T red[8][SLICE];
+    pdl_wait();
+    pdl_trigger();
+    if (*done)
+        return;
+    const int w = blockIdx.x, q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    size_t base;
+    int K;
+    slice_span(M, w, base, K);
+    base += 2 * lane;
+    const int i0 = w * SLICE + 2 * lane;
+    T a0 = 0, a1 = 0, s0 = 0, s1 = 0;
+    if (DIFF) {  // the self entry (k = 0) holds the row sum; the others take u_j - u_i
+        s0 = i0 < M.nrows ? __ldg(u + i0) : T(0);
+        s1 = i0 + 1 < M.nrows ? __ldg(u + i0 + 1) : T(0);
+    }
+    bool packed = false;
+    if constexpr (sizeof(V) == 4) {
+        if (M.pk) {
+            packed = true;
+            const int4 *P = reinterpret_cast<const int4 *>(M.pk + base);
+#pragma unroll 2
+            for (int k = q; k < K; k += 8) {
+                const int4 e = ldop<EVF>(P + (size_t)k * (SLICE / 2));
+                const T g0 = __ldg(u + e.x), g1 = __ldg(u + e.z);
+                if (DIFF && k == 0) {
+                    a0 = fma((T)__int_as_float(e.y), s0, a0);
+                    a1 = fma((T)__int_as_float(e.w), s1, a1);
+                } else {
+                    a0 = fma((T)__int_as_float(e.y), DIFF ? g0 - s0 : g0, a0);
+                    a1 = fma((T)__int_as_float(e.w), DIFF ? g1 - s1 : g1, a1);
+                }
+            }
+        }
+    }
+    if (!packed) {
+#pragma unroll 2
+        for (int k = q; k < K; k += 8) {
+            const size_t o = base + (size_t)k * SLICE;
+            const int2 cl = ldop<EVF>(reinterpret_cast<const int2 *>(M.cols + o));
+            const V2 v = ldop<EVF>(reinterpret_cast<const V2 *>(M.vals + o));
+            const T g0 = __ldg(u + cl.x), g1 = __ldg(u + cl.y);
+            if (DIFF && k == 0) {
+                a0 = fma((T)v.x, s0, a0);
+                a1 = fma((T)v.y, s1, a1);
+            } else {
+                a0 = fma((T)v.x, DIFF ? g0 - s0 : g0, a0);
+                a1 = fma((T)v.y, DIFF ? g1 - s1 : g1, a1);
+            }
+        }
+    }
+    red[q][2 * lane] = a0;
+    red[q][2 * lane + 1] = a1;
+    __syncthreads();
+    if (q != 0)
+        return;
+    T t0 = 0, t1 = 0;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        t0 += red[r][2 * lane];
+        t1 += red[r][2 * lane + 1];
+    }
+    if (i0 < M.nrows)
+        level_epilogue<T, EP>(i0, t0, b, dinv, d, x, y, c);
+    if (i0 + 1 < M.nrows)
+        level_epilogue<T, EP>(i0 + 1, t1, b, dinv, d, x, y, c);
+}
+
 // d = dinv b / theta (start of the pre-smoother from a zero guess)
 template <class T>
 __global__ void k_cheb_start(int n, const T *b, const T *dinv, T *d, T inv_theta, const int *done) {
@@ -1134,7 +1213,8 @@ static int level_op(int mode, const EllView<V> &E, const CsrView<V> &Cv, const T
     case 1: e = launch_pdl(k_level_csr<T, V, 4, DIFF, EVF, EP>, dim3((unsigned)((n * 4 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
     case 2: e = launch_pdl(k_level_csr<T, V, 8, DIFF, EVF, EP>, dim3((unsigned)((n * 8 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
     case 3: e = launch_pdl(k_level_csr<T, V, 16, DIFF, EVF, EP>, dim3((unsigned)((n * 16 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
-    default: e = launch_pdl(k_level_csr<T, V, 32, DIFF, EVF, EP>, dim3((unsigned)(((size_t)n * 32 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
+    case 4: e = launch_pdl(k_level_csr<T, V, 32, DIFF, EVF, EP>, dim3((unsigned)(((size_t)n * 32 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
+    default: e = launch_pdl(k_level_ks<T, V, DIFF, EVF, EP>, dim3((unsigned)((n + SLICE - 1) / SLICE)), blk, s, E, u, b, dinv, d, x, y, c, done); break;
     }
     if (e != cudaSuccess)
         return fail(MP_CUDA_ERROR, "multigrid launch: %s", cudaGetErrorString(e));
@@ -1335,7 +1415,7 @@ static int tune_one(size_t l, const EllView<V> &E, const CsrView<V> &Cv, int nco
     constexpr int REPS = 5;
     float best = 1e30f;
     int rc = MP_OK;
-    for (int mode = sell ? 0 : 1; mode <= 4 && rc == MP_OK; mode++) {
+    for (int mode = sell ? 0 : 1; mode <= (sell ? 5 : 4) && rc == MP_OK; mode++) {
         float t[REPS];
         for (int rep = 0; rep < REPS && rc == MP_OK; rep++) {
             cudaMemsetAsync(flush.p, rep & 0xff, flush.n, s);

@@ -32,10 +32,11 @@ struct DCsr {
 };
 
 // kernel schedule of one operator, chosen by the setup-time autotuner:
-// 0 = sliced ELL (2 rows per lane), 1..4 = CSR with 4, 8, 16, 32 lanes per row
+// 0 = sliced ELL (2 rows per lane), 1..4 = CSR with 4, 8, 16, 32 lanes per row,
+// 5 = sliced ELL with each slice's entries split over a CTA's 8 warps
 struct OpSched {
     int mode = 0;
-    float us[5] = {0, 0, 0, 0, 0};
+    float us[6] = {0, 0, 0, 0, 0, 0};
 };
 
 struct AmgLevel {
