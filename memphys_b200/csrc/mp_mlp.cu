@@ -237,7 +237,10 @@ __global__ void __launch_bounds__(128 * MLP_WG, 1) k_mlp_forward(MlpFwdArgs A) {
     uint32_t phase = 0;
     bool ok = true;
     const int ntiles = (A.n + MLP_TILE - 1) / MLP_TILE;
+    // tiles interleaved over the CTAs (tile = wg * grid + cta): a batch of fewer tiles
+    // than SMs gets one CTA per tile instead of sharing a few SMs' tensor cores
     const int stride = gridDim.x * MLP_WG;
+    const int first = wg * gridDim.x + blockIdx.x;
     // this thread's 128-byte feature row of tile t (zeros past the end)
     auto load_row = [&](int t, uint4 (&f)[MLP_IN / 8]) {
         const int r = t * MLP_TILE + tid;
@@ -249,8 +252,8 @@ __global__ void __launch_bounds__(128 * MLP_WG, 1) k_mlp_forward(MlpFwdArgs A) {
             f[c] = lv ? xr[c] : make_uint4(0, 0, 0, 0);
     };
     uint4 feat[MLP_IN / 8];
-    load_row(blockIdx.x * MLP_WG + wg, feat);
-    for (int tile = blockIdx.x * MLP_WG + wg; tile < ntiles; tile += stride) {
+    load_row(first, feat);
+    for (int tile = first; tile < ntiles; tile += stride) {
         const int row = tile * MLP_TILE + tid;
         const bool live = row < A.n;
         // ---- this thread's feature row into the A operand; the next tile's row is
@@ -833,7 +836,7 @@ template <int MODE> static int launch_forward(MlpFwdArgs &a, cudaStream_t s) {
     const int sm = fwd_smem();
     MP_CUDA(cudaFuncSetAttribute(k_mlp_forward<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     const int tiles = (a.n + MLP_TILE - 1) / MLP_TILE;
-    const int grid = std::max(1, std::min((tiles + MLP_WG - 1) / MLP_WG, sm_count()));
+    const int grid = std::max(1, std::min(tiles, sm_count()));
     k_mlp_forward<MODE><<<grid, 128 * MLP_WG, sm, s>>>(a);
     MP_CHECK_LAUNCH();
     return MP_OK;
