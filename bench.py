@@ -435,7 +435,8 @@ def run_ours(args, ws, rank, local, pg):
         "solver": "BiCGSTAB + smoothed-aggregation multigrid on the GPU, FP64",
         "pressure_iters_per_step": float(iters64.mean()),
         "max_relres": float(log64[:, 1].max()),
-        # the north star's comparison, after the spin-up (variants: every configuration)
+        # learned + mixed precision against plain FP64, after the spin-up (variants: every
+        # configuration)
         "learned_mixed_speedup_vs_plain_fp64": lm.get("speedup_vs_plain_fp64"),
         "learned_vs_projected": (round(pj["ms_per_step"] / lg_["ms_per_step"], 3)
                                  if pj and lg_ else None),
