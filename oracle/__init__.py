@@ -1,7 +1,7 @@
 """CPU oracle for the MeMPhyS hot path -- TEST INFRASTRUCTURE ONLY.
 
-This package is the checker the CUDA product path is compared against and the
-CPU baseline that ``bench.py`` times beside the GPU.  It is imported only by
+This package is what the CUDA product path is compared against in the tests, and
+the CPU baseline that ``bench.py`` times beside the GPU.  It is imported only by
 ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s cpu-baseline leg;
 nothing under ``memphys_b200/`` imports it.
 

@@ -1,8 +1,8 @@
 /*
  * memphys_oracle.c -- CPU FP64 restatement of the MeMPhyS hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA product
- * path (memphys_b200/csrc) is compared against, and the CPU baseline that
+ * TEST INFRASTRUCTURE ONLY.  This file is what the tests compare the CUDA
+ * product path (memphys_b200/csrc) against, and the CPU baseline that
  * bench.py times beside the GPU.  Nothing in the product links or calls it.
  *
  * Reference paths below are relative to "MeMPhyS Latest Version/" of
