@@ -100,7 +100,7 @@ int mp_device_info(int *sm, int *major, int *minor, size_t *total_mem) {
     if (total_mem)
         *total_mem = p.totalGlobalMem;
     if (p.major != 10)
-        return fail(MP_NO_DEVICE, "device is sm_%d%d; this build runs on sm_100 (B200) only",
+        return fail(MP_NO_DEVICE, "device is sm_%d%d; the library is compiled for sm_100a (B200) only",
                     p.major, p.minor);
     return MP_OK;
 }
