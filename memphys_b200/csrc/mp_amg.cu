@@ -565,6 +565,99 @@ int ell_diff32(const Ell &A0, dbuf<float> &v32, dbuf<int2> &pk, cudaStream_t s) 
     return pack_pairs(A0.cols.p, v32.p, A0.v64.n, pk, s);
 }
 
+// k-paired copy of a uniform-width FP32 operator (EllView::qv/qd): one warp per
+// slice writes its values and deltas and sets the slice's flag when every delta
+// fits 16 bits.  An odd width gets a zero entry pointing at the row itself
+// (padding rows past nrows point at column 0, as everywhere in the layout).
+__global__ void k_pair_deltas(int nrows, int K, const int *cols, const float *v, float *qv,
+                              short *qd, unsigned char *flag) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= (nrows + SLICE - 1) / SLICE)
+        return;
+    const int J = (K + 1) >> 1;
+    const size_t base = (size_t)w * K * SLICE;
+    bool fits = true;
+    for (int t = lane; t < 2 * J * SLICE; t += 32) {
+        const int k = t / SLICE, r = t % SLICE, row = w * SLICE + r;
+        const int col = k < K ? cols[base + (size_t)k * SLICE + r] : (row < nrows ? row : 0);
+        const long long dl = (long long)col - row;
+        const bool ok = dl >= -32768 && dl <= 32767;
+        fits = fits && ok;
+        const size_t q = (((size_t)w * J + (k >> 1)) * 32 + (r >> 1)) * 4 + (k & 1) * 2 + (r & 1);
+        qv[q] = k < K ? v[base + (size_t)k * SLICE + r] : 0.f;
+        qd[q] = ok ? (short)dl : (short)0;
+    }
+    fits = __all_sync(0xffffffffu, fits);
+    if (lane == 0)
+        flag[w] = fits ? 1 : 0;
+}
+
+// entries 1..K-1 of every row (the self entry stays first) in ascending column
+// order, one thread per row (padded rows included): consecutive rows then meet their
+// k-th neighbours at nearly the same offset, so a warp's gather of entry k touches
+// few cache lines (in a 2D cavity 6.3 instead of 14.8 128-byte lines per gather,
+// against the distance order of the stencil lists)
+constexpr int SORT_KMAX = 64;
+__global__ void k_sort_row_entries(int np, int K, const int *cols, const float *v, int *oc,
+                                   float *ov) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np)
+        return;
+    const size_t base = (size_t)(i / SLICE) * K * SLICE + i % SLICE;
+    int c[SORT_KMAX];
+    float w[SORT_KMAX];
+    for (int k = 0; k < K; k++) {
+        c[k] = cols[base + (size_t)k * SLICE];
+        w[k] = v[base + (size_t)k * SLICE];
+    }
+    for (int k = 2; k < K; k++) {  // insertion sort of entries 1..K-1
+        const int ck = c[k];
+        const float wk = w[k];
+        int j = k - 1;
+        while (j >= 1 && c[j] > ck) {
+            c[j + 1] = c[j];
+            w[j + 1] = w[j];
+            j--;
+        }
+        c[j + 1] = ck;
+        w[j + 1] = wk;
+    }
+    for (int k = 0; k < K; k++) {
+        oc[base + (size_t)k * SLICE] = c[k];
+        ov[base + (size_t)k * SLICE] = w[k];
+    }
+}
+
+static int pair_deltas(const Ell &A0, const float *v32, AmgLevel &L, cudaStream_t s) {
+    const int nsl = (A0.nrows + SLICE - 1) / SLICE, J = (A0.K + 1) / 2;
+    const size_t nq = (size_t)nsl * J * 32;
+    MP_TRY(L.qv.alloc(nq));
+    MP_TRY(L.qd.alloc(nq));
+    MP_TRY(L.qslice.alloc(nsl));
+    const int *cols = A0.cols.p;
+    const float *vals = v32;
+    dbuf<int> sc;
+    dbuf<float> sv;
+    if (A0.K <= SORT_KMAX) {
+        const int np = nsl * SLICE;
+        MP_TRY(sc.alloc((size_t)np * A0.K));
+        MP_TRY(sv.alloc((size_t)np * A0.K));
+        k_sort_row_entries<<<(np + 255) / 256, 256, 0, s>>>(np, A0.K, A0.cols.p, v32, sc.p, sv.p);
+        MP_CHECK_LAUNCH();
+        cols = sc.p;
+        vals = sv.p;
+    }
+    k_pair_deltas<<<(unsigned)(((size_t)nsl * 32 + 255) / 256), 256, 0, s>>>(
+        A0.nrows, A0.K, cols, vals, reinterpret_cast<float *>(L.qv.p),
+        reinterpret_cast<short *>(L.qd.p), L.qslice.p);
+    MP_CHECK_LAUNCH();
+    MP_CUDA(cudaStreamSynchronize(s));  // the sorted copies are freed on return
+    L.Ad32.qv = L.qv.p;
+    L.Ad32.qd = L.qd.p;
+    L.Ad32.qslice = L.qslice.p;
+    return MP_OK;
+}
+
 static int diff_level0(const Ell &A0, AmgLevel &L, cudaStream_t s) {
     const EllView<double> A = A0.view64();
     MP_TRY(L.Ad.v32.alloc(A0.v64.n));
@@ -582,6 +675,8 @@ static int diff_level0(const Ell &A0, AmgLevel &L, cudaStream_t s) {
                                 "own node (%d rows do not)", hb);
     MP_TRY(pack_pairs(A0.cols.p, L.Ad.v32.p, A0.v64.n, L.Adpk, s));
     L.Ad32 = EllView<float>{A0.nrows, A0.ncols, A0.K, A0.cols.p, L.Ad.v32.p, A0.soff.p, L.Adpk.p};
+    if (!A0.soff.p && A0.K > 0)
+        MP_TRY(pair_deltas(A0, L.Ad.v32.p, L, s));
     return MP_OK;
 }
 
@@ -817,7 +912,11 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
             if (L.Pc.n)
                 fprintf(stderr, " P.nnz/row=%.1f R.nnz/row=%.1f", (double)L.Pc.ci.n / L.Pc.n,
                         (double)L.Rc.ci.n / L.Rc.n);
-            fprintf(stderr, " sched A=%d P=%d R=%d\n", L.sA.mode, L.sP.mode, L.sR.mode);
+            fprintf(stderr, " sched A=%d P=%d R=%d (A us:", L.sA.mode, L.sP.mode, L.sR.mode);
+            for (int m = 0; m < 6; m++)
+                if (L.sA.us[m] > 0)
+                    fprintf(stderr, " %d:%.1f", m, L.sA.us[m]);
+            fprintf(stderr, ")\n");
         }
         fprintf(stderr,
                 "[memphys amg] coarse n=%d setup %.2f s (download %.2f aggregate %.2f power %.2f "
@@ -863,6 +962,35 @@ __device__ __forceinline__ void spmv_pair(const EllView<V> &A, int w, int lane,
     T s0 = 0, s1 = 0;
     int k0 = 0;
     if constexpr (sizeof(V) == 4) {
+        if (A.qv && A.qslice[w]) {  // entries k, k + 1 of both rows: float4 values, short4 deltas
+            const int i0 = w * SLICE + 2 * lane, J = (K + 1) >> 1;
+            const size_t qb = (size_t)w * J * 32 + lane;
+            const float4 *QV = A.qv + qb;
+            const short4 *QD = A.qd + qb;
+            int j0 = 0;
+            if (DIFF && K > 0) {  // the self entry (row sum) and entry 1
+                s0 = i0 < A.nrows ? __ldg(x + i0) : T(0);
+                s1 = i0 + 1 < A.nrows ? __ldg(x + i0 + 1) : T(0);
+                const float4 v = ldop<EVF>(QV);
+                const short4 c = ldop<EVF>(QD);
+                const T g0 = __ldg(x + i0 + c.z), g1 = __ldg(x + i0 + 1 + c.w);
+                a0 = fma((T)v.z, g0 - s0, (T)v.x * s0);
+                a1 = fma((T)v.w, g1 - s1, (T)v.y * s1);
+                j0 = 1;
+            }
+#pragma unroll 2
+            for (int j = j0; j < J; j++) {
+                const float4 v = ldop<EVF>(QV + (size_t)j * 32);
+                const short4 c = ldop<EVF>(QD + (size_t)j * 32);
+                const T g0 = __ldg(x + i0 + c.x), g1 = __ldg(x + i0 + 1 + c.y);
+                const T g2 = __ldg(x + i0 + c.z), g3 = __ldg(x + i0 + 1 + c.w);
+                a0 = fma((T)v.x, DIFF ? g0 - s0 : g0, a0);
+                a1 = fma((T)v.y, DIFF ? g1 - s1 : g1, a1);
+                a0 = fma((T)v.z, DIFF ? g2 - s0 : g2, a0);
+                a1 = fma((T)v.w, DIFF ? g3 - s1 : g3, a1);
+            }
+            return;
+        }
         if (A.pk) {  // {col, value} of both rows in one 16-byte load
             const int4 *P = reinterpret_cast<const int4 *>(A.pk + base);
             if (DIFF && K > 0) {
@@ -1057,7 +1185,26 @@ __global__ void __launch_bounds__(256)
     }
     bool packed = false;
     if constexpr (sizeof(V) == 4) {
-        if (M.pk) {
+        if (M.qv && M.qslice[w]) {  // k-paired values and 16-bit deltas, one entry at a time
+            packed = true;
+            const size_t qb = (size_t)w * ((K + 1) >> 1) * 32 + lane;
+            const float *QV = reinterpret_cast<const float *>(M.qv + qb);
+            const short *QD = reinterpret_cast<const short *>(M.qd + qb);
+#pragma unroll 2
+            for (int k = q; k < K; k += 8) {
+                const size_t o = (size_t)(k >> 1) * 128 + (k & 1) * 2;
+                const float2 v = ldop<EVF>(reinterpret_cast<const float2 *>(QV + o));
+                const short2 cd = ldop<EVF>(reinterpret_cast<const short2 *>(QD + o));
+                const T g0 = __ldg(u + i0 + cd.x), g1 = __ldg(u + i0 + 1 + cd.y);
+                if (DIFF && k == 0) {
+                    a0 = fma((T)v.x, s0, a0);
+                    a1 = fma((T)v.y, s1, a1);
+                } else {
+                    a0 = fma((T)v.x, DIFF ? g0 - s0 : g0, a0);
+                    a1 = fma((T)v.y, DIFF ? g1 - s1 : g1, a1);
+                }
+            }
+        } else if (M.pk) {
             packed = true;
             const int4 *P = reinterpret_cast<const int4 *>(M.pk + base);
 #pragma unroll 2
@@ -1071,6 +1218,23 @@ __global__ void __launch_bounds__(256)
                     a0 = fma((T)__int_as_float(e.y), DIFF ? g0 - s0 : g0, a0);
                     a1 = fma((T)__int_as_float(e.w), DIFF ? g1 - s1 : g1, a1);
                 }
+            }
+        }
+    }
+    if (!packed && M.dslice && M.dslice[w]) {  // 16-bit column deltas
+        packed = true;
+#pragma unroll 2
+        for (int k = q; k < K; k += 8) {
+            const size_t o = base + (size_t)k * SLICE;
+            const short2 cd = ldop<EVF>(reinterpret_cast<const short2 *>(M.dcols + o));
+            const V2 v = ldop<EVF>(reinterpret_cast<const V2 *>(M.vals + o));
+            const T g0 = __ldg(u + i0 + cd.x), g1 = __ldg(u + i0 + 1 + cd.y);
+            if (DIFF && k == 0) {
+                a0 = fma((T)v.x, s0, a0);
+                a1 = fma((T)v.y, s1, a1);
+            } else {
+                a0 = fma((T)v.x, DIFF ? g0 - s0 : g0, a0);
+                a1 = fma((T)v.y, DIFF ? g1 - s1 : g1, a1);
             }
         }
     }
@@ -1258,7 +1422,7 @@ static int vcycle(const Amg &a, size_t l, const T *b, T *x, const int *done, boo
     const CsrView<V> Ac = LO::Ac(L), Pc = LO::Pc(L), Rc = LO::Rc(L);
     const T *dinv = LV::dinv(L);
     T *d = LV::d(L), *r = LV::r(L);
-    const int mA = l == 0 ? 0 : L.sA.mode;
+    const int mA = L.sA.mode;
     if (!head_ready) {
         const unsigned vb = (unsigned)std::min((L.n + 255) / 256, sm_count() * 8);
         const cudaError_t e = launch_pdl(k_cheb_start<T>, dim3(vb), dim3(256), s, L.n, b, dinv, d,
@@ -1398,8 +1562,9 @@ int amg_filter(const Amg &a, const double *c, double *work1, const double *scale
 template <class T, class V, bool DIFF>
 static int tune_one(size_t l, const EllView<V> &E, const CsrView<V> &Cv, int ncols, bool allow_sell,
                     OpSched &out, const int *zero, dbuf<char> &flush, cudaStream_t s) {
-    const int n = Cv.nrows;
-    if (!n) {
+    const bool csr = Cv.nrows > 0;  // level 0 has no CSR copy: sliced-ELL schedules only
+    const int n = csr ? Cv.nrows : E.nrows;
+    if (!n || (!csr && !allow_sell)) {
         out.mode = 0;
         return MP_OK;
     }
@@ -1416,6 +1581,8 @@ static int tune_one(size_t l, const EllView<V> &E, const CsrView<V> &Cv, int nco
     float best = 1e30f;
     int rc = MP_OK;
     for (int mode = sell ? 0 : 1; mode <= (sell ? 5 : 4) && rc == MP_OK; mode++) {
+        if (!csr && mode >= 1 && mode <= 4)
+            continue;
         float t[REPS];
         for (int rep = 0; rep < REPS && rc == MP_OK; rep++) {
             cudaMemsetAsync(flush.p, rep & 0xff, flush.n, s);
@@ -1479,8 +1646,7 @@ template <class T, class V, bool DIFF> static int tune_levels(Amg &a, cudaStream
         }
         if (!flush.p)
             MP_TRY(flush.alloc((size_t)192 << 20));
-        if (l > 0)
-            MP_TRY((tune_one<T, V, DIFF>(l, LO::A(L), LO::Ac(L), L.n, true, L.sA, z, flush, s)));
+        MP_TRY((tune_one<T, V, DIFF>(l, LO::A(L), LO::Ac(L), L.n, true, L.sA, z, flush, s)));
         MP_TRY((tune_one<T, V, false>(l, LT::P(L), LT::Pc(L), a.L[l + 1]->n, true, L.sP, z, flush, s)));
         MP_TRY((tune_one<T, V, false>(l, LT::R(L), LT::Rc(L), L.n, true, L.sR, z, flush, s)));
         g_tuned[key] = TuneVal{L.sA, L.sP, L.sR};

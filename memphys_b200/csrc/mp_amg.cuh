@@ -60,6 +60,11 @@ struct AmgLevel {
     Ell Ad;
     EllView<float> Ad32{};
     dbuf<int2> Adpk;         // Ad as (column, value bits) pairs
+    // level 0: Ad with entries k, k + 1 of a lane's two rows side by side (values,
+    // 16-bit column deltas, per-slice flags: EllView::qv/qd/qslice)
+    dbuf<float4> qv;
+    dbuf<short4> qd;
+    dbuf<unsigned char> qslice;
     DCsr Acd;
 };
 

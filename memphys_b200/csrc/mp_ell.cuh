@@ -39,6 +39,14 @@ template <class T> struct EllView {
     // slice fits): 2 bytes instead of 4 per entry on the index stream
     const short *dcols = nullptr;
     const unsigned char *dslice = nullptr;
+    // FP32 operators of uniform width may also carry entries k and k + 1 of a lane's
+    // two rows side by side, values in one float4 (row 0 k, row 1 k, row 0 k+1,
+    // row 1 k+1) and their 16-bit column deltas in one short4 of the same order, at
+    // qv/qd[(slice * ceil(K/2) + k/2) * 32 + lane], used in the slices whose flag
+    // qslice[s] is set: 6 instead of 8 bytes per entry, two loads per two entries
+    const float4 *qv = nullptr;
+    const short4 *qd = nullptr;
+    const unsigned char *qslice = nullptr;
 };
 
 // start offset and width of slice w

@@ -375,7 +375,10 @@ def test_fs1_projected_guess(mp_lib, make, dt, strict):
     gv, gp, rv, rp_, log = run_fs1_pair(cl, dt, 12, tol=1e-10, guess=capi.MP_GUESS_PROJECT)
     for d in range(2):
         assert np.abs(gv[d] - rv[d]).max() <= 1e-7 * max(np.abs(rv[d]).max(), 1e-12)
-    assert np.all(log[:, 1] <= 1e-10)
+    # the solve stops on the recurrence residual, as Eigen's BiCGSTAB does, and logs
+    # the true one (solver.cpp:342-343); at 1e-10 the unbordered channel system is
+    # near its FP64 floor (~1e-11) and the two differ by up to a few tens of percent
+    assert np.all(log[:, 1] <= 1.5e-10)
     *_, logx = run_fs1_pair(cl, dt, 12, tol=1e-10, guess=capi.MP_GUESS_EXTRAPOLATE)
     print("relres0 projected / extrapolated:", log[4:, 4].mean(), logx[4:, 4].mean(),
           "iterations:", log[4:, 0].sum(), logx[4:, 0].sum())
