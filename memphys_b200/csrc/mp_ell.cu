@@ -101,6 +101,46 @@ __global__ void k_ell_deltas(int nrows, int K, const int *cols, short *d, unsign
     }
 }
 
+// one thread per row (padded rows included: all column 0, value 0)
+constexpr int SORT_KMAX = 64;
+__global__ void k_ell_sort_rows(int np, int K, int *cols, double *vals) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np)
+        return;
+    const size_t base = (size_t)(i / SLICE) * K * SLICE + i % SLICE;
+    int c[SORT_KMAX];
+    double w[SORT_KMAX];
+    for (int k = 0; k < K; k++) {
+        c[k] = cols[base + (size_t)k * SLICE];
+        w[k] = vals[base + (size_t)k * SLICE];
+    }
+    for (int k = 2; k < K; k++) {  // insertion sort of entries 1..K-1
+        const int ck = c[k];
+        const double wk = w[k];
+        int j = k - 1;
+        while (j >= 1 && c[j] > ck) {
+            c[j + 1] = c[j];
+            w[j + 1] = w[j];
+            j--;
+        }
+        c[j + 1] = ck;
+        w[j + 1] = wk;
+    }
+    for (int k = 1; k < K; k++) {
+        cols[base + (size_t)k * SLICE] = c[k];
+        vals[base + (size_t)k * SLICE] = w[k];
+    }
+}
+
+int ell_sort_rows(Ell &E, cudaStream_t s) {
+    if (E.soff.p || E.K > SORT_KMAX || !E.v64.p || E.nrows == 0)
+        return MP_OK;
+    const int np = ell_padded_rows(E.nrows);
+    k_ell_sort_rows<<<(np + 255) / 256, 256, 0, s>>>(np, E.K, E.cols.p, E.v64.p);
+    MP_CHECK_LAUNCH();
+    return MP_OK;
+}
+
 int ell_make_deltas(Ell &E, cudaStream_t s, double *frac) {
     if (E.soff.p || !E.cols.p)
         return fail(MP_BAD_ARG, "ell_make_deltas: uniform-width operators only");

@@ -88,6 +88,11 @@ int ell_make_fp32(Ell &E, cudaStream_t s);
 // boundary nodes numbered last, keep their 32-bit columns).  Returns the fraction of
 // slices that use deltas in *frac (nullable).
 int ell_make_deltas(Ell &E, cudaStream_t s, double *frac = nullptr);
+// Entries 1..K-1 of every row of a uniform-width FP64 operator in ascending column
+// order (entry 0, a stencil's own node, stays first; widths above 64 are left as
+// they are).  Consecutive rows then gather their k-th neighbours at nearly the same
+// offset, and a warp's gather of entry k touches fewer cache lines.
+int ell_sort_rows(Ell &E, cudaStream_t s);
 
 // up to 4 value arrays sharing one column structure (mp_op_apply_multi)
 template <class T> struct MultiVals {

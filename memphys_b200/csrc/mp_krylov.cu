@@ -927,7 +927,8 @@ int Ppe::refresh_diag(cudaStream_t st) {
 
 int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet,
                 const double *normal, double unsteady, double conv, double diff,
-                const mp_solver_cfg &cfg_in, cudaStream_t st, int border_rule) {
+                const mp_solver_cfg &cfg_in, cudaStream_t st, int border_rule,
+                bool stencil_order) {
     cfg = Cfg::from(cfg_in);
     if (cfg.precond == MP_PRECOND_SOR)
         border_rule = 0;  // solver.cpp:30-31: no regularisation for SOR
@@ -974,6 +975,8 @@ int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet
     MP_CUDA(cudaStreamSynchronize(st));
     if (hbad)
         return fail(MP_BAD_ARG, "%d stencils do not start with their own node", hbad);
+    if (!stencil_order)
+        MP_TRY(ell_sort_rows(sys.A, st));
     const bool mixed = cfg.precision == MP_FP32;  // FP32 Krylov + FP64 refinement
     if (mixed) {
         MP_TRY(ell_make_fp32(sys.A, st));

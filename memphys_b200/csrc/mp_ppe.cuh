@@ -47,10 +47,14 @@ struct Ppe {
     Sor *sor = nullptr;  // MP_PRECOND_SOR: the row colouring
     ~Ppe();
     // border_rule 1: bordered unless a boundary node is Dirichlet (solver.cpp:29-38);
-    // 0: never bordered (systems with a nonsingular diagonal, e.g. implicit velocity)
+    // 0: never bordered (systems with a nonsingular diagonal, e.g. implicit velocity).
+    // stencil_order: keep each row's entries in the cloud's stencil order (systems
+    // whose values are rewritten in that order later); otherwise entries 1..K-1 are
+    // sorted by column (ell_sort_rows), the same matrix with better-coalesced gathers.
     int create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet,
                const double *normal, double unsteady, double conv, double diff,
-               const mp_solver_cfg &cfg, cudaStream_t st, int border_rule = 1);
+               const mp_solver_cfg &cfg, cudaStream_t st, int border_rule = 1,
+               bool stencil_order = false);
     // after the operator's values changed in place: the Jacobi diagonal again
     // (systems without a multigrid hierarchy only)
     int refresh_diag(cudaStream_t st);

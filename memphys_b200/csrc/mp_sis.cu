@@ -382,8 +382,10 @@ extern "C" int mp_sis_create(mp_cloud c, const uint8_t *boundary, const double *
     int rc;
     // solver_p.init(..., 0, 0, 1, ...) (:28): the Laplacian pressure system
     if ((rc = s->P.create(c, boundary, p_dir, normal, 0.0, 0.0, 1.0, *p_solver, st)) != MP_OK ||
-        (rc = s->U.create(c, boundary, u_dir, normal, 0.0, 0.0, 0.0, *vel_solver, st, 0)) != MP_OK ||
-        (rc = s->V.create(c, boundary, v_dir, normal, 0.0, 0.0, 0.0, *vel_solver, st, 0)) != MP_OK)
+        (rc = s->U.create(c, boundary, u_dir, normal, 0.0, 0.0, 0.0, *vel_solver, st, 0,
+                          true)) != MP_OK ||
+        (rc = s->V.create(c, boundary, v_dir, normal, 0.0, 0.0, 0.0, *vel_solver, st, 0,
+                          true)) != MP_OK)
         return bail(rc);
     s->nsys = s->P.sys.nsys;
     for (dbuf<uint8_t> *d : {&s->udir, &s->vdir, &s->pdir})
@@ -666,7 +668,8 @@ extern "C" int mp_ist_create(mp_cloud c, const uint8_t *boundary, const double *
     s->conv = conv_coeff;
     s->diff = diff_coeff;
     int rc;
-    if ((rc = s->T.create(c, boundary, dirichlet, normal, 0.0, 0.0, 0.0, *solver, 0, 0)) != MP_OK)
+    if ((rc = s->T.create(c, boundary, dirichlet, normal, 0.0, 0.0, 0.0, *solver, 0, 0, true)) !=
+        MP_OK)
         return bail(rc);
     if ((rc = s->dir.alloc(nv)) != MP_OK)
         return bail(rc);
