@@ -836,8 +836,10 @@ def profile_range(args, cl, cld, make, fs, vel0, p0, stream, pts, prm):
         in_range(lambda timed: meshless.CLOUD(pts, prm, compute_cond=True))
         return {"profile": "cloud", "builds": args.steps, "nodes": nv}
     if args.profile == "sis":
+        # --no-graph: kernels inside graphs with conditional nodes cannot be profiled
         sis = meshless.SEMI_IMPLICIT_SPLIT_SOLVER(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
-                                                  cl.p_dirichlet, 5, 1e-4, 10000)
+                                                  cl.p_dirichlet, 5, 1e-4, 10000,
+                                                  use_graph=not args.no_graph)
         st = {"u": cl.vel_bc[0].copy(), "v": cl.vel_bc[1].copy(), "p": np.zeros(sis.system_size),
               "it": 0}
 
