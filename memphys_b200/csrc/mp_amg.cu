@@ -912,11 +912,16 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
             if (L.Pc.n)
                 fprintf(stderr, " P.nnz/row=%.1f R.nnz/row=%.1f", (double)L.Pc.ci.n / L.Pc.n,
                         (double)L.Rc.ci.n / L.Rc.n);
-            fprintf(stderr, " sched A=%d P=%d R=%d (A us:", L.sA.mode, L.sP.mode, L.sR.mode);
-            for (int m = 0; m < 6; m++)
-                if (L.sA.us[m] > 0)
-                    fprintf(stderr, " %d:%.1f", m, L.sA.us[m]);
-            fprintf(stderr, ")\n");
+            fprintf(stderr, " sched A=%d P=%d R=%d", L.sA.mode, L.sP.mode, L.sR.mode);
+            const OpSched *sc[3] = {&L.sA, &L.sP, &L.sR};
+            for (int o = 0; o < 3; o++) {  // cold-L2 timings of the schedules tried
+                fprintf(stderr, " (%c us:", "APR"[o]);
+                for (int m = 0; m < OP_MODES; m++)
+                    if (sc[o]->us[m] > 0)
+                        fprintf(stderr, " %d:%.1f", m, sc[o]->us[m]);
+                fprintf(stderr, ")");
+            }
+            fprintf(stderr, "\n");
         }
         fprintf(stderr,
                 "[memphys amg] coarse n=%d setup %.2f s (download %.2f aggregate %.2f power %.2f "
@@ -1156,18 +1161,19 @@ __global__ void __launch_bounds__(256)
         level_epilogue<T, EP>(row, acc, b, dinv, d, x, y, c);
 }
 
-// sliced ELL with the slice's entries split over the CTA's 8 warps: one 64-row slice
-// per CTA, warp q takes entries k = q, q + 8, ... of both rows of every lane, the
+// sliced ELL with the slice's entries split over the CTA's KS warps: one 64-row slice
+// per CTA, warp q takes entries k = q, q + KS, ... of both rows of every lane, the
 // partial sums meet in shared memory and warp 0 adds them in warp order and runs the
 // epilogue.  For coarse levels whose slices are few and wide (level 1: 2,007 slices
 // of ~35-50 entries), where one warp per slice leaves the GPU a fifth full and a
-// lane's entries form a long dependent chain.
-template <class T, class V, bool DIFF, bool EVF, int EP>
-__global__ void __launch_bounds__(256)
+// lane's entries form a long dependent chain; KS = 8, 4, 2 trade the chain's length
+// against the number of CTAs resident at once.
+template <class T, class V, bool DIFF, bool EVF, int EP, int KS>
+__global__ void __launch_bounds__(32 * KS)
     k_level_ks(EllView<V> M, const T *__restrict__ u, const T *__restrict__ b,
                const T *__restrict__ dinv, T *d, T *x, T *y, ChebC c, const int *done) {
     using V2 = typename V2a<V>::type;
-    __shared__ T red[8][SLICE];
+    __shared__ T red[KS][SLICE];
     pdl_wait();
     pdl_trigger();
     if (*done)
@@ -1191,7 +1197,7 @@ __global__ void __launch_bounds__(256)
             const float *QV = reinterpret_cast<const float *>(M.qv + qb);
             const short *QD = reinterpret_cast<const short *>(M.qd + qb);
 #pragma unroll 2
-            for (int k = q; k < K; k += 8) {
+            for (int k = q; k < K; k += KS) {
                 const size_t o = (size_t)(k >> 1) * 128 + (k & 1) * 2;
                 const float2 v = ldop<EVF>(reinterpret_cast<const float2 *>(QV + o));
                 const short2 cd = ldop<EVF>(reinterpret_cast<const short2 *>(QD + o));
@@ -1208,7 +1214,7 @@ __global__ void __launch_bounds__(256)
             packed = true;
             const int4 *P = reinterpret_cast<const int4 *>(M.pk + base);
 #pragma unroll 2
-            for (int k = q; k < K; k += 8) {
+            for (int k = q; k < K; k += KS) {
                 const int4 e = ldop<EVF>(P + (size_t)k * (SLICE / 2));
                 const T g0 = __ldg(u + e.x), g1 = __ldg(u + e.z);
                 if (DIFF && k == 0) {
@@ -1224,7 +1230,7 @@ __global__ void __launch_bounds__(256)
     if (!packed && M.dslice && M.dslice[w]) {  // 16-bit column deltas
         packed = true;
 #pragma unroll 2
-        for (int k = q; k < K; k += 8) {
+        for (int k = q; k < K; k += KS) {
             const size_t o = base + (size_t)k * SLICE;
             const short2 cd = ldop<EVF>(reinterpret_cast<const short2 *>(M.dcols + o));
             const V2 v = ldop<EVF>(reinterpret_cast<const V2 *>(M.vals + o));
@@ -1240,7 +1246,7 @@ __global__ void __launch_bounds__(256)
     }
     if (!packed) {
 #pragma unroll 2
-        for (int k = q; k < K; k += 8) {
+        for (int k = q; k < K; k += KS) {
             const size_t o = base + (size_t)k * SLICE;
             const int2 cl = ldop<EVF>(reinterpret_cast<const int2 *>(M.cols + o));
             const V2 v = ldop<EVF>(reinterpret_cast<const V2 *>(M.vals + o));
@@ -1261,7 +1267,7 @@ __global__ void __launch_bounds__(256)
         return;
     T t0 = 0, t1 = 0;
 #pragma unroll
-    for (int r = 0; r < 8; r++) {
+    for (int r = 0; r < KS; r++) {
         t0 += red[r][2 * lane];
         t1 += red[r][2 * lane + 1];
     }
@@ -1378,7 +1384,9 @@ static int level_op(int mode, const EllView<V> &E, const CsrView<V> &Cv, const T
     case 2: e = launch_pdl(k_level_csr<T, V, 8, DIFF, EVF, EP>, dim3((unsigned)((n * 8 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
     case 3: e = launch_pdl(k_level_csr<T, V, 16, DIFF, EVF, EP>, dim3((unsigned)((n * 16 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
     case 4: e = launch_pdl(k_level_csr<T, V, 32, DIFF, EVF, EP>, dim3((unsigned)(((size_t)n * 32 + 255) / 256)), blk, s, Cv, u, b, dinv, d, x, y, c, done); break;
-    default: e = launch_pdl(k_level_ks<T, V, DIFF, EVF, EP>, dim3((unsigned)((n + SLICE - 1) / SLICE)), blk, s, E, u, b, dinv, d, x, y, c, done); break;
+    case 5: e = launch_pdl(k_level_ks<T, V, DIFF, EVF, EP, 8>, dim3((unsigned)((n + SLICE - 1) / SLICE)), dim3(256), s, E, u, b, dinv, d, x, y, c, done); break;
+    case 6: e = launch_pdl(k_level_ks<T, V, DIFF, EVF, EP, 4>, dim3((unsigned)((n + SLICE - 1) / SLICE)), dim3(128), s, E, u, b, dinv, d, x, y, c, done); break;
+    default: e = launch_pdl(k_level_ks<T, V, DIFF, EVF, EP, 2>, dim3((unsigned)((n + SLICE - 1) / SLICE)), dim3(64), s, E, u, b, dinv, d, x, y, c, done); break;
     }
     if (e != cudaSuccess)
         return fail(MP_CUDA_ERROR, "multigrid launch: %s", cudaGetErrorString(e));
@@ -1553,12 +1561,13 @@ int amg_filter(const Amg &a, const double *c, double *work1, const double *scale
 
 // ------------------------------------------------------------- autotuner
 // For each level operator and transfer, time y = M u with every schedule
-// (sliced ELL, CSR with 4/8/16/32 lanes per row) in the precision and form the
-// cycle will run (FP64; FP32; FP32 difference form for the MG32 level
-// operators) and keep the fastest.  Each timed launch starts with L2 flushed
-// (a write larger than L2), as inside the cycle, where the finer levels'
-// traffic evicts a coarse operator between its uses; an operator timed warm
-// from L2 ranks the schedules differently.  The median of five launches decides.
+// (sliced ELL with one warp or 8 / 4 / 2 warps per slice, CSR with 4/8/16/32 lanes
+// per row) in the precision and form the cycle will run (FP64; FP32; FP32
+// difference form for the MG32 level operators) and keep the fastest.  Each timed
+// launch starts with L2 flushed (a write larger than L2), as inside the cycle,
+// where the finer levels' traffic evicts a coarse operator between its uses; an
+// operator timed warm from L2 ranks the schedules differently.  The mean of the
+// middle five of nine launches decides.
 template <class T, class V, bool DIFF>
 static int tune_one(size_t l, const EllView<V> &E, const CsrView<V> &Cv, int ncols, bool allow_sell,
                     OpSched &out, const int *zero, dbuf<char> &flush, cudaStream_t s) {
@@ -1577,10 +1586,12 @@ static int tune_one(size_t l, const EllView<V> &E, const CsrView<V> &Cv, int nco
     MP_CUDA(cudaEventCreate(&e1));
     const ChebC c{};
     const bool sell = allow_sell && (E.vals || E.pk);
-    constexpr int REPS = 5;
+    // the event clock ticks in steps of about 2 us, as long as a coarse level's launch:
+    // the mean of the middle of 9 cold launches resolves what one reading cannot
+    constexpr int REPS = 9, TRIM = 2;
     float best = 1e30f;
     int rc = MP_OK;
-    for (int mode = sell ? 0 : 1; mode <= (sell ? 5 : 4) && rc == MP_OK; mode++) {
+    for (int mode = sell ? 0 : 1; mode < (sell ? OP_MODES : 5) && rc == MP_OK; mode++) {
         if (!csr && mode >= 1 && mode <= 4)
             continue;
         float t[REPS];
@@ -1595,7 +1606,10 @@ static int tune_one(size_t l, const EllView<V> &E, const CsrView<V> &Cv, int nco
             cudaEventElapsedTime(&t[rep], e0, e1);
         }
         std::sort(t, t + REPS);
-        const float ms = t[REPS / 2];
+        float ms = 0.f;
+        for (int r = TRIM; r < REPS - TRIM; r++)
+            ms += t[r];
+        ms /= (float)(REPS - 2 * TRIM);
         out.us[mode] = ms * 1e3f;
         if (ms < best) {
             best = ms;

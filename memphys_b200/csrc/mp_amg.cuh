@@ -33,10 +33,11 @@ struct DCsr {
 
 // kernel schedule of one operator, chosen by the setup-time autotuner:
 // 0 = sliced ELL (2 rows per lane), 1..4 = CSR with 4, 8, 16, 32 lanes per row,
-// 5 = sliced ELL with each slice's entries split over a CTA's 8 warps
+// 5, 6, 7 = sliced ELL with each slice's entries split over a CTA of 8, 4, 2 warps
+constexpr int OP_MODES = 8;
 struct OpSched {
     int mode = 0;
-    float us[6] = {0, 0, 0, 0, 0, 0};
+    float us[OP_MODES] = {};
 };
 
 struct AmgLevel {
