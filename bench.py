@@ -587,8 +587,8 @@ def integrators(args, cl, cld, prm, pts):
         o = [np.zeros((nv, N)) for _ in range(4)]
         fsf.single_timestep(*o, *g, 0)
         g = [a.copy() for a in o]
-        # end to end through the Python mirror: host (nv, N) arrays, transposed to the
-        # C ABI's plane-contiguous (Eigen column-major) layout and back on the host
+        # end to end through the Python mirror: host (nv, N) arrays, node-major, which
+        # the library transposes to its plane-contiguous layout and back on the device
         with capi.Timer(None) as tm:
             for k in range(K):
                 fsf.single_timestep(*o, *g, 1 + k)
@@ -597,6 +597,7 @@ def integrators(args, cl, cld, prm, pts):
         # device-resident through the C ABI: plane-contiguous device fields, ping-pong
         import ctypes as C
         L = capi.lib()
+        capi.check(L.mp_fsf_set_layout(fsf.handle, 0), "mp_fsf_set_layout")
         stream = capi.Stream()
         dev = [[capi.DeviceArray.from_host(np.ascontiguousarray(a.T)) for a in g],
                [capi.DeviceArray((N, nv)) for _ in range(4)]]
@@ -615,8 +616,8 @@ def integrators(args, cl, cld, prm, pts):
                 "unknowns_per_field": nv * N, "setup_s": round(t_setup, 2),
                 "ms_per_step_host_arrays": round(e2e_ms, 3),
                 "timing": "device fields through mp_fsf_single_timestep (ms_per_step); host "
-                          "(nv, N) arrays through the Python mirror, which transposes them to "
-                          "the plane-contiguous layout and back (ms_per_step_host_arrays)",
+                          "(nv, N) node-major arrays through the Python mirror, copied in and "
+                          "out and transposed on the device (ms_per_step_host_arrays)",
                 "w_max": float(np.abs(g[2]).max())}
 
     for name, fn in (("semi_implicit", semi_implicit), ("scalar_transport", scalar_transport),

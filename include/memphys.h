@@ -428,6 +428,11 @@ int mp_fsf_create(mp_cloud c, const uint8_t *boundary, const double *normal, con
                   int nw, int temporal_order, double rho, double mu, double dt,
                   const mp_solver_cfg *solver, mp_fsf *out);
 int mp_fsf_set_graph(mp_fsf f, int use_graph);
+/* Field layout of mp_fsf_single_timestep: 0 (default) column-major nv x N, plane c at
+ * offset c * nv, as the reference's Eigen::MatrixXd; 1 node-major (row-major nv x N,
+ * plane c of node i at i * N + c, a C-ordered numpy (nv, N) array), transposed on the
+ * device on the way in and out. */
+int mp_fsf_set_layout(mp_fsf f, int node_major);
 /* single_timestep (:250-266): vel_old = {u, v, w}, p_old -> vel_new, p_new (nv x N each);
  * the Fourier coefficients are taken from the old fields at it = 0 and carried by
  * the object afterwards, as the reference does.  Host or device pointers. */

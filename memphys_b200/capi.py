@@ -38,7 +38,8 @@ EXPORTS = [
     "mp_sis_create", "mp_sis_system_size", "mp_sis_set_graph", "mp_sis_set_tolerance",
     "mp_sis_single_timestep",
     "mp_sis_destroy", "mp_ist_create", "mp_ist_set_graph", "mp_ist_single_timestep",
-    "mp_ist_destroy", "mp_fsf_create", "mp_fsf_set_graph", "mp_fsf_single_timestep",
+    "mp_ist_destroy", "mp_fsf_create", "mp_fsf_set_graph", "mp_fsf_set_layout",
+    "mp_fsf_single_timestep",
     "mp_fsf_destroy",
     "mp_stencil_weights",
     "mp_stencil_weights_batched", "mp_stencil_plan_create", "mp_stencil_plan_run",
@@ -119,7 +120,7 @@ def lib() -> C.CDLL:
             "mp_ist_single_timestep": [vp, vp, vp, vp, vp, i, C.POINTER(i), C.POINTER(d), vp],
             "mp_ist_destroy": [vp],
             "mp_fsf_create": [vp, vp, vp, vp, vp, vp, vp, d, i, i, d, d, d, vp, C.POINTER(vp)],
-            "mp_fsf_set_graph": [vp, i],
+            "mp_fsf_set_graph": [vp, i], "mp_fsf_set_layout": [vp, i],
             "mp_fsf_single_timestep": [vp, vp, vp, vp, vp, i, vp], "mp_fsf_destroy": [vp],
             "mp_stencil_weights": [vp, i, i, vp, i, i, i, vp, vp, vp, vp, vp, vp],
             "mp_stencil_weights_batched": [i, vp, vp, vp, i, i, i, vp, vp, vp],

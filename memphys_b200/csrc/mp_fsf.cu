@@ -63,6 +63,25 @@ __global__ void k_fsf_idft(FsfDims d, const double *fre, const double *fim, cons
     phys[(size_t)ic * d.nv + iv] = v + 2.0 * acc;
 }
 
+// node-major (nv x N, row-major: plane c of node i at i N + c) <-> plane-contiguous
+// (plane c at c nv); one thread per entry, consecutive threads on consecutive nodes
+// of one plane (the plane-contiguous side coalesced, the node-major side a stride
+// of N doubles that L1/L2 absorb for the few planes of a Fourier step)
+__global__ void k_fsf_to_planes(int nv, int N, const double *node_major, double *planes) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)nv * N)
+        return;
+    const int i = (int)(t % nv), c = (int)(t / nv);
+    planes[t] = node_major[(size_t)i * N + c];
+}
+__global__ void k_fsf_to_nodes(int nv, int N, const double *planes, double *node_major) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)nv * N)
+        return;
+    const int i = (int)(t % nv), c = (int)(t / nv);
+    node_major[(size_t)i * N + c] = planes[t];
+}
+
 __device__ __forceinline__ double stencil_dot(const int *cols, const double *w, int i, int K,
                                               const double *x) {
     const size_t base = (size_t)(i / SLICE) * K * SLICE + (i % SLICE);
@@ -256,6 +275,10 @@ struct mp_fsf_s {
     dbuf<double> phys[4], uphi, vphi, xy, z, ft[4];
     bool started = false;
     bool use_graph = true;
+    // node-major fields (mp_fsf_set_layout): each passes through `stage` and a
+    // device transpose on its way in and out
+    bool node_major = false;
+    dbuf<double> stage;
     // the modes' pressure solves are independent (each mode has its own system,
     // hierarchy and Krylov vectors): one stream per mode, joined after the solves;
     // each solve's final scalars are kept (real, imaginary) for the status check
@@ -408,6 +431,17 @@ extern "C" int mp_fsf_set_graph(mp_fsf f, int use_graph) {
     return MP_OK;
 }
 
+extern "C" int mp_fsf_set_layout(mp_fsf f, int node_major) {
+    if (!f)
+        return fail(MP_BAD_ARG, "null Fourier fractional step");
+    if (node_major != 0 && node_major != 1)
+        return fail(MP_BAD_ARG, "mp_fsf_set_layout: node_major must be 0 or 1, not %d", node_major);
+    if (node_major && !f->stage.p)
+        MP_TRY(f->stage.alloc((size_t)f->d.nv * f->d.N));
+    f->node_major = node_major != 0;
+    return MP_OK;
+}
+
 extern "C" int mp_fsf_single_timestep(mp_fsf f, const double *const *vel_old, const double *p_old,
                                       double *const *vel_new, double *p_new, int it,
                                       mp_stream stream) {
@@ -424,9 +458,17 @@ extern "C" int mp_fsf_single_timestep(mp_fsf f, const double *const *vel_old, co
     const unsigned bn = (unsigned)((nn + 255) / 256), bm = (unsigned)((nm + 255) / 256);
     // physical old fields (u, v, w, p)
     const double *src_phys[4] = {vel_old[0], vel_old[1], vel_old[2], p_old};
-    for (int a = 0; a < 4; a++)
-        MP_CUDA(cudaMemcpyAsync(f->phys[a].p, src_phys[a], sizeof(double) * nn, cudaMemcpyDefault,
-                                st));
+    for (int a = 0; a < 4; a++) {
+        if (f->node_major) {
+            MP_CUDA(cudaMemcpyAsync(f->stage.p, src_phys[a], sizeof(double) * nn,
+                                    cudaMemcpyDefault, st));
+            k_fsf_to_planes<<<bn, 256, 0, st>>>(nv, d.N, f->stage.p, f->phys[a].p);
+            MP_CHECK_LAUNCH();
+        } else {
+            MP_CUDA(cudaMemcpyAsync(f->phys[a].p, src_phys[a], sizeof(double) * nn,
+                                    cudaMemcpyDefault, st));
+        }
+    }
     if (it == 0 || !f->started) {  // :254-258: coefficients of the old fields
         for (int a = 0; a < 4; a++) {
             k_fsf_dft<<<bm, 256, 0, st>>>(d, f->phys[a].p, f->twr.p, f->twi.p, f->f[a][0].p,
@@ -554,7 +596,14 @@ extern "C" int mp_fsf_single_timestep(mp_fsf f, const double *const *vel_old, co
         k_fsf_idft<<<bn, 256, 0, st>>>(d, f->f[a][0].p, f->f[a][1].p, f->itr.p, f->iti.p,
                                        f->phys[a].p);
         MP_CHECK_LAUNCH();
-        MP_CUDA(cudaMemcpyAsync(outs[a], f->phys[a].p, sizeof(double) * nn, cudaMemcpyDefault, st));
+        const double *res = f->phys[a].p;
+        if (f->node_major) {
+            // stage is free again: the inputs were transposed out of it at the start
+            k_fsf_to_nodes<<<bn, 256, 0, st>>>(nv, d.N, f->phys[a].p, f->stage.p);
+            MP_CHECK_LAUNCH();
+            res = f->stage.p;
+        }
+        MP_CUDA(cudaMemcpyAsync(outs[a], res, sizeof(double) * nn, cudaMemcpyDefault, st));
     }
     MP_CUDA(cudaStreamSynchronize(st));
     return MP_OK;

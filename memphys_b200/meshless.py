@@ -582,23 +582,30 @@ class FRACTIONAL_STEP_FOURIER:
         self.cloud = cloud
         self.nv, self.N = points.nv, 2 * int(nw) + 1
         check(capi.lib().mp_fsf_set_graph(h, int(use_graph)))
+        # numpy's C-ordered (nv, N) arrays are node-major; the library transposes them
+        # to and from its plane-contiguous layout (Eigen's column-major) on the device
+        check(capi.lib().mp_fsf_set_layout(h, 1), "mp_fsf_set_layout")
 
     def single_timestep(self, u_new, v_new, w_new, p_new, u_old, v_old, w_old, p_old, it):
         """single_timestep (:250-266): (nv, 2 nw + 1) float64 arrays; the new fields are
         written in place."""
         shape = (self.nv, self.N)
-        # Eigen's MatrixXd is column-major: plane c is contiguous, i.e. the C-ordered
-        # (N, nv) transpose
-        olds = [np.ascontiguousarray(np.asarray(a, np.float64).reshape(shape).T) for a in
+        olds = [np.ascontiguousarray(np.asarray(a, np.float64).reshape(shape)) for a in
                 (u_old, v_old, w_old, p_old)]
-        outs = [np.zeros((self.N, self.nv)) for _ in range(4)]
+        news = (u_new, v_new, w_new, p_new)
+        # results straight into C-contiguous float64 (nv, N) outputs, through a
+        # temporary otherwise
+        outs = [a if (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.shape == shape
+                      and a.flags.c_contiguous and a.flags.writeable) else np.empty(shape)
+                for a in news]
         vin = (C.c_void_p * 3)(*[a.ctypes.data for a in olds[:3]])
         vout = (C.c_void_p * 3)(*[a.ctypes.data for a in outs[:3]])
         check(capi.lib().mp_fsf_single_timestep(self.handle, vin, ptr(olds[3]), vout,
                                                 ptr(outs[3]), int(it), None),
               "mp_fsf_single_timestep")
-        for dst, src in zip((u_new, v_new, w_new, p_new), outs):
-            dst[...] = src.T
+        for dst, src in zip(news, outs):
+            if dst is not src:
+                dst[...] = src.reshape(np.shape(dst))
 
     def __del__(self):
         try:

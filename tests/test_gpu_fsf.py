@@ -51,3 +51,44 @@ def test_fsf_matches_oracle(mp_lib, period):
         print(name, np.abs(a - b).max() / scale)
         assert np.abs(a - b).max() <= 1e-7 * scale, name
     assert np.abs(g[2]).max() > 1e-3          # the z-dependent part survives the steps
+
+
+def test_fsf_layouts_agree(mp_lib):
+    """The two field layouts of mp_fsf_single_timestep: plane-contiguous (Eigen's
+    column-major, host arrays straight through the C ABI) and node-major (numpy's
+    C-ordered (nv, N), transposed on the device, the Python mirror's) give the same
+    fields bit for bit; an unknown layout is refused."""
+    import ctypes as C
+    from memphys_b200 import capi
+    cl = clouds.cavity_2d(16, seed=5)
+    nw, N = 2, 5
+    prm = meshless.PARAMETERS(solver_type="cuda_bicgstab_amg", solver_tolerance=1e-9, n_iter=5000)
+    prm.rho, prm.mu, prm.dt = 1.0, 0.01, 1e-3
+    pts = meshless.POINTS(cl)
+    cld = meshless.CLOUD(pts, prm, compute_cond=False)
+    make = lambda: meshless.FRACTIONAL_STEP_FOURIER(pts, cld, prm, cl.u_dirichlet, cl.v_dirichlet,
+                                                    cl.u_dirichlet, cl.p_dirichlet, 1.0, nw, 2)
+    a, b = make(), make()
+    L = capi.lib()
+    assert L.mp_fsf_set_layout(b.handle, 2) == capi.MP_BAD_ARG
+    capi.check(L.mp_fsf_set_layout(b.handle, 0))
+    z = np.arange(N) / N
+    x, y = cl.xyz[:, 0], cl.xyz[:, 1]
+    g = [np.repeat(cl.vel_bc[0][:, None], N, 1), np.zeros((cl.nv, N)),
+         np.where(cl.boundary[:, None], 0.0,
+                  0.05 * (np.sin(np.pi * x) * np.sin(np.pi * y))[:, None]
+                  * np.cos(2 * np.pi * z)[None, :]), np.zeros((cl.nv, N))]
+    ga = [q.copy() for q in g]
+    gb = [np.ascontiguousarray(q.T) for q in g]     # (N, nv): plane c contiguous
+    for it in range(3):
+        oa = [np.zeros((cl.nv, N)) for _ in range(4)]
+        a.single_timestep(*oa, *ga, it)
+        ga = oa
+        ob = [np.zeros((N, cl.nv)) for _ in range(4)]
+        vin = (C.c_void_p * 3)(*[q.ctypes.data for q in gb[:3]])
+        vout = (C.c_void_p * 3)(*[q.ctypes.data for q in ob[:3]])
+        capi.check(L.mp_fsf_single_timestep(b.handle, vin, capi.ptr(gb[3]), vout,
+                                            capi.ptr(ob[3]), it, None))
+        gb = ob
+    for name, qa, qb in zip("uvwp", ga, gb):
+        assert np.array_equal(qa, qb.T), name
