@@ -906,7 +906,8 @@ int amg_create(Amg **out, const Ell &A0, const Cfg &cfg, int store, cudaStream_t
         fprintf(stderr, "[memphys amg] hierarchy checksum %016llx\n", (unsigned long long)hsum);
         for (size_t l = 0; l < a->L.size(); l++) {
             const AmgLevel &L = *a->L[l];
-            fprintf(stderr, "[memphys amg] level %zu n=%d A.K=%d", l, L.n, L.A64.K);
+            fprintf(stderr, "[memphys amg] level %zu n=%d A.K=%d lmax=%.3f", l, L.n, L.A64.K,
+                    L.lmax);
             if (L.Ac.n)
                 fprintf(stderr, " A.nnz/row=%.1f", (double)L.Ac.ci.n / L.n);
             if (L.Pc.n)

@@ -3,6 +3,7 @@
 // C ABI (SOLVER::init / SOLVER::general_solve, solver.cpp:14-79, 283-363).
 #include <cstddef>
 #include <cmath>
+#include <vector>
 #include "mp_krylov.cuh"
 #include "mp_amg.cuh"
 #include "mp_cloud.cuh"
@@ -89,6 +90,25 @@ __device__ __forceinline__ void ell_pair(const EllView<T> &A, int w, int lane,
 struct RedBuf {
     double *partials;
     unsigned int *ticket;
+};
+
+// Preconditioner of a bordered system B = [A e; e^T 0] (e = ones, A e = 0: the
+// all-Neumann pressure operator) under the multigrid cycle V:
+//   M^-1 [r; r_n] = [V(r - a e) + c e; a],  a = mean(r),  c = (r_n - e^T V(r - a e)) / n.
+// Feeding V the constant component of r (the border's column) and taking the border
+// entry as it comes makes B M^-1 badly conditioned in those two directions; with them
+// taken out B M^-1 is the identity up to a rank-one term for an exact V, and the
+// Krylov iteration needs about what the same operator needs without the border
+// (measured at 1M nodes: 26 instead of 41 sweeps for one right-hand side).  V is
+// linear, so V(r - a e) = V(r) - a V(e): the cycle runs on r as before (its first
+// smoothing step stays fused into the update that writes r) and the kernels after it
+// apply the correction with ve = V(e), ave = A ve and sve = e^T ve, computed once.
+// As A e = 0 to rounding, the c e part enters B y only through the border row, whose
+// value is then r_n by construction.  ve == nullptr: no deflation.
+template <class T> struct Defl {
+    const T *ve, *ave;
+    double sve;
+    int nv;
 };
 
 #define KRYLOV_SMEM __shared__ double red_smem[32 * 4];
@@ -292,12 +312,14 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
 template <class T, int PK>
 __global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_update_p(int nv, int bordered, const T *r, T *p, const T *v, T *y, const T *dinv,
-               const BicgScalars *S, AmgHead<T> H) {
+               BicgScalars *S, AmgHead<T> H, RedBuf R, Defl<T> D) {
+    KRYLOV_SMEM
     if (S->done)
         return;
     const double beta = (S->rho / S->rho_old) * (S->alpha / S->omega);
     const T bt = (T)beta, om = (T)S->omega;
     const int stride = gridDim.x * blockDim.x;
+    double acc[1] = {0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += stride) {
         const T pi = r[i] + bt * (p[i] - om * v[i]);
         p[i] = pi;
@@ -305,20 +327,25 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
             y[i] = dinv[i] * pi;
         if (PK == PK_EXTERNAL && H.d)
             H.d[i] = H.dinv[i] * pi * H.inv_theta;
+        acc[0] += (double)pi;
     }
     if (bordered && blockIdx.x == 0 && threadIdx.x == 0) {
         const T pi = r[nv] + bt * (p[nv] - om * v[nv]);
         p[nv] = pi;
         if (PK != PK_NONE)
-            y[nv] = pi;
+            y[nv] = pi;  // the deflated preconditioner reads p_n here (k_spmv_alpha)
     }
+    if (D.ve && grid_reduce<1>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0)
+        S->dfl_a[0] = acc[0] / nv;
 }
 
-// v = A y, alpha = rho / (r0 . v)
+// v = B y, alpha = rho / (r0 . v).  Deflated (D.ve): y holds V(p) and p_n in its
+// border entry; v = B y' for y' = [V(p) - a ve + c e; a] (see Defl), whose border
+// entry replaces p_n in y for the x update
 template <class T>
 __global__ void __launch_bounds__(KT, KT_BLOCKS)
-    k_spmv_alpha(EllView<T> A, int bordered, const T *y, T *v, const T *r0, BicgScalars *S,
-                 RedBuf R) {
+    k_spmv_alpha(EllView<T> A, int bordered, T *y, T *v, const T *r0, BicgScalars *S,
+                 RedBuf R, Defl<T> D) {
     KRYLOV_SMEM
     if (S->done)
         return;
@@ -328,14 +355,18 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
     for (int w = gwarp(); w < nsl; w += nwarps) {
         T a0, a1, s0, s1;
         ell_pair(A, w, lane, y, a0, a1, s0, s1);
-        const T yb = bordered ? y[nv] : T(0);
+        // the border column's value (read after the gathers: nothing extra stays live
+        // across them)
+        const T yb = D.ve ? (T)S->dfl_a[0] : (bordered ? y[nv] : T(0));
         const int i0 = w * SLICE + 2 * lane;
         T as[2] = {a0, a1}, ss[2] = {s0, s1};
 #pragma unroll
         for (int q = 0; q < 2; q++) {
             const int i = i0 + q;
             if (i < nv) {
-                const T vi = as[q] + yb;
+                T vi = as[q] + yb;
+                if (D.ve)
+                    vi -= yb * D.ave[i];
                 v[i] = vi;
                 acc[0] += (double)r0[i] * vi;
                 acc[1] += (double)ss[q];
@@ -345,7 +376,13 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
     if (grid_reduce<2>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
         double d = acc[0];
         if (bordered) {
-            const T vb = (T)acc[1];
+            T vb = (T)acc[1];
+            if (D.ve) {
+                const T pn = y[nv], da = (T)S->dfl_a[0];
+                S->dfl_c[0] = ((double)pn - acc[1] + (double)da * D.sve) / nv;
+                vb = pn;
+                y[nv] = da;
+            }
             v[nv] = vb;
             d += (double)r0[nv] * vb;
         }
@@ -361,12 +398,15 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
 template <class T, int PK>
 __global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_update_s(int nv, int bordered, const T *r, const T *v, T *s, T *z, const T *dinv, T *x,
-               const T *y, BicgScalars *S, RedBuf R, cudaGraphConditionalHandle h, AmgHead<T> H) {
+               const T *y, BicgScalars *S, RedBuf R, cudaGraphConditionalHandle h, AmgHead<T> H,
+               Defl<T> D) {
     KRYLOV_SMEM
     if (S->done)
         return;
     const T al = (T)S->alpha;
-    double acc[1] = {0};
+    // deflated: x += alpha y' with y'_i = y_i - a ve_i + c (the border entry of y is a)
+    const T da = D.ve ? (T)S->dfl_a[0] : T(0), dc = D.ve ? (T)S->dfl_c[0] : T(0);
+    double acc[2] = {0, 0};
     const int stride = gridDim.x * blockDim.x;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += stride) {
         const T si = r[i] - al * v[i];
@@ -375,11 +415,15 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
             z[i] = dinv[i] * si;
         if (PK == PK_EXTERNAL && H.d)
             H.d[i] = H.dinv[i] * si * H.inv_theta;
-        x[i] = x[i] + al * y[i];
+        const T yi = D.ve ? y[i] - da * D.ve[i] + dc : y[i];
+        x[i] = x[i] + al * yi;
         acc[0] += (double)si * si;
+        acc[1] += (double)si;
     }
-    if (grid_reduce<1>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
+    if (grid_reduce<2>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
         double ss = acc[0];
+        if (D.ve)
+            S->dfl_a[1] = acc[1] / nv;
         if (bordered) {
             const T si = r[nv] - al * v[nv];
             s[nv] = si;
@@ -399,11 +443,11 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
     }
 }
 
-// t = A z, omega = (t . s) / (t . t)
+// t = B z, omega = (t . s) / (t . t); deflated as k_spmv_alpha, z' = [V(s) - a ve + c e; a]
 template <class T>
 __global__ void __launch_bounds__(KT, KT_BLOCKS)
-    k_spmv_omega(EllView<T> A, int bordered, const T *z, T *t, const T *s, BicgScalars *S,
-                 RedBuf R) {
+    k_spmv_omega(EllView<T> A, int bordered, T *z, T *t, const T *s, BicgScalars *S,
+                 RedBuf R, Defl<T> D) {
     KRYLOV_SMEM
     if (S->done)
         return;
@@ -413,14 +457,16 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
     for (int w = gwarp(); w < nsl; w += nwarps) {
         T a0, a1, s0, s1;
         ell_pair(A, w, lane, z, a0, a1, s0, s1);
-        const T zb = bordered ? z[nv] : T(0);
+        const T zb = D.ve ? (T)S->dfl_a[1] : (bordered ? z[nv] : T(0));
         const int i0 = w * SLICE + 2 * lane;
         T as[2] = {a0, a1}, ss[2] = {s0, s1};
 #pragma unroll
         for (int q = 0; q < 2; q++) {
             const int i = i0 + q;
             if (i < nv) {
-                const T ti = as[q] + zb;
+                T ti = as[q] + zb;
+                if (D.ve)
+                    ti -= zb * D.ave[i];
                 t[i] = ti;
                 acc[0] += (double)ti * ti;
                 acc[1] += (double)ti * s[i];
@@ -431,7 +477,13 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
     if (grid_reduce<3>(acc, R.partials, R.ticket, red_smem) && threadIdx.x == 0) {
         double tt = acc[0], ts = acc[1];
         if (bordered) {
-            const T tb = (T)acc[2];
+            T tb = (T)acc[2];
+            if (D.ve) {
+                const T da = (T)S->dfl_a[1];
+                S->dfl_c[1] = ((double)s[nv] - acc[2] + (double)da * D.sve) / nv;
+                tb = s[nv];
+                z[nv] = da;
+            }
             t[nv] = tb;
             tt += (double)tb * tb;
             ts += (double)tb * s[nv];
@@ -447,15 +499,17 @@ __global__ void __launch_bounds__(KT, KT_BLOCKS)
 template <class T>
 __global__ void __launch_bounds__(KT, KT_BLOCKS)
     k_update_xr(int nsys, T *x, const T *z, const T *s, const T *t, T *r, const T *r0,
-                BicgScalars *S, RedBuf R, cudaGraphConditionalHandle h) {
+                BicgScalars *S, RedBuf R, cudaGraphConditionalHandle h, Defl<T> D) {
     KRYLOV_SMEM
     if (S->done)
         return;
     const T om = (T)S->omega;
+    const T da = D.ve ? (T)S->dfl_a[1] : T(0), dc = D.ve ? (T)S->dfl_c[1] : T(0);
     double acc[2] = {0, 0};
     const int stride = gridDim.x * blockDim.x;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsys; i += stride) {
-        x[i] = x[i] + om * z[i];
+        const T zi = (D.ve && i < D.nv) ? z[i] - da * D.ve[i] + dc : z[i];
+        x[i] = x[i] + om * zi;
         const T ri = s[i] - om * t[i];
         r[i] = ri;
         acc[0] += (double)ri * ri;
@@ -670,7 +724,8 @@ int Krylov::alloc(int nv_, int bordered_, bool mixed, bool external_pc) {
 template <class T>
 static int issue_iteration(const PpeSystem &P, const EllView<T> &A, const T *dinv, T *x, T *b,
                            T *r, T *r0, T *p, T *v, T *s_, T *t, T *y, T *z, BicgScalars *S,
-                           RedBuf R, int pk, cudaGraphConditionalHandle h, cudaStream_t st) {
+                           RedBuf R, int pk, cudaGraphConditionalHandle h, cudaStream_t st,
+                           Defl<T> D) {
     const int nv = P.nv, nsys = P.nsys, bd = P.bordered;
     T *yy = pk == PK_NONE ? p : y;
     T *zz = pk == PK_NONE ? s_ : z;
@@ -680,31 +735,32 @@ static int issue_iteration(const PpeSystem &P, const EllView<T> &A, const T *din
     k_restart<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, x, b, r, r0, S, R);
     MP_CHECK_LAUNCH();
     if (pk == PK_JACOBI)
-        k_update_p<T, PK_JACOBI><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S, H);
+        k_update_p<T, PK_JACOBI><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S, H, R, D);
     else if (pk == PK_NONE)
-        k_update_p<T, PK_NONE><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S, H);
+        k_update_p<T, PK_NONE><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S, H, R, D);
     else
-        k_update_p<T, PK_EXTERNAL><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S, H);
+        k_update_p<T, PK_EXTERNAL><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, p, v, yy, dinv, S, H, R,
+                                                                  D);
     MP_CHECK_LAUNCH();
     if (pk == PK_EXTERNAL)
         MP_TRY(amg_apply<T>(*P.amg, p, yy, &S->done, st, head));
-    k_spmv_alpha<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, yy, v, r0, S, R);
+    k_spmv_alpha<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, yy, v, r0, S, R, D);
     MP_CHECK_LAUNCH();
     if (pk == PK_JACOBI)
         k_update_s<T, PK_JACOBI><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, x, yy,
-                                                                S, R, h, H);
+                                                                S, R, h, H, D);
     else if (pk == PK_NONE)
         k_update_s<T, PK_NONE><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, x, yy, S,
-                                                              R, h, H);
+                                                              R, h, H, D);
     else
         k_update_s<T, PK_EXTERNAL><<<vec_blocks(nv), KT, 0, st>>>(nv, bd, r, v, s_, zz, dinv, x,
-                                                                  yy, S, R, h, H);
+                                                                  yy, S, R, h, H, D);
     MP_CHECK_LAUNCH();
     if (pk == PK_EXTERNAL)
         MP_TRY(amg_apply<T>(*P.amg, s_, zz, &S->done, st, head));
-    k_spmv_omega<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, zz, t, s_, S, R);
+    k_spmv_omega<T><<<slice_blocks(nv), KT, 0, st>>>(A, bd, zz, t, s_, S, R, D);
     MP_CHECK_LAUNCH();
-    k_update_xr<T><<<vec_blocks(nsys), KT, 0, st>>>(nsys, x, zz, s_, t, r, r0, S, R, h);
+    k_update_xr<T><<<vec_blocks(nsys), KT, 0, st>>>(nsys, x, zz, s_, t, r, r0, S, R, h, D);
     MP_CHECK_LAUNCH();
     return MP_OK;
 }
@@ -720,7 +776,8 @@ int Ppe::issue_prologue64(cudaGraphConditionalHandle h, cudaStream_t st) {
 int Ppe::issue_sweep64(cudaGraphConditionalHandle h, cudaStream_t st) {
     return issue_iteration<double>(sys, sys.A.view64(), sys.dinv.p, W.x.p, W.b64.p, W.r.p,
                                    W.r0.p, W.p.p, W.v.p, W.s.p, W.t.p, W.y.p, W.z.p, W.scal.p,
-                                   RedBuf{W.partials.p, W.ticket.p}, pk(), h, st);
+                                   RedBuf{W.partials.p, W.ticket.p}, pk(), h, st,
+                                   Defl<double>{W.ve.p, W.ave.p, W.sve, sys.nv});
 }
 
 int Ppe::issue_epilogue64(cudaStream_t st) {
@@ -755,7 +812,8 @@ int Ppe::issue_ir_inner_prologue(cudaGraphConditionalHandle h, cudaStream_t st) 
 int Ppe::issue_ir_sweep(cudaGraphConditionalHandle h, cudaStream_t st) {
     return issue_iteration<float>(sys, sys.diff32(), sys.dinv32.p, W.e32.p, W.b32.p, W.r32.p,
                                   W.r032.p, W.p32.p, W.v32.p, W.s32.p, W.t32.p, W.y32.p, W.z32.p,
-                                  W.scal.p, RedBuf{W.partials.p, W.ticket.p}, pk(), h, st);
+                                  W.scal.p, RedBuf{W.partials.p, W.ticket.p}, pk(), h, st,
+                                  Defl<float>{W.ve32.p, W.ave32.p, W.sve32, sys.nv});
 }
 
 int Ppe::issue_ir_update(cudaStream_t st) {
@@ -925,6 +983,85 @@ int Ppe::refresh_diag(cudaStream_t st) {
     return MP_OK;
 }
 
+// ------------------------------------------- deflated preconditioner set-up
+__global__ void k_defl_ones(int nv, int nsys, double *e, float *e32) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nsys)
+        return;
+    const double v = i < nv ? 1.0 : 0.0;
+    if (e)
+        e[i] = v;
+    if (e32)
+        e32[i] = (float)v;
+}
+__global__ void k_defl_f2d(int n, const float *a, double *b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        b[i] = (double)a[i];
+}
+__global__ void k_defl_d2f(int n, const double *a, float *b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        b[i] = (float)a[i];
+}
+
+// ve = V(e), ave = A ve and sve = e^T ve of a bordered system under a multigrid of two or
+// more levels (Defl), in the precision its Krylov iteration runs: FP32 for MP_FP32's
+// inner solves (the FP32 cycle; A ve formed in FP64 and rounded), FP64 otherwise.  A
+// one-level hierarchy is already the bordered system's exact inverse.
+static int defl_setup(Ppe &P, cudaStream_t st) {
+    PpeSystem &sys = P.sys;
+    Krylov &W = P.W;
+    if (P.cfg.precond != MP_PRECOND_AMG || !sys.bordered || !sys.amg || sys.amg->L.size() < 2)
+        return MP_OK;
+    const int nv = sys.nv, nsys = sys.nsys;
+    const unsigned g = (unsigned)((nsys + 255) / 256);
+    const int *zero = sys.amg->zero_flag.p;
+    std::vector<double> h(nv);
+    dbuf<double> ve64;
+    if (P.cfg.precision == MP_FP32) {
+        dbuf<float> e32;
+        dbuf<double> ave64;
+        MP_TRY(e32.alloc(nsys));
+        MP_TRY(W.ve32.alloc(nsys));
+        MP_TRY(W.ave32.alloc(nv));
+        MP_TRY(ve64.alloc(nsys));
+        MP_TRY(ave64.alloc(nv));
+        k_defl_ones<<<g, 256, 0, st>>>(nv, nsys, nullptr, e32.p);
+        MP_CHECK_LAUNCH();
+        MP_CUDA(cudaMemsetAsync(W.ve32.p, 0, sizeof(float) * nsys, st));
+        MP_TRY(amg_apply<float>(*sys.amg, e32.p, W.ve32.p, zero, st, false));
+        k_defl_f2d<<<g, 256, 0, st>>>(nv, W.ve32.p, ve64.p);
+        MP_CHECK_LAUNCH();
+        MP_TRY(ell_spmv<double>(sys.A.view64(), ve64.p, ave64.p, 1.0, 0.0, st));
+        k_defl_d2f<<<g, 256, 0, st>>>(nv, ave64.p, W.ave32.p);
+        MP_CHECK_LAUNCH();
+        MP_CUDA(cudaMemcpyAsync(h.data(), ve64.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
+        MP_CUDA(cudaStreamSynchronize(st));
+        double sum = 0.0;
+        for (double v : h)
+            sum += v;
+        W.sve32 = sum;
+        return MP_OK;
+    }
+    dbuf<double> e;
+    MP_TRY(e.alloc(nsys));
+    MP_TRY(W.ve.alloc(nsys));
+    MP_TRY(W.ave.alloc(nv));
+    k_defl_ones<<<g, 256, 0, st>>>(nv, nsys, e.p, nullptr);
+    MP_CHECK_LAUNCH();
+    MP_CUDA(cudaMemsetAsync(W.ve.p, 0, sizeof(double) * nsys, st));
+    MP_TRY(amg_apply<double>(*sys.amg, e.p, W.ve.p, zero, st, false));
+    MP_TRY(ell_spmv<double>(sys.A.view64(), W.ve.p, W.ave.p, 1.0, 0.0, st));
+    MP_CUDA(cudaMemcpyAsync(h.data(), W.ve.p, sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
+    MP_CUDA(cudaStreamSynchronize(st));
+    double sum = 0.0;
+    for (double v : h)
+        sum += v;
+    W.sve = sum;
+    return MP_OK;
+}
+
 int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet,
                 const double *normal, double unsteady, double conv, double diff,
                 const mp_solver_cfg &cfg_in, cudaStream_t st, int border_rule,
@@ -998,6 +1135,7 @@ int Ppe::create(mp_cloud_s *c, const uint8_t *boundary, const uint8_t *dirichlet
     if (cfg.precond == MP_PRECOND_SOR)
         MP_TRY(sor_setup(*this, st));
     MP_TRY(W.alloc(nv, bordered, mixed, cfg.precond == MP_PRECOND_AMG));
+    MP_TRY(defl_setup(*this, st));
     MP_CUDA(cudaStreamSynchronize(st));
     return MP_OK;
 }

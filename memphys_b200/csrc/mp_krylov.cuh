@@ -34,6 +34,10 @@ struct BicgScalars {
     double relres0;     // ||b - A x0|| / ||b|| of the initial guess (first residual of a solve)
     double abs_tol2;    // absolute floor of the stopping ||r||^2 (0: the relative test alone)
     double guess_theta; // weight of the learned correction in the last initial guess
+    // bordered systems under the multigrid: the mean of each preconditioner input
+    // (dfl_a) and the constant that satisfies the border row (dfl_c), first and second
+    // application of a sweep (see Defl in mp_krylov.cu)
+    double dfl_a[2], dfl_c[2];
 };
 
 struct PpeSystem {

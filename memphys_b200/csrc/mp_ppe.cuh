@@ -34,6 +34,12 @@ struct Krylov {
     dbuf<double> partials;
     dbuf<unsigned int> ticket;
     dbuf<BicgScalars> scal;
+    // bordered systems under the multigrid: ve = V(1), the cycle applied to the
+    // constant vector, ave = A ve and sve = sum(ve), per Krylov precision (empty when
+    // the preconditioner is not deflated)
+    dbuf<double> ve, ave;
+    dbuf<float> ve32, ave32;
+    double sve = 0.0, sve32 = 0.0;
     int alloc(int nv, int bordered, bool mixed, bool external_pc);
 };
 
