@@ -36,10 +36,13 @@ struct Krylov {
     dbuf<BicgScalars> scal;
     // bordered systems under the multigrid: ve = V(1), the cycle applied to the
     // constant vector, ave = A ve and sve = sum(ve), per Krylov precision (empty when
-    // the preconditioner is not deflated)
+    // the preconditioner is not deflated); the weights of the input's mean, 1 on
+    // interior rows and dbeta on boundary rows (dflag), and their sum dwe
     dbuf<double> ve, ave;
     dbuf<float> ve32, ave32;
     double sve = 0.0, sve32 = 0.0;
+    dbuf<unsigned char> dflag;
+    double dbeta = 1.0, dwe = 0.0;
     int alloc(int nv, int bordered, bool mixed, bool external_pc);
 };
 

@@ -303,6 +303,42 @@ def test_pressure_solve(cav, solver_type):
     assert p.n_iter_actual[-1] == it and x_old[-1] == x[-1]
 
 
+@pytest.mark.parametrize("solver_type", ["cuda_bicgstab_amg", "cuda_bicgstab_amg_mg32"])
+def test_bordered_system_needs_no_extra_iterations(mp_lib, solver_type):
+    """The all-Neumann pressure system is bordered (solver.cpp:205-213).  Its multigrid
+    preconditioner takes the border's two directions out of the cycle (the mean of the
+    cycle's input, weighted as the left null vector, and the constant that satisfies
+    the border row); a bordered solve had needed twice the iterations of the same
+    operator with Dirichlet boundary rows.  A right-hand side in the operator's range
+    (b = A f): the bordered solve stays within a few sweeps of the Dirichlet one, and
+    returns f up to the constant the border row fixes, with a border unknown of 0."""
+    cl = clouds.cavity_2d(150, seed=7)
+    prm = meshless.PARAMETERS(solver_type=solver_type, solver_tolerance=1e-8, n_iter=1000)
+    pts = meshless.POINTS(cl)
+    cld = meshless.CLOUD(pts, prm, compute_cond=False).fetch()
+    nv, bnd = cl.nv, cl.boundary
+    W = np.where(bnd[:, None], cl.normal[:, :1] * cld.grad_x_coeff
+                 + cl.normal[:, 1:2] * cld.grad_y_coeff, cld.laplacian_coeff)
+    nb = cld.nb_points_col
+    A = sp.csr_matrix((W.ravel(), nb.ravel(), np.arange(nv + 1) * nb.shape[1]), shape=(nv, nv))
+    x, y = cl.xyz[:, 0], cl.xyz[:, 1]
+    f = np.cos(np.pi * x) * np.cos(2 * np.pi * y) + 0.3 * x * y
+    its = {}
+    for name, dflag, b in (("neumann", np.zeros(nv, np.uint8), np.append(A @ f, 0.0)),
+                           ("dirichlet", bnd.astype(np.uint8), np.where(bnd, f, A @ f))):
+        s = meshless.SOLVER().init(pts, cld, prm, dflag, 0.0, 0.0, 1.0, False)
+        assert s.system_size == len(b)
+        out = np.zeros(len(b))
+        its[name], rr = s.general_solve(pts, prm, out, np.zeros(len(b)), b)
+        assert rr <= 1e-8
+        if name == "neumann":
+            g = f - f.mean()
+            assert np.abs(out[:nv] - g).max() <= 1e-5 * np.abs(g).max()
+            assert abs(out[nv]) <= 1e-8 * np.abs(b).max()
+    print("sweeps bordered / Dirichlet rows:", its)
+    assert its["neumann"] <= its["dirichlet"] + 4
+
+
 def run_fs1_pair(cl, dt, nsteps, solver_type="cuda_bicgstab_amg", tol=1e-11, use_graph=True,
                  guess=None):
     prm = meshless.PARAMETERS(solver_type=solver_type, solver_tolerance=tol, n_iter=5000)
