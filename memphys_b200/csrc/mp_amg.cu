@@ -1431,7 +1431,10 @@ static int vcycle(const Amg &a, size_t l, const T *b, T *x, const int *done, boo
     const CsrView<V> Ac = LO::Ac(L), Pc = LO::Pc(L), Rc = LO::Rc(L);
     const T *dinv = LV::dinv(L);
     T *d = LV::d(L), *r = LV::r(L);
-    const int mA = L.sA.mode;
+    // the finest operator keeps one warp per slice: timed cold, the split schedules
+    // come within a few percent of it and the tuner picked them at times, but inside
+    // the cycle they ran slower (38-42 against 32-35 us per pass at 1M nodes)
+    const int mA = l == 0 ? 0 : L.sA.mode;
     if (!head_ready) {
         const unsigned vb = (unsigned)std::min((L.n + 255) / 256, sm_count() * 8);
         const cudaError_t e = launch_pdl(k_cheb_start<T>, dim3(vb), dim3(256), s, L.n, b, dinv, d,
@@ -1661,7 +1664,8 @@ template <class T, class V, bool DIFF> static int tune_levels(Amg &a, cudaStream
         }
         if (!flush.p)
             MP_TRY(flush.alloc((size_t)192 << 20));
-        MP_TRY((tune_one<T, V, DIFF>(l, LO::A(L), LO::Ac(L), L.n, true, L.sA, z, flush, s)));
+        if (l > 0)
+            MP_TRY((tune_one<T, V, DIFF>(l, LO::A(L), LO::Ac(L), L.n, true, L.sA, z, flush, s)));
         MP_TRY((tune_one<T, V, false>(l, LT::P(L), LT::Pc(L), a.L[l + 1]->n, true, L.sP, z, flush, s)));
         MP_TRY((tune_one<T, V, false>(l, LT::R(L), LT::Rc(L), L.n, true, L.sR, z, flush, s)));
         g_tuned[key] = TuneVal{L.sA, L.sP, L.sR};
