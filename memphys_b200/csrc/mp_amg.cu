@@ -10,6 +10,7 @@
 #include <type_traits>
 #include <cmath>
 #include <unordered_map>
+#include <condition_variable>
 #include "mp_amg.cuh"
 #include "mp_ppe.cuh"
 
@@ -467,35 +468,78 @@ static int coarse_inverse(const Csr &A, std::vector<double> &inv, bool *bordered
     inv.assign((size_t)m * m, 0.0);
     for (int i = 0; i < m; i++)
         inv[(size_t)i * m + i] = 1.0;
-    for (int k = 0; k < m; k++) {
-        int p = k;
-        for (int i = k + 1; i < m; i++)
-            if (std::fabs(M[(size_t)i * m + k]) > std::fabs(M[(size_t)p * m + k]))
-                p = i;
-        if (M[(size_t)p * m + k] == 0.0)
-            return fail(MP_BREAKDOWN, "multigrid coarse operator is singular");
-        if (p != k)
-            for (int j = 0; j < m; j++) {
-                std::swap(M[(size_t)k * m + j], M[(size_t)p * m + j]);
-                std::swap(inv[(size_t)k * m + j], inv[(size_t)p * m + j]);
-            }
-        const double d = 1.0 / M[(size_t)k * m + k];
-        for (int j = 0; j < m; j++) {
-            M[(size_t)k * m + j] *= d;
-            inv[(size_t)k * m + j] *= d;
+    // Gauss-Jordan with partial pivoting.  Each step's pivot row is chosen and scaled
+    // by thread 0, then every other row is updated by the thread that owns it (rows
+    // split in fixed ranges): the rows' updates are independent, so the inverse does
+    // not depend on the thread count.  Columns left of the pivot are already reduced
+    // and are skipped in M.
+    const unsigned nt = std::max(1u, std::min(host_threads(), (unsigned)(m / 64 + 1)));
+    std::mutex mu;
+    std::condition_variable cv;
+    unsigned arrived = 0, gen = 0;
+    auto barrier = [&]() {
+        std::unique_lock<std::mutex> lk(mu);
+        const unsigned g = gen;
+        if (++arrived == nt) {
+            arrived = 0;
+            gen++;
+            cv.notify_all();
+        } else {
+            cv.wait(lk, [&] { return gen != g; });
         }
-        for (int i = 0; i < m; i++) {
-            if (i == k)
-                continue;
-            const double f = M[(size_t)i * m + k];
-            if (f == 0.0)
-                continue;
-            for (int j = 0; j < m; j++) {
-                M[(size_t)i * m + j] -= f * M[(size_t)k * m + j];
-                inv[(size_t)i * m + j] -= f * inv[(size_t)k * m + j];
+    };
+    bool singular = false;
+    auto work = [&](unsigned t) {
+        const int lo = (int)((long long)m * t / nt), hi = (int)((long long)m * (t + 1) / nt);
+        for (int k = 0; k < m; k++) {
+            if (t == 0) {
+                int p = k;
+                for (int i = k + 1; i < m; i++)
+                    if (std::fabs(M[(size_t)i * m + k]) > std::fabs(M[(size_t)p * m + k]))
+                        p = i;
+                if (M[(size_t)p * m + k] == 0.0) {
+                    singular = true;
+                } else {
+                    if (p != k)
+                        for (int j = 0; j < m; j++) {
+                            std::swap(M[(size_t)k * m + j], M[(size_t)p * m + j]);
+                            std::swap(inv[(size_t)k * m + j], inv[(size_t)p * m + j]);
+                        }
+                    const double d = 1.0 / M[(size_t)k * m + k];
+                    for (int j = k; j < m; j++)
+                        M[(size_t)k * m + j] *= d;
+                    for (int j = 0; j < m; j++)
+                        inv[(size_t)k * m + j] *= d;
+                }
             }
+            barrier();
+            if (singular)
+                return;
+            const double *mk = &M[(size_t)k * m], *ik = &inv[(size_t)k * m];
+            for (int i = lo; i < hi; i++) {
+                if (i == k)
+                    continue;
+                double *mi = &M[(size_t)i * m], *ii = &inv[(size_t)i * m];
+                const double f = mi[k];
+                if (f == 0.0)
+                    continue;
+                for (int j = k + 1; j < m; j++)
+                    mi[j] -= f * mk[j];
+                mi[k] = 0.0;
+                for (int j = 0; j < m; j++)
+                    ii[j] -= f * ik[j];
+            }
+            barrier();
         }
-    }
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; t++)
+        th.emplace_back(work, t);
+    work(0);
+    for (auto &x : th)
+        x.join();
+    if (singular)
+        return fail(MP_BREAKDOWN, "multigrid coarse operator is singular");
     return MP_OK;
 }
 
